@@ -1,0 +1,393 @@
+"""Benchmark: effective-stiffness solves of a 128^3 cross-ply fibre composite on B200.
+
+Workload (one "step"): the six unit-load Lippmann-Schwinger solves (tol 1e-6, rtol on the
+normalised equilibrium residual) of one seeded 128^3 microstructure with 4 alternating
+0/90 layers, fibre radius 4 voxels, 45% fibre volume fraction, phase contrast ~26
+(matrix lambda, mu = 2.593, 1.111; fibres 19.44, 29.17), solved as one batch of six
+instances; outputs the 6x6 effective stiffness. Each rank solves its own microstructure
+(seed = rank): weak scaling, no collective on the data path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Rank 0 prints one JSON line. `value` = solves/s over all ranks with inputs resident in
+HBM; `e2e` = the same through the public API from pinned host buffers (lambda, mu in,
+C_eff out) per step.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s & voxel-iter/s at 1e-6 resid: learned+batched vs plain (1 B200)"
+WORKLOAD = "c2_128"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--depth", type=int, default=0)
+    p.add_argument("--cpu-sample-s", type=float, default=12.0)
+    return p.parse_args()
+
+
+def workload(seed):
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+
+    st = fibres.config_structure(WORKLOAD, seed=seed)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(*st.n, *st.extents)
+    return st, g, lm, mu
+
+
+def config_dict(st, depth):
+    n = st.n
+    return {
+        "workload": f"{WORKLOAD}: {n[0]}^3 cross-ply, 4 layers 0/90, fibre radius 4 vox, "
+                    f"vf {st.volume_fraction:.3f}, contrast ~26, 6 unit loads per step, "
+                    f"tol rtol=1e-6 on the equilibrium residual, "
+                    f"{'plain Moulinec-Suquet' if depth == 0 else f'Anderson m={depth}'}",
+        "grid": list(n),
+        "loads_per_step": 6,
+        "anderson_depth": depth,
+        "fields": "FP32 fields and FFTs, FP64 residual norms",
+        "l2": "inputs larger than L2: 6 instances x (strain 50 MB + spectrum 51 MB) + Lame 17 MB",
+    }
+
+
+def fixture_iters(depth):
+    path = os.path.join(ROOT, "tests", "golden", f"bench_{WORKLOAD}.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        key = f"iters_d{depth}"
+        if key in d:
+            return [int(v) for v in d[key]]
+    return None
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.idx)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(lm, mu, g, depth, budget_s, threads):
+    """Oracle (NumPy/SciPy port of the reference JAX solver) on the host cores: time whole
+    iterations of one load case until `budget_s` is spent. Returns (s per voxel-iter,
+    iterations timed)."""
+    from oracle import ls_oracle as O
+
+    og = O.Grid(g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz)
+    eb = np.zeros(6)
+    eb[0] = 1.0
+    total_t, total_it = 0.0, 0
+    chunk = 2
+    while total_t < budget_s:
+        t0 = time.perf_counter()
+        _, _, it = O.lippmann_schwinger(lm, mu, eb, og, rtol=0.0, atol=0.0, depth=depth,
+                                        maxiter=chunk, dtype=np.float32, workers=threads)
+        total_t += time.perf_counter() - t0
+        total_it += it
+        chunk = min(chunk * 2, 16)
+    return total_t / (total_it * g.number_of_voxels), total_it
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count()
+    st, g, lm, mu = workload(0)
+    iters = fixture_iters(args.depth)
+    if iters is None:
+        print(json.dumps({"impl": "reference", "unavailable": "iteration-count fixture missing"}))
+        return
+    mean_iters = float(np.mean(iters))
+    nv = g.number_of_voxels
+    budget = max(2.0, args.cpu_sample_s / 2)
+    for _ in range(args.warmup):
+        cpu_sample(lm, mu, g, args.depth, 0.5, threads)
+    spv = []
+    its = 0
+    for _ in range(args.steps):
+        s, n = cpu_sample(lm, mu, g, args.depth, budget, threads)
+        spv.append(s)
+        its += n
+    s_per_vi = float(np.mean(spv))
+    vips = 1.0 / s_per_vi
+    solves = vips / (nv * mean_iters)
+    sample = (f"{its} iterations of one load case at {g.nx}^3 over {args.steps} steps, "
+              f"scaled by the FP64 oracle's iterations per solve ({mean_iters:.1f})")
+    out = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": solves,
+        "unit": "solves/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 6.0 / solves * 1000.0,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": config_dict(st, args.depth),
+        "voxel_iter_per_s": vips,
+        "cpu_baseline": {"value": solves, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": solves, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "reference JAX CPU path unavailable (jax not installed); timed the NumPy/SciPy "
+                "port of lippmann_schwinger_jax (oracle/ls_oracle.py) with all host threads",
+    }
+    print(json.dumps(out))
+
+
+def own_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from jaxmaterials_b200.solver import CONVERGED, Solver
+
+    st, g, lm, mu = workload(rank)
+    dev = torch.device("cuda", local)
+    lm_d = torch.as_tensor(lm, device=dev)
+    mu_d = torch.as_tensor(mu, device=dev)
+    eye = np.eye(6, dtype=np.float32)
+    s = Solver(g, batch=6, depth=args.depth)
+    stream = torch.cuda.current_stream(dev)
+    maxiter = 20000
+
+    def step(lm_t, mu_t):
+        return s.solve(lm_t, mu_t, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
+
+    for _ in range(max(args.warmup, 3)):
+        r = step(lm_d, mu_d)
+    assert np.all(r.status == CONVERGED), r.status
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timing
+    launches0 = s.kernel_launches()
+    iters_total = 0
+    c_eff = None
+    with ClockSampler(local) as clocks:
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            r = step(lm_d, mu_d)
+            iters_total += int(r.iters.sum())
+            c_eff = r.mean_sigma
+        t1.record(stream)
+        barrier()
+    launches = s.kernel_launches() - launches0
+    ms = t0.elapsed_time(t1)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    it_t = torch.tensor([iters_total], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(it_t, op=dist.ReduceOp.SUM)
+    ms_max = float(ms_t.item())
+    solves = 6.0 * args.steps * world / (ms_max / 1000.0)
+    vips = float(it_t.item()) * g.number_of_voxels / (ms_max / 1000.0)
+
+    # ---- end to end through the public API from pinned host buffers
+    lm_h = torch.from_numpy(lm).pin_memory()
+    mu_h = torch.from_numpy(mu).pin_memory()
+    lm_e = torch.empty_like(lm_d)
+    mu_e = torch.empty_like(mu_d)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        lm_e.copy_(lm_h, non_blocking=True)
+        mu_e.copy_(mu_h, non_blocking=True)
+        r = step(lm_e, mu_e)  # returns C_eff (6x6 FP64) on the host
+    e1.record(stream)
+    barrier()
+    ems = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ems, op=dist.ReduceOp.MAX)
+    e2e = 6.0 * args.steps * world / (float(ems.item()) / 1000.0)
+
+    # ---- per-pass timing for the roofline (same stream, CUDA events, full workload)
+    passes = s.profile_passes(lm_d, mu_d, batch=6, reps=5)
+    nv, nm, b = g.number_of_voxels, g.number_of_modes, 6
+    spec = 6 * nm * 8
+    real = 6 * nv * 4
+    alg = {
+        "xpass": b * 2 * spec,
+        "ypass_inverse": b * 2 * spec,
+        "ypass_forward": b * 2 * spec,
+        "zpass": b * (2 * spec + 2 * real) + 2 * nv * 4,
+        "finalize": 0,
+    }
+    top = max(passes, key=passes.get)
+    peak, peak_kind = measured_peak()
+    achieved = alg[top] / (passes[top] / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(f"{WORKLOAD}:{top}")
+    loop_ms = sum(passes.values())
+    loop_gbs = 152.0 * nv * b / (loop_ms / 1000.0) / 1e9
+
+    if rank == 0:
+        out = {
+            "metric": METRIC,
+            "value": solves,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": config_dict(st, args.depth),
+            "voxel_iter_per_s": vips,
+            "iters_per_solve": float(iters_total) / (6 * args.steps),
+            "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
+            "gpu_launches": int(launches),
+            "roofline": {
+                "bound": "hbm",
+                "kernel": top,
+                "achieved": achieved,
+                "peak": peak,
+                "peak_source": peak_kind,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg[top],
+                "ms_per_launch": passes[top],
+                "passes_ms": passes,
+                "loop_at_152B_per_voxel_iter_GBs": loop_gbs,
+                "loop_frac_of_peak": loop_gbs / peak,
+            },
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 2 * nv * 4,
+                    "d2h_bytes_per_step": 36 * 8},
+            "clocks": clocks.summary(),
+        }
+        if world == 1:
+            iters = fixture_iters(args.depth)
+            threads = os.cpu_count()
+            s_per_vi, n = cpu_sample(lm, mu, g, args.depth, args.cpu_sample_s, threads)
+            mean_it = float(np.mean(iters)) if iters else out["iters_per_solve"]
+            out["cpu_baseline"] = {
+                "value": 1.0 / s_per_vi / (nv * mean_it),
+                "unit": "solves/s",
+                "cores": threads,
+                "kind": "port",
+                "sample": f"{n} iterations of one load case at {g.nx}^3 (NumPy/SciPy port, FP32), "
+                          f"scaled by {mean_it:.1f} iterations per solve",
+                "voxel_iter_per_s": 1.0 / s_per_vi,
+            }
+        print(json.dumps(out))
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        own_arm(args)
+
+
+if __name__ == "__main__":
+    main()

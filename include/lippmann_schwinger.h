@@ -1,0 +1,114 @@
+/* C ABI of liblippmannschwinger.so, the B200 (sm_100a) Lippmann-Schwinger solver.
+ *
+ * Drop-in for the reference library built from cuda/src (yang-chen-2022/JaxMaterials):
+ * the first entry point has the reference's exact signature and meaning; the others are
+ * additive. No function takes or returns torch or other framework types.
+ *
+ * Conventions shared by every entry point:
+ *   - fields are float32, C order, z fastest: Lame fields [nx][ny][nz]; strain and
+ *     stress [6][nx][ny][nz] in Voigt order (xx, yy, zz, xy, xz, yz) with TENSOR shear
+ *     entries (eps_xy, not gamma_xy = 2 eps_xy);
+ *   - voxels = (nx, ny, nz), extents = (Lx, Ly, Lz) (cuda/src/common.hh:73-91);
+ *   - the criterion is e = sqrt(<|div sigma|^2>) / |<sigma>| evaluated in Fourier space
+ *     (cuda/src/lippmann_schwinger.hh:76-89) and the loop stops when
+ *     e < max(rtol * e0, atol), e0 being e at the first iterate.
+ *   - a negative return value is an error; lsb_last_error() describes it.
+ */
+#ifndef LIPPMANN_SCHWINGER_B200_H
+#define LIPPMANN_SCHWINGER_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces lippmann_schwinger_solve (cuda/src/lippmann_schwinger.hh:176-184,
+ * cuda/src/lippmann_schwinger.cu:236-257), bound by ctypes in
+ * src/jaxmaterials/solver/lippmann_schwinger.py:284-322.
+ *
+ * lambda, mu:   host float[nx*ny*nz]  (lambda FIRST, as in the C signature)
+ * epsilon_bar:  host float[6]          macroscopic strain
+ * epsilon, sigma: caller-allocated host float[6*nx*ny*nz], overwritten with the
+ *               solution and sigma = C : epsilon
+ * Returns the number of updates performed; == maxiter means "not converged", as in the
+ * reference. Negative on error (the reference only printed errors). Device buffers are
+ * cached between calls with the same grid on the same device; see
+ * lippmann_schwinger_release(). */
+int lippmann_schwinger_solve(float *lambda, float *mu, float *epsilon_bar,
+                             float *epsilon, float *sigma, int *voxels, float *extents,
+                             float rtol, float atol, int maxiter, int verbose);
+
+/* No reference counterpart: frees the buffers cached by lippmann_schwinger_solve. */
+void lippmann_schwinger_release(void);
+
+/* ------------------------------------------------------------------ handle API
+ * Additive exports (no reference counterpart). A solver owns the device buffers of one
+ * grid and a batch capacity; every solve takes DEVICE pointers and runs on the
+ * solver's stream. Instances of one call share lambda and mu (e.g. the six load cases
+ * of an effective-stiffness computation). */
+typedef struct lsb_solver lsb_solver;
+
+/* Statuses written to status[] by the solve calls. */
+enum {
+  LSB_CONVERGED = 1,
+  LSB_MAXITER = 2,
+  LSB_NONFINITE = 3
+};
+
+/* Stop rules: LSB_RULE_CUDA stops when e < max(rtol e0, atol)
+ * (cuda/src/lippmann_schwinger.cu:205); LSB_RULE_JAX when e <= max(rtol e0, atol)
+ * (src/jaxmaterials/solver/lippmann_schwinger.py:196-206). */
+enum { LSB_RULE_CUDA = 0, LSB_RULE_JAX = 1 };
+
+/* Creates a solver for voxels/extents with room for `batch` instances and Anderson
+ * depth `depth` (0 = plain Moulinec-Suquet iteration) on the current CUDA device. */
+int lsb_create(lsb_solver **out, const int voxels[3], const float extents[3], int batch,
+               int depth);
+void lsb_destroy(lsb_solver *solver);
+/* Stream (cudaStream_t passed as void*) for all later work; NULL = legacy default. */
+int lsb_set_stream(lsb_solver *solver, void *stream);
+
+/* Solves `batch` instances that share d_lambda, d_mu (device float[nv]).
+ * eps_bar:   host float[batch*6]
+ * d_eps0:    optional device float[batch*6*nv] warm start (NULL: eps = eps_bar)
+ * d_eps:     device float[batch*6*nv] output strain
+ * d_sigma:   optional device float[batch*6*nv] output stress sigma(eps)
+ * mean_sigma: optional host double[batch*6], mean stress per instance (FP64 sums)
+ * iters, status: host int[batch]; residual: optional host double[batch] final e.
+ * Blocks the calling thread until every instance has stopped. */
+int lsb_solve(lsb_solver *solver, int batch, const float *d_lambda, const float *d_mu,
+              const float *eps_bar, const float *d_eps0, float *d_eps, float *d_sigma,
+              double *mean_sigma, float rtol, float atol, int maxiter, int rule,
+              int *iters, int *status, double *residual);
+
+/* Criterion history of the last solve: host double[batch*len], e after every
+ * evaluation (0 for evaluations that did not happen). len <= maxiter + 1. */
+int lsb_history(lsb_solver *solver, double *out, int len);
+
+/* No reference counterpart: number of kernels this solver has enqueued so far. */
+long long lsb_kernel_launches(lsb_solver *solver);
+
+/* No reference counterpart: times every pass of one iteration with CUDA events on the
+ * solver's stream, averaged over `reps` iterations that never stop (tolerances 0).
+ * ms_out (host float[5]) = x pass (forward DFT, residual, Gamma^0, inverse DFT),
+ * finalize, inverse y pass, z pass (C2R, update, stress, R2C), forward y pass.
+ * d_eps (device float[batch*6*nv]) is used as the strain work buffer. */
+int lsb_profile_passes(lsb_solver *solver, int batch, const float *d_lambda,
+                       const float *d_mu, float *d_eps, int reps, float *ms_out);
+
+/* Effective stiffness from the six unit macroscopic strains (the caller in
+ * src/jaxmaterials/data/data.py:178-186): row k of c_eff (host double[36]) is the mean
+ * stress for eps_bar = e_k. Host lambda/mu float[nv]; iters host int[6]. */
+int lsb_c_eff(const float *lambda, const float *mu, const int voxels[3],
+              const float extents[3], float rtol, float atol, int maxiter, int depth,
+              double *c_eff, int *iters);
+
+/* Message of the last error on this thread ("" if none). */
+const char *lsb_last_error(void);
+/* Library ABI version. */
+int lsb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIPPMANN_SCHWINGER_B200_H */

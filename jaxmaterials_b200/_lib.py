@@ -1,0 +1,84 @@
+"""ctypes binding of ``liblippmannschwinger.so`` (declarations in
+``include/lippmann_schwinger.h``).
+
+The library is looked up next to this file first, then through the dynamic loader
+(``LD_LIBRARY_PATH``), as the reference wrapper does
+(``src/jaxmaterials/solver/lippmann_schwinger.py:284-290``). A missing library is an
+error: there is no fallback implementation.
+"""
+
+import ctypes
+import os
+import threading
+
+LIB_NAME = "liblippmannschwinger.so"
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_lock = threading.Lock()
+_lib = None
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_void_p = ctypes.c_void_p
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "lippmann_schwinger_solve": (ctypes.c_int, [c_float_p, c_float_p, c_float_p, c_float_p,
+                                                c_float_p, c_int_p, c_float_p, ctypes.c_float,
+                                                ctypes.c_float, ctypes.c_int, ctypes.c_int]),
+    "lippmann_schwinger_release": (None, []),
+    "lsb_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), c_int_p, c_float_p, ctypes.c_int,
+                                  ctypes.c_int]),
+    "lsb_destroy": (None, [c_void_p]),
+    "lsb_set_stream": (ctypes.c_int, [c_void_p, c_void_p]),
+    "lsb_solve": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_float_p,
+                                 c_void_p, c_void_p, c_void_p, c_double_p, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
+                                 c_double_p]),
+    "lsb_history": (ctypes.c_int, [c_void_p, c_double_p, ctypes.c_int]),
+    "lsb_kernel_launches": (ctypes.c_longlong, [c_void_p]),
+    "lsb_profile_passes": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p,
+                                          ctypes.c_int, c_float_p]),
+    "lsb_c_eff": (ctypes.c_int, [c_float_p, c_float_p, c_int_p, c_float_p, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_int, ctypes.c_int, c_double_p,
+                                 c_int_p]),
+    "lsb_last_error": (ctypes.c_char_p, []),
+    "lsb_version": (ctypes.c_int, []),
+}
+
+
+class LibraryError(RuntimeError):
+    pass
+
+
+def library_path():
+    return os.path.join(_HERE, LIB_NAME)
+
+
+def load():
+    """Load the library once and attach the signatures; raise if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = library_path()
+        try:
+            lib = ctypes.CDLL(path if os.path.exists(path) else LIB_NAME)
+        except OSError as exc:
+            raise LibraryError(
+                f"Unable to load {LIB_NAME}: build it with `make -C jaxmaterials_b200/csrc` "
+                "(or __graft_entry__.build()) or put it on LD_LIBRARY_PATH.") from exc
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc, what="call"):
+    """Raise on a negative return code, with the library's message."""
+    if rc < 0:
+        msg = load().lsb_last_error().decode(errors="replace")
+        raise LibraryError(f"{what} failed ({rc}): {msg}")
+    return rc

@@ -1,0 +1,269 @@
+"""Lippmann-Schwinger solver entry points (reference:
+``src/jaxmaterials/solver/lippmann_schwinger.py``).
+
+* ``lippmann_schwinger_cuda`` keeps the reference wrapper's signature and behaviour
+  (``:268-329``): host NumPy arrays in, ``(epsilon, sigma, iter)`` out, ``RuntimeError``
+  when ``iter == maxiter``. Unlike the reference wrapper it passes lambda FIRST, matching
+  the C signature (the reference passes ``mu`` into the ``lambda`` slot, ``:310-312``).
+* ``lippmann_schwinger`` (also exported as ``lippmann_schwinger_jax``) keeps the
+  signature of ``lippmann_schwinger_jax`` (``:146-265``) and accepts NumPy arrays or
+  CUDA torch tensors; torch tensors stay on the device.
+* ``Solver`` is the reusable handle behind both (device buffers, batches of load
+  cases sharing lambda and mu), and ``c_eff`` assembles the effective stiffness from the
+  six unit loads (``src/jaxmaterials/data/data.py:178-186``).
+
+All arithmetic happens in the CUDA library; this module only marshals arguments.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from .. import _lib
+from ..common import GridSpec
+
+__all__ = [
+    "Solver",
+    "SolveResult",
+    "lippmann_schwinger",
+    "lippmann_schwinger_jax",
+    "lippmann_schwinger_cuda",
+    "c_eff",
+    "CONVERGED",
+    "MAXITER",
+    "NONFINITE",
+    "RULE_CUDA",
+    "RULE_JAX",
+]
+
+CONVERGED, MAXITER, NONFINITE = 1, 2, 3
+RULE_CUDA, RULE_JAX = 0, 1
+
+
+def _fptr(a):
+    return a.ctypes.data_as(_lib.c_float_p)
+
+
+def _grid_args(grid_spec):
+    voxels = np.array([grid_spec.nx, grid_spec.ny, grid_spec.nz], dtype=np.int32)
+    extents = np.array([grid_spec.Lx, grid_spec.Ly, grid_spec.Lz], dtype=np.float32)
+    return voxels, extents
+
+
+def lippmann_schwinger_cuda(lmbda, mu, epsilon_bar, grid_spec, rtol=1e-6, atol=1.0e-20,
+                            maxiter=32, verbose=0):
+    """Solve through the reference C signature ``lippmann_schwinger_solve``.
+
+    :arg lmbda: Lame parameter lambda, shape (nx, ny, nz)
+    :arg mu: Lame parameter mu, shape (nx, ny, nz)
+    :arg epsilon_bar: macroscopic strain (6,), Voigt order, tensor shear entries
+    :arg grid_spec: grid specification
+    :arg rtol, atol: tolerances on the normalised divergence
+    :arg maxiter: maximal number of iterations
+    :arg verbose: 0 silent, 1 summary, 2 per-iteration table (printed by the library)
+    Returns ``(epsilon, sigma, iter)`` as float32 arrays of shape (6, nx, ny, nz).
+    """
+    lib = _lib.load()
+    voxels, extents = _grid_args(grid_spec)
+    lm = np.ascontiguousarray(lmbda, dtype=np.float32)
+    m = np.ascontiguousarray(mu, dtype=np.float32)
+    eb = np.ascontiguousarray(epsilon_bar, dtype=np.float32)
+    shape = (6, grid_spec.nx, grid_spec.ny, grid_spec.nz)
+    if lm.shape != shape[1:] or m.shape != shape[1:] or eb.shape != (6,):
+        raise ValueError("lmbda/mu must have shape (nx, ny, nz) and epsilon_bar shape (6,)")
+    epsilon = np.empty(shape, dtype=np.float32)
+    sigma = np.empty(shape, dtype=np.float32)
+    it = lib.lippmann_schwinger_solve(
+        _fptr(lm), _fptr(m), _fptr(eb), _fptr(epsilon), _fptr(sigma),
+        voxels.ctypes.data_as(_lib.c_int_p), _fptr(extents), float(rtol), float(atol),
+        int(maxiter), int(verbose))
+    _lib.check(it, "lippmann_schwinger_solve")
+    if it == maxiter:
+        raise RuntimeError(f"Solver failed to converge after {maxiter} iterations")
+    return epsilon, sigma, it
+
+
+@dataclass
+class SolveResult:
+    epsilon: object        # (B, 6, nx, ny, nz) torch tensor on the device
+    sigma: object          # same, or None
+    iters: np.ndarray      # (B,) updates performed
+    status: np.ndarray     # (B,) CONVERGED / MAXITER / NONFINITE
+    residual: np.ndarray   # (B,) final criterion value
+    mean_sigma: np.ndarray  # (B, 6) FP64 mean stress
+
+
+class Solver:
+    """Reusable solver for one grid: owns the device buffers of ``batch`` instances.
+
+    Instances of one ``solve`` call share lambda and mu and differ in epsilon_bar (and
+    optionally the warm start). Uses the current CUDA device and torch's current stream.
+    """
+
+    def __init__(self, grid_spec, batch=1, depth=0):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise _lib.LibraryError("a CUDA device is required")
+        self._lib = _lib.load()
+        self.grid_spec = grid_spec
+        self.batch = int(batch)
+        self.depth = int(depth)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        voxels, extents = _grid_args(grid_spec)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.lsb_create(ctypes.byref(h), voxels.ctypes.data_as(_lib.c_int_p),
+                                        _fptr(extents), self.batch, self.depth), "lsb_create")
+        self._h = h
+        self._last_batch = 0
+        self._last_maxiter = 0
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.lsb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _as_device(self, a, shape):
+        import torch
+
+        t = torch.as_tensor(a, dtype=torch.float32, device=self.device)
+        t = t.contiguous()
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"expected shape {tuple(shape)}, got {tuple(t.shape)}")
+        return t
+
+    def solve(self, lmbda, mu, epsilon_bar, rtol=1e-6, atol=1e-20, maxiter=32,
+              rule=RULE_CUDA, epsilon0=None, want_sigma=True, out=None):
+        """Run the fixed point for every row of ``epsilon_bar`` (shape (B, 6) or (6,))."""
+        import torch
+
+        g = self.grid_spec
+        nshape = (g.nx, g.ny, g.nz)
+        eb = np.ascontiguousarray(np.atleast_2d(np.asarray(epsilon_bar, dtype=np.float32)))
+        b = eb.shape[0]
+        if eb.shape[1] != 6 or b < 1 or b > self.batch:
+            raise ValueError(f"epsilon_bar must have shape (B, 6) with 1 <= B <= {self.batch}")
+        lm = self._as_device(lmbda, nshape)
+        m = self._as_device(mu, nshape)
+        e0 = None
+        if epsilon0 is not None:
+            e0 = self._as_device(epsilon0, (b, 6) + nshape)
+        eps = out if out is not None else torch.empty((b, 6) + nshape, dtype=torch.float32,
+                                                      device=self.device)
+        sig = torch.empty_like(eps) if want_sigma else None
+        iters = np.zeros(b, dtype=np.int32)
+        status = np.zeros(b, dtype=np.int32)
+        resid = np.zeros(b, dtype=np.float64)
+        mean = np.zeros((b, 6), dtype=np.float64)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(self._lib.lsb_set_stream(self._h, ctypes.c_void_p(stream)), "lsb_set_stream")
+        rc = self._lib.lsb_solve(
+            self._h, b, ctypes.c_void_p(lm.data_ptr()), ctypes.c_void_p(m.data_ptr()),
+            _fptr(eb), ctypes.c_void_p(e0.data_ptr() if e0 is not None else 0),
+            ctypes.c_void_p(eps.data_ptr()),
+            ctypes.c_void_p(sig.data_ptr() if sig is not None else 0),
+            mean.ctypes.data_as(_lib.c_double_p), float(rtol), float(atol), int(maxiter),
+            int(rule), iters.ctypes.data_as(_lib.c_int_p), status.ctypes.data_as(_lib.c_int_p),
+            resid.ctypes.data_as(_lib.c_double_p))
+        _lib.check(rc, "lsb_solve")
+        self._last_batch = b
+        self._last_maxiter = int(maxiter)
+        return SolveResult(eps, sig, iters, status, resid, mean)
+
+    def kernel_launches(self):
+        """Kernels enqueued by this solver so far."""
+        return int(self._lib.lsb_kernel_launches(self._h))
+
+    def profile_passes(self, lmbda, mu, batch=None, reps=5):
+        """Average CUDA-event time (ms) of each pass of one iteration:
+        dict with keys xpass, finalize, ypass_inverse, zpass, ypass_forward."""
+        import torch
+
+        g = self.grid_spec
+        b = self.batch if batch is None else int(batch)
+        lm = self._as_device(lmbda, g.shape)
+        m = self._as_device(mu, g.shape)
+        work = torch.empty((b, 6) + g.shape, dtype=torch.float32, device=self.device)
+        ms = np.zeros(5, dtype=np.float32)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(self._lib.lsb_set_stream(self._h, ctypes.c_void_p(stream)), "lsb_set_stream")
+        _lib.check(self._lib.lsb_profile_passes(
+            self._h, b, ctypes.c_void_p(lm.data_ptr()), ctypes.c_void_p(m.data_ptr()),
+            ctypes.c_void_p(work.data_ptr()), int(reps), _fptr(ms)), "lsb_profile_passes")
+        return dict(zip(["xpass", "finalize", "ypass_inverse", "zpass", "ypass_forward"],
+                        [float(v) for v in ms]))
+
+    def history(self):
+        """Criterion after every evaluation of the last solve, shape (B, maxiter + 1)."""
+        n = self._last_maxiter + 1
+        out = np.zeros((self._last_batch, n), dtype=np.float64)
+        _lib.check(self._lib.lsb_history(self._h, out.ctypes.data_as(_lib.c_double_p), n),
+                   "lsb_history")
+        return out
+
+
+_solver_cache = {}
+
+
+def _cached_solver(grid_spec, batch, depth):
+    import torch
+
+    key = (grid_spec.nx, grid_spec.ny, grid_spec.nz, grid_spec.Lx, grid_spec.Ly,
+           grid_spec.Lz, batch, depth, torch.cuda.current_device())
+    s = _solver_cache.get(key)
+    if s is None:
+        if len(_solver_cache) > 8:
+            _solver_cache.clear()
+        s = Solver(grid_spec, batch=batch, depth=depth)
+        _solver_cache[key] = s
+    return s
+
+
+def lippmann_schwinger(lmbda, mu, epsilon_bar, grid_spec, rtol=1e-6, atol=1e-20, depth=0,
+                       maxiter=32, dtype=np.float32, epsilon0=None):
+    """Signature of the reference ``lippmann_schwinger_jax`` (``:146-265``).
+
+    Returns ``(epsilon, sigma, iter)`` with fields of shape (6, nx, ny, nz): NumPy arrays
+    for NumPy input, CUDA tensors for torch input. Stops when
+    e <= max(rtol e0, atol) or after ``maxiter`` updates, without raising (as the
+    reference). Fields are FP32; norms and the stop decision are FP64.
+    """
+    if np.dtype(dtype) != np.float32:
+        raise NotImplementedError("the CUDA solver carries FP32 fields (dtype=float32)")
+    import torch
+
+    as_torch = isinstance(lmbda, torch.Tensor)
+    s = _cached_solver(grid_spec, 1, depth)
+    e0 = None if epsilon0 is None else (
+        epsilon0.reshape((1, 6) + grid_spec.shape) if as_torch
+        else np.asarray(epsilon0, np.float32).reshape((1, 6) + grid_spec.shape))
+    eb = np.asarray(epsilon_bar.cpu() if isinstance(epsilon_bar, torch.Tensor) else epsilon_bar,
+                    dtype=np.float32).reshape(1, 6)
+    r = s.solve(lmbda, mu, eb, rtol=rtol, atol=atol, maxiter=maxiter, rule=RULE_JAX,
+                epsilon0=e0)
+    eps, sig = r.epsilon[0], r.sigma[0]
+    if not as_torch:
+        eps, sig = eps.cpu().numpy(), sig.cpu().numpy()
+    return eps, sig, int(r.iters[0])
+
+
+lippmann_schwinger_jax = lippmann_schwinger
+
+
+def c_eff(lmbda, mu, grid_spec, rtol=1e-6, atol=1e-20, maxiter=1000, depth=0, solver=None):
+    """Effective stiffness: row k = mean stress for the unit strain e_k (tensor shear).
+
+    Solves the six load cases as one batch. Returns ``(C, iters, result)``."""
+    s = solver if solver is not None else _cached_solver(grid_spec, 6, depth)
+    r = s.solve(lmbda, mu, np.eye(6, dtype=np.float32), rtol=rtol, atol=atol,
+                maxiter=maxiter, rule=RULE_CUDA, want_sigma=False)
+    return r.mean_sigma.copy(), r.iters.copy(), r

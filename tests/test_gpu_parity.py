@@ -1,0 +1,242 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle, the golden fixtures of the
+reference's Python solver and, when built, the reference's own CUDA library.
+
+Tolerances (FP32 fields, FP64 norms):
+* fields vs an FP64 oracle run with the same number of updates: max-abs error relative to
+  the field's max-abs below 2e-5;
+* C_eff vs the FP64 oracle at tol 1e-6: relative Frobenius error below 1e-5;
+* iteration counts: equal to the oracle's, +-1 where round-off sits at the threshold.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ls_oracle as O
+from tests.conftest import ROOT, reference_material
+
+pytestmark = pytest.mark.gpu
+
+EXT = (1.2, 0.8, 0.9)
+PY_SIZES = {"even": (64, 48, 32), "odd": (57, 43, 37)}
+CU_SIZES = {"even": (48, 64, 32), "odd": (47, 61, 37)}
+CU_EXT = (1.1, 0.9, 0.7)
+EPS_BAR = np.array([2.1, 0.9, 0.8, 0.4, 0.9, 0.5], dtype=np.float32)
+
+
+def relmax(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.fixture(scope="module")
+def ls(built_library):
+    import torch
+
+    assert torch.cuda.is_available()
+    from jaxmaterials_b200 import solver
+
+    return solver
+
+
+def oracle_fixed_iters(lm, mu, eb, g, iters):
+    """FP64 oracle run with exactly `iters` updates."""
+    return O.lippmann_schwinger(lm, mu, eb, g, rtol=0.0, atol=0.0, depth=0, maxiter=iters,
+                                dtype=np.float64)
+
+
+@pytest.mark.parametrize("tag,n", [("even", (12, 10, 8)), ("odd", (11, 9, 7)),
+                                   ("prime", (37, 47, 61)), ("mixed", (48, 20, 30)),
+                                   ("line", (1, 1, 16)), ("flat", (16, 8, 1))])
+def test_fields_match_oracle(ls, tag, n):
+    from jaxmaterials_b200 import GridSpec
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    eps, sig, it = ls.lippmann_schwinger(lm, mu, EPS_BAR, g, rtol=1e-20, atol=1e-5, maxiter=32)
+    og = O.Grid(*n, *EXT)
+    e64, s64, it64 = oracle_fixed_iters(lm, mu, EPS_BAR, og, it)
+    assert it64 == it
+    assert relmax(eps, e64) < 2e-5
+    assert relmax(sig, s64) < 2e-5
+    # the mean strain is preserved exactly up to round-off (Gamma^0 kills the zero mode)
+    assert relmax(eps.mean(axis=(1, 2, 3)), EPS_BAR) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_golden_small(ls, golden, tag):
+    from jaxmaterials_b200 import GridSpec
+
+    n = {"even": (12, 10, 8), "odd": (11, 9, 7)}[tag]
+    g = GridSpec(*n, *EXT)
+    eps, sig, it = ls.lippmann_schwinger(golden[f"ls_lambda_{tag}"], golden[f"ls_mu_{tag}"],
+                                         EPS_BAR, g, rtol=1e-20, atol=1e-5, maxiter=32)
+    key = f"ls_{tag}_f32_d0"
+    assert abs(it - int(golden[key + "_iter"])) <= 1
+    assert relmax(eps, golden[key + "_eps"]) < 2e-5
+    assert relmax(sig, golden[key + "_sigma"]) < 2e-5
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_reference_convergence_suite(ls, golden, tag):
+    """tests/test_lippmann_schwinger.py:64-99 (FP32, depth 0) on the CUDA path."""
+    from jaxmaterials_b200 import GridSpec
+
+    n = PY_SIZES[tag]
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    _, sig, it = ls.lippmann_schwinger(lm, mu, EPS_BAR, g, rtol=1e-20, atol=1e-5, maxiter=32)
+    assert it < 8
+    assert O.relative_divergence(sig.astype(np.float64), O.Grid(*n, *EXT)) < 1e-5
+    assert abs(it - int(golden[f"big_{tag}_f32_d0_iter"])) <= 1
+    assert relmax(sig.astype(np.float64).mean(axis=(1, 2, 3)),
+                  golden[f"big_{tag}_f32_d0_sigma_mean"]) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_homogeneous_zero_iterations(ls, tag):
+    """cuda/src/tests/test_lippmann_schwinger.hh:104-128 through the reference C signature."""
+    from jaxmaterials_b200 import GridSpec
+
+    g = GridSpec(*CU_SIZES[tag], *CU_EXT)
+    lm = np.full(g.shape, 1.2, np.float32)
+    eb = np.array([1.0, 0.4, 0.3, 0.1, -0.4, 0.7], np.float32)
+    eps, sig, it = ls.lippmann_schwinger_cuda(lm, lm, eb, g, rtol=1e-20, atol=1e-4, maxiter=100)
+    assert it == 0
+    assert relmax(eps, np.broadcast_to(eb[:, None, None, None], eps.shape)) < 1e-6
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_cuda_suite_convergence(ls, tag):
+    """cuda/src/tests/test_lippmann_schwinger.hh:132-180."""
+    from jaxmaterials_b200 import GridSpec
+
+    g = GridSpec(*CU_SIZES[tag], *CU_EXT)
+    rng = np.random.default_rng(1)
+    mu = rng.uniform(0.8, 0.9, size=g.shape).astype(np.float32)
+    lm = rng.uniform(0.8, 0.9, size=g.shape).astype(np.float32)
+    eb = np.array([1.0, 0.4, 0.3, 0.1, -0.4, 0.7], np.float32)
+    _, sig, it = ls.lippmann_schwinger_cuda(lm, mu, eb, g, rtol=1e-20, atol=1e-4, maxiter=100)
+    og = O.Grid(*CU_SIZES[tag], *CU_EXT)
+    div = np.sqrt(np.sum(O.backward_divergence(sig.astype(np.float64), og) ** 2))
+    avg = sig.astype(np.float64).mean(axis=(1, 2, 3))
+    assert it < 10
+    assert div / np.sqrt(np.sum(avg[:3] ** 2) + 2 * np.sum(avg[3:] ** 2)) < 1e-2
+
+
+def test_lambda_mu_order(ls):
+    """lambda is the FIRST argument of the C signature; the result differs if swapped."""
+    from jaxmaterials_b200 import GridSpec
+
+    n = (16, 12, 10)
+    g = GridSpec(*n, *EXT)
+    rng = np.random.default_rng(4)
+    lm = rng.uniform(0.5, 3.0, size=n).astype(np.float32)
+    mu = rng.uniform(0.5, 1.0, size=n).astype(np.float32)
+    eps, sig, it = ls.lippmann_schwinger_cuda(lm, mu, EPS_BAR, g, rtol=1e-6, atol=1e-20, maxiter=500)
+    e64, s64, it64 = oracle_fixed_iters(lm, mu, EPS_BAR, O.Grid(*n, *EXT), it)
+    assert relmax(sig, s64) < 2e-5
+    e_sw, s_sw, _ = oracle_fixed_iters(mu, lm, EPS_BAR, O.Grid(*n, *EXT), it)
+    assert relmax(sig, s_sw) > 1e-2
+
+
+def test_ceff_config1_vs_fp64_oracle(ls):
+    """Config-1 workload: 32^3 cross-ply, contrast ~26, tol 1e-6, six unit loads."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+
+    st = fibres.config_structure("c1", seed=0)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(32, 32, 32, 32.0, 32.0, 32.0)
+    c, its, _ = ls.c_eff(lm, mu, g, rtol=1e-6, atol=1e-20, maxiter=2000)
+    c64, its64 = O.c_eff(lm.astype(np.float64), mu.astype(np.float64), O.Grid(32, 32, 32, 32.0, 32.0, 32.0),
+                         rtol=1e-6, atol=1e-20, maxiter=2000)
+    err = np.linalg.norm(c - c64) / np.linalg.norm(c64)
+    assert err < 1e-5, err
+    assert np.all(np.abs(np.array(its) - np.array(its64)) <= 2), (its, its64)
+    # symmetry of the engineering-shear stiffness S^-1 C (size-independent property)
+    s = np.array([1, 1, 1, 2, 2, 2], float)
+    ce = c / s[:, None]
+    assert np.abs(ce - ce.T).max() / np.abs(ce).max() < 1e-5
+
+
+def test_golden_fibre_ceff(ls, golden):
+    from jaxmaterials_b200 import GridSpec
+
+    g = GridSpec(16, 16, 16, 16.0, 16.0, 16.0)
+    c, its, _ = ls.c_eff(golden["fib_lambda"], golden["fib_mu"], g, rtol=1e-6, atol=1e-20, maxiter=1000)
+    ref = golden["fib_d0_ceff"]
+    assert np.linalg.norm(c - ref) / np.linalg.norm(ref) < 1e-5
+    assert np.all(np.abs(its - golden["fib_d0_iters"]) <= 2)
+
+
+def test_linearity_and_batch(ls):
+    """Size-independent properties at 128^3: the solution is linear in eps_bar and a
+    batch of instances equals separate solves."""
+    import torch
+
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+
+    st = fibres.generate_layered_fibres(128, 4, 4.0, 0.45, seed=3)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(128, 128, 128, 128.0, 128.0, 128.0)
+    s = ls.Solver(g, batch=3)
+    ebs = np.zeros((3, 6), np.float32)
+    ebs[0, 0] = 1.0
+    ebs[1, 3] = 1.0
+    ebs[2] = 0.5 * ebs[0] - 2.0 * ebs[1]
+    r = s.solve(lm, mu, ebs, rtol=1e-6, atol=1e-20, maxiter=3000)
+    assert np.all(r.status == ls.CONVERGED)
+    comb = 0.5 * r.epsilon[0] - 2.0 * r.epsilon[1]
+    d = (comb - r.epsilon[2]).abs().max().item() / r.epsilon[2].abs().max().item()
+    assert d < 1e-4
+    r1 = s.solve(lm, mu, ebs[1:2], rtol=1e-6, atol=1e-20, maxiter=3000)
+    assert r1.iters[0] == r.iters[1]
+    assert torch.equal(r1.epsilon[0], r.epsilon[1])  # deterministic, batch-independent
+    # real-space criterion of the converged stress agrees with the Fourier one
+    e_real = O.relative_divergence(r.sigma[0].cpu().numpy().astype(np.float64),
+                                   O.Grid(128, 128, 128, 128.0, 128.0, 128.0))
+    assert abs(e_real / r.residual[0] - 1) < 1e-2
+    s.close()
+
+
+def _reference_cuda():
+    path = os.path.join(ROOT, "oracle", "_ref", "liblippmannschwinger.so")
+    if not os.path.exists(path):
+        pytest.skip("reference CUDA library not built (make -C oracle)")
+    lib = ctypes.CDLL(path)
+    f = lib.lippmann_schwinger_solve
+    fp = ctypes.POINTER(ctypes.c_float)
+    f.argtypes = [fp, fp, fp, fp, fp, ctypes.POINTER(ctypes.c_int), fp, ctypes.c_float,
+                  ctypes.c_float, ctypes.c_int, ctypes.c_int]
+    f.restype = ctypes.c_int
+    return f
+
+
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_matches_reference_cuda_library(ls, tag):
+    """Same inputs through the reference library (built from its sources, lambda first)
+    and through ours."""
+    from jaxmaterials_b200 import GridSpec
+
+    ref = _reference_cuda()
+    n = CU_SIZES[tag]
+    g = GridSpec(*n, *CU_EXT)
+    lm, mu = reference_material(n)
+    lm = lm.astype(np.float32)
+    mu = mu.astype(np.float32)
+    eb = np.array([1.0, 0.4, 0.3, 0.1, -0.4, 0.7], np.float32)
+    fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    e_ref = np.empty((6,) + n, np.float32)
+    s_ref = np.empty((6,) + n, np.float32)
+    vox = np.array(n, np.int32)
+    ext = np.array(CU_EXT, np.float32)
+    it_ref = ref(fp(lm), fp(mu), fp(eb), fp(e_ref), fp(s_ref),
+                 vox.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), fp(ext), 1e-20, 1e-4, 100, 0)
+    eps, sig, it = ls.lippmann_schwinger_cuda(lm, mu, eb, g, rtol=1e-20, atol=1e-4, maxiter=100)
+    assert abs(it - it_ref) <= 1
+    assert relmax(eps, e_ref) < 1e-4
