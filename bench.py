@@ -240,14 +240,14 @@ def own_arm(args):
     eye = np.eye(6, dtype=np.float32)
     s = Solver(g, batch=6, depth=args.depth)
     stream = torch.cuda.current_stream(dev)
-    maxiter = 20000
+    maxiter = 5000
 
     def step(lm_t, mu_t):
         return s.solve(lm_t, mu_t, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
 
     for _ in range(max(args.warmup, 3)):
         r = step(lm_d, mu_d)
-    assert np.all(r.status == CONVERGED), r.status
+    converged = bool(np.all(r.status == CONVERGED))
 
     def barrier():
         if world > 1:
@@ -340,6 +340,7 @@ def own_arm(args):
             "config": config_dict(st, args.depth),
             "voxel_iter_per_s": vips,
             "iters_per_solve": float(iters_total) / (6 * args.steps),
+            "all_converged": converged,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "gpu_launches": int(launches),
             "roofline": {

@@ -8,7 +8,9 @@
  *   - fields are float32, C order, z fastest: Lame fields [nx][ny][nz]; strain and
  *     stress [6][nx][ny][nz] in Voigt order (xx, yy, zz, xy, xz, yz) with TENSOR shear
  *     entries (eps_xy, not gamma_xy = 2 eps_xy);
- *   - voxels = (nx, ny, nz), extents = (Lx, Ly, Lz) (cuda/src/common.hh:73-91);
+ *   - voxels = (nx, ny, nz), extents = (Lx, Ly, Lz) (cuda/src/common.hh:73-91); the
+ *     reference signature takes float extents, the handle API double extents (FP64
+ *     runs resolve the grid spacing to FP64);
  *   - the criterion is e = sqrt(<|div sigma|^2>) / |<sigma>| evaluated in Fourier space
  *     (cuda/src/lippmann_schwinger.hh:76-89) and the loop stops when
  *     e < max(rtol * e0, atol), e0 being e at the first iterate.
@@ -30,7 +32,9 @@ extern "C" {
  * epsilon, sigma: caller-allocated host float[6*nx*ny*nz], overwritten with the
  *               solution and sigma = C : epsilon
  * Returns the number of updates performed; == maxiter means "not converged", as in the
- * reference. Negative on error (the reference only printed errors). Device buffers are
+ * reference. Negative on error (the reference only printed errors). Runs in
+ * LSB_PREC_MIXED precision, so the tolerance is met even where FP32 round-off alone
+ * would stall above it. Device buffers are
  * cached between calls with the same grid on the same device; see
  * lippmann_schwinger_release(). */
 int lippmann_schwinger_solve(float *lambda, float *mu, float *epsilon_bar,
@@ -51,8 +55,17 @@ typedef struct lsb_solver lsb_solver;
 enum {
   LSB_CONVERGED = 1,
   LSB_MAXITER = 2,
-  LSB_NONFINITE = 3
+  LSB_NONFINITE = 3,
+  LSB_STALLED = 4 /* FP32 round-off floor above the tolerance (LSB_PREC_FP32 only) */
 };
+
+/* Field precision of the iteration (norms and the stop decision are always FP64):
+ * LSB_PREC_FP32   FP32 fields and FFTs; a solve whose criterion stalls on FP32
+ *                 round-off above the tolerance ends with LSB_STALLED;
+ * LSB_PREC_MIXED  FP32 fields until the criterion stalls near the tolerance, then the
+ *                 stalled instances continue from their iterate with FP64 fields (default);
+ * LSB_PREC_FP64   FP64 fields from the start. */
+enum { LSB_PREC_FP32 = 0, LSB_PREC_MIXED = 1, LSB_PREC_FP64 = 2 };
 
 /* Stop rules: LSB_RULE_CUDA stops when e < max(rtol e0, atol)
  * (cuda/src/lippmann_schwinger.cu:205); LSB_RULE_JAX when e <= max(rtol e0, atol)
@@ -61,11 +74,16 @@ enum { LSB_RULE_CUDA = 0, LSB_RULE_JAX = 1 };
 
 /* Creates a solver for voxels/extents with room for `batch` instances and Anderson
  * depth `depth` (0 = plain Moulinec-Suquet iteration) on the current CUDA device. */
-int lsb_create(lsb_solver **out, const int voxels[3], const float extents[3], int batch,
+int lsb_create(lsb_solver **out, const int voxels[3], const double extents[3], int batch,
                int depth);
 void lsb_destroy(lsb_solver *solver);
 /* Stream (cudaStream_t passed as void*) for all later work; NULL = legacy default. */
 int lsb_set_stream(lsb_solver *solver, void *stream);
+
+/* Precision mode (LSB_PREC_*) and the stall window: the number of criterion evaluations
+ * without a 2% improvement, while the criterion is within 4x of the tolerance, after
+ * which FP32 round-off is taken to have stalled the iteration (default 8; 0 disables). */
+int lsb_set_precision(lsb_solver *solver, int precision, int stall_window);
 
 /* Solves `batch` instances that share d_lambda, d_mu (device float[nv]).
  * eps_bar:   host float[batch*6]
@@ -79,6 +97,14 @@ int lsb_solve(lsb_solver *solver, int batch, const float *d_lambda, const float 
               const float *eps_bar, const float *d_eps0, float *d_eps, float *d_sigma,
               double *mean_sigma, float rtol, float atol, int maxiter, int rule,
               int *iters, int *status, double *residual);
+
+/* FP64 variant of lsb_solve (the reference's dtype=float64 path,
+ * src/jaxmaterials/solver/lippmann_schwinger.py:146-265): FP64 Lame fields, strain,
+ * stress and FFTs on the device; eps_bar host double[batch*6]. */
+int lsb_solve_f64(lsb_solver *solver, int batch, const double *d_lambda, const double *d_mu,
+                  const double *eps_bar, const double *d_eps0, double *d_eps, double *d_sigma,
+                  double *mean_sigma, double rtol, double atol, int maxiter, int rule,
+                  int *iters, int *status, double *residual);
 
 /* Criterion history of the last solve: host double[batch*len], e after every
  * evaluation (0 for evaluations that did not happen). len <= maxiter + 1. */
@@ -99,7 +125,7 @@ int lsb_profile_passes(lsb_solver *solver, int batch, const float *d_lambda,
  * src/jaxmaterials/data/data.py:178-186): row k of c_eff (host double[36]) is the mean
  * stress for eps_bar = e_k. Host lambda/mu float[nv]; iters host int[6]. */
 int lsb_c_eff(const float *lambda, const float *mu, const int voxels[3],
-              const float extents[3], float rtol, float atol, int maxiter, int depth,
+              const double extents[3], float rtol, float atol, int maxiter, int depth,
               double *c_eff, int *iters);
 
 /* Message of the last error on this thread ("" if none). */

@@ -27,7 +27,7 @@ SIGNATURES = {
                                                 c_float_p, c_int_p, c_float_p, ctypes.c_float,
                                                 ctypes.c_float, ctypes.c_int, ctypes.c_int]),
     "lippmann_schwinger_release": (None, []),
-    "lsb_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), c_int_p, c_float_p, ctypes.c_int,
+    "lsb_create": (ctypes.c_int, [ctypes.POINTER(c_void_p), c_int_p, c_double_p, ctypes.c_int,
                                   ctypes.c_int]),
     "lsb_destroy": (None, [c_void_p]),
     "lsb_set_stream": (ctypes.c_int, [c_void_p, c_void_p]),
@@ -35,11 +35,16 @@ SIGNATURES = {
                                  c_void_p, c_void_p, c_void_p, c_double_p, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
                                  c_double_p]),
+    "lsb_set_precision": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lsb_solve_f64": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_double_p,
+                                     c_void_p, c_void_p, c_void_p, c_double_p, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int, ctypes.c_int, c_int_p,
+                                     c_int_p, c_double_p]),
     "lsb_history": (ctypes.c_int, [c_void_p, c_double_p, ctypes.c_int]),
     "lsb_kernel_launches": (ctypes.c_longlong, [c_void_p]),
     "lsb_profile_passes": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p,
                                           ctypes.c_int, c_float_p]),
-    "lsb_c_eff": (ctypes.c_int, [c_float_p, c_float_p, c_int_p, c_float_p, ctypes.c_float,
+    "lsb_c_eff": (ctypes.c_int, [c_float_p, c_float_p, c_int_p, c_double_p, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_int, ctypes.c_int, c_double_p,
                                  c_int_p]),
     "lsb_last_error": (ctypes.c_char_p, []),

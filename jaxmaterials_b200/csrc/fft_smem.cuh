@@ -1,4 +1,5 @@
-// Block-cooperative mixed-radix FFTs on lines held in shared memory.
+// Block-cooperative mixed-radix FFTs on lines held in shared memory, for float2 or
+// double2 complex values.
 //
 // A "line set" is nlines complex lines of length n at buf[line * ls + e * es].
 // All threads of the block call fft_lines() together (it contains __syncthreads()).
@@ -21,23 +22,33 @@
 
 namespace lsb {
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <typename C>
+__device__ __forceinline__ C mk(decltype(C::x) x, decltype(C::x) y) {
+  C r;
+  r.x = x;
+  r.y = y;
+  return r;
 }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
 // multiply by -i
-__device__ __forceinline__ float2 cmul_mi(float2 a) { return make_float2(a.y, -a.x); }
+template <typename C>
+__device__ __forceinline__ C cmul_mi(C a) { return mk<C>(a.y, -a.x); }
 
 template <int R>
 struct Bfly;
 
 template <>
 struct Bfly<2> {
-  static __device__ __forceinline__ void run(float2* v) {
-    float2 a = v[0], b = v[1];
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   }
@@ -45,9 +56,10 @@ struct Bfly<2> {
 
 template <>
 struct Bfly<4> {
-  static __device__ __forceinline__ void run(float2* v) {
-    float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-    float2 t2 = cadd(v[1], v[3]), t3 = cmul_mi(csub(v[1], v[3]));
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), t3 = cmul_mi(csub(v[1], v[3]));
     v[0] = cadd(t0, t2);
     v[2] = csub(t0, t2);
     v[1] = cadd(t1, t3);
@@ -57,16 +69,18 @@ struct Bfly<4> {
 
 template <>
 struct Bfly<8> {
-  static __device__ __forceinline__ void run(float2* v) {
-    const float h = 0.70710678118654752440f;
-    float2 e[4] = {v[0], v[2], v[4], v[6]};
-    float2 o[4] = {v[1], v[3], v[5], v[7]};
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(C::x);
+    const R h = (R)0.70710678118654752440;
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
     Bfly<4>::run(e);
     Bfly<4>::run(o);
     // o[k] *= exp(-2 pi i k / 8)
-    o[1] = make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    o[1] = mk<C>(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
     o[2] = cmul_mi(o[2]);
-    o[3] = make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    o[3] = mk<C>(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       v[k] = cadd(e[k], o[k]);
@@ -77,12 +91,14 @@ struct Bfly<8> {
 
 template <>
 struct Bfly<3> {
-  static __device__ __forceinline__ void run(float2* v) {
-    const float s = 0.86602540378443864676f;  // sin(2 pi / 3)
-    float2 b = cadd(v[1], v[2]);
-    float2 d = csub(v[1], v[2]);
-    float2 t = make_float2(v[0].x - 0.5f * b.x, v[0].y - 0.5f * b.y);
-    float2 u = make_float2(s * d.y, -s * d.x);  // -i s d
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(C::x);
+    const R s = (R)0.86602540378443864676;  // sin(2 pi / 3)
+    C b = cadd(v[1], v[2]);
+    C d = csub(v[1], v[2]);
+    C t = mk<C>(v[0].x - (R)0.5 * b.x, v[0].y - (R)0.5 * b.y);
+    C u = mk<C>(s * d.y, -s * d.x);  // -i s d
     v[0] = cadd(v[0], b);
     v[1] = cadd(t, u);
     v[2] = csub(t, u);
@@ -91,19 +107,21 @@ struct Bfly<3> {
 
 template <>
 struct Bfly<5> {
-  static __device__ __forceinline__ void run(float2* v) {
-    const float c1 = 0.30901699437494742410f;   // cos(2 pi/5)
-    const float c2 = -0.80901699437494742410f;  // cos(4 pi/5)
-    const float s1 = 0.95105651629515357212f;   // sin(2 pi/5)
-    const float s2 = 0.58778525229247312917f;   // sin(4 pi/5)
-    float2 b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
-    float2 d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
-    float2 a0 = v[0];
-    float2 p1 = make_float2(a0.x + c1 * b1.x + c2 * b2.x, a0.y + c1 * b1.y + c2 * b2.y);
-    float2 p2 = make_float2(a0.x + c2 * b1.x + c1 * b2.x, a0.y + c2 * b1.y + c1 * b2.y);
-    float2 q1 = make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
-    float2 q2 = make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
-    v[0] = make_float2(a0.x + b1.x + b2.x, a0.y + b1.y + b2.y);
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(C::x);
+    const R c1 = (R)0.30901699437494742410;   // cos(2 pi/5)
+    const R c2 = (R)-0.80901699437494742410;  // cos(4 pi/5)
+    const R s1 = (R)0.95105651629515357212;   // sin(2 pi/5)
+    const R s2 = (R)0.58778525229247312917;   // sin(4 pi/5)
+    C b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+    C d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+    C a0 = v[0];
+    C p1 = mk<C>(a0.x + c1 * b1.x + c2 * b2.x, a0.y + c1 * b1.y + c2 * b2.y);
+    C p2 = mk<C>(a0.x + c2 * b1.x + c1 * b2.x, a0.y + c2 * b1.y + c1 * b2.y);
+    C q1 = mk<C>(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
+    C q2 = mk<C>(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
+    v[0] = mk<C>(a0.x + b1.x + b2.x, a0.y + b1.y + b2.y);
     v[1] = cadd(p1, cmul_mi(q1));
     v[4] = csub(p1, cmul_mi(q1));
     v[2] = cadd(p2, cmul_mi(q2));
@@ -112,15 +130,15 @@ struct Bfly<5> {
 };
 
 // One Stockham stage with an unrolled radix-R butterfly.
-template <int R, int VPT, bool LF>
-__device__ __forceinline__ void stage_bfly(float2* buf, int nlines, int es, int ls, int n, int Ns,
-                                           const float2* __restrict__ tw) {
+template <int R, int VPT, bool LF, typename C>
+__device__ __forceinline__ void stage_bfly(C* buf, int nlines, int es, int ls, int n, int Ns,
+                                           const C* __restrict__ tw) {
   constexpr int IT = VPT / R > 0 ? VPT / R : 1;
   const int nb = n / R;
   const int total = nlines * nb;
   const int tws = n / (Ns * R);
   const int tid = threadIdx.x, nt = blockDim.x;
-  float2 v[IT][R];
+  C v[IT][R];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
     int w = tid + it * nt;
@@ -128,12 +146,12 @@ __device__ __forceinline__ void stage_bfly(float2* buf, int nlines, int es, int 
       int line, j;
       if (LF) { j = w / nlines; line = w - j * nlines; } else { line = w / nb; j = w - line * nb; }
       int k = j % Ns;
-      const float2* L = buf + (size_t)line * ls;
+      const C* L = buf + (size_t)line * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) v[it][r] = L[(j + r * nb) * es];
       if (Ns > 1) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[it][r] = cmul(v[it][r], __ldg(tw + k * r * tws));
+        for (int r = 1; r < R; ++r) v[it][r] = cmul(v[it][r], tw[k * r * tws]);
       }
       Bfly<R>::run(v[it]);
     }
@@ -147,7 +165,7 @@ __device__ __forceinline__ void stage_bfly(float2* buf, int nlines, int es, int 
       if (LF) { j = w / nlines; line = w - j * nlines; } else { line = w / nb; j = w - line * nb; }
       int k = j % Ns;
       int base = (j / Ns) * Ns * R + k;
-      float2* L = buf + (size_t)line * ls;
+      C* L = buf + (size_t)line * ls;
 #pragma unroll
       for (int r = 0; r < R; ++r) L[(base + r * Ns) * es] = v[it][r];
     }
@@ -156,14 +174,14 @@ __device__ __forceinline__ void stage_bfly(float2* buf, int nlines, int es, int 
 }
 
 // One Stockham stage of arbitrary radix R: each work item produces one output.
-template <int VPT, bool LF>
-__device__ __forceinline__ void stage_generic(float2* buf, int nlines, int es, int ls, int n, int Ns,
-                                              int R, const float2* __restrict__ tw) {
+template <int VPT, bool LF, typename C>
+__device__ __forceinline__ void stage_generic(C* buf, int nlines, int es, int ls, int n, int Ns,
+                                              int R, const C* __restrict__ tw) {
   const int nb = n / R;
   const int total = nlines * n;
   const int tws = n / (Ns * R);
   const int tid = threadIdx.x, nt = blockDim.x;
-  float2 o[VPT];
+  C o[VPT];
 #pragma unroll
   for (int it = 0; it < VPT; ++it) {
     int w = tid + it * nt;
@@ -173,14 +191,14 @@ __device__ __forceinline__ void stage_generic(float2* buf, int nlines, int es, i
       int k = e % Ns;
       int q = (e / Ns) % R;
       int j = (e / (Ns * R)) * Ns + k;
-      const float2* L = buf + (size_t)line * ls;
-      float2 acc = make_float2(0.f, 0.f);
+      const C* L = buf + (size_t)line * ls;
+      C acc = mk<C>(0, 0);
       int rq = 0;  // (r * q) mod R
       for (int r = 0; r < R; ++r) {
-        float2 x = L[(j + r * nb) * es];
-        if (r > 0) x = cmul(x, __ldg(tw + k * r * tws));
-        float2 wv = __ldg(tw + rq * nb);
-        acc = make_float2(acc.x + x.x * wv.x - x.y * wv.y, acc.y + x.x * wv.y + x.y * wv.x);
+        C x = L[(j + r * nb) * es];
+        if (r > 0) x = cmul(x, tw[k * r * tws]);
+        C wv = tw[rq * nb];
+        acc = mk<C>(acc.x + x.x * wv.x - x.y * wv.y, acc.y + x.x * wv.y + x.y * wv.x);
         rq += q;
         if (rq >= R) rq -= R;
       }
@@ -200,19 +218,20 @@ __device__ __forceinline__ void stage_generic(float2* buf, int nlines, int es, i
   __syncthreads();
 }
 
-// Forward (exp(-i...)) unnormalised FFT of every line in the set.
-template <int VPT, bool LF>
-__device__ void fft_lines(float2* buf, int nlines, int es, int ls, const Plan1D& p) {
+// Forward (exp(-i...)) unnormalised FFT of every line in the set; tw = twiddle table of
+// the plan in the precision of C.
+template <int VPT, bool LF, typename C>
+__device__ void fft_lines(C* buf, int nlines, int es, int ls, const Plan1D& p, const C* tw) {
   int Ns = 1;
   for (int s = 0; s < p.nst; ++s) {
     const int R = p.radix[s];
     switch (R) {
-      case 2: stage_bfly<2, VPT, LF>(buf, nlines, es, ls, p.n, Ns, p.tw); break;
-      case 3: stage_bfly<3, VPT, LF>(buf, nlines, es, ls, p.n, Ns, p.tw); break;
-      case 4: stage_bfly<4, VPT, LF>(buf, nlines, es, ls, p.n, Ns, p.tw); break;
-      case 5: stage_bfly<5, VPT, LF>(buf, nlines, es, ls, p.n, Ns, p.tw); break;
-      case 8: stage_bfly<8, VPT, LF>(buf, nlines, es, ls, p.n, Ns, p.tw); break;
-      default: stage_generic<VPT, LF>(buf, nlines, es, ls, p.n, Ns, R, p.tw); break;
+      case 2: stage_bfly<2, VPT, LF>(buf, nlines, es, ls, p.n, Ns, tw); break;
+      case 3: stage_bfly<3, VPT, LF>(buf, nlines, es, ls, p.n, Ns, tw); break;
+      case 4: stage_bfly<4, VPT, LF>(buf, nlines, es, ls, p.n, Ns, tw); break;
+      case 5: stage_bfly<5, VPT, LF>(buf, nlines, es, ls, p.n, Ns, tw); break;
+      case 8: stage_bfly<8, VPT, LF>(buf, nlines, es, ls, p.n, Ns, tw); break;
+      default: stage_generic<VPT, LF>(buf, nlines, es, ls, p.n, Ns, R, tw); break;
     }
     Ns *= R;
   }
@@ -224,10 +243,8 @@ __host__ inline int threads_for(const Plan1D& p, long long n_elems, int vpt) {
   long long need = 32;
   for (int s = 0; s < p.nst; ++s) {
     int R = p.radix[s];
-    long long per;
     if (R == 2 || R == 3 || R == 4 || R == 5 || R == 8) {
-      long long it = vpt / R > 0 ? vpt / R : 1;
-      per = it;  // butterflies per thread
+      long long per = vpt / R > 0 ? vpt / R : 1;  // butterflies per thread
       long long nb = n_elems / R;
       long long t = (nb + per - 1) / per;
       if (t > need) need = t;

@@ -6,13 +6,14 @@
 //
 //   xpass    forward x-DFT, FP64 equilibrium-residual partials and the zero mode,
 //            r_hat = -Gamma^0 sigma_hat in registers, inverse x-DFT      (per ky, kz tile)
-//   finalize criterion e, stop decision, iteration count               (one block / instance)
+//   finalize criterion e, stop / stall decision, iteration count       (one block / instance)
 //   ypass    inverse y-DFT                                              (per x, kz tile)
 //   zpass    z-C2R, eps += r / N, sigma = lambda tr(eps) I + 2 mu eps, z-R2C (per z line)
 //   ypass    forward y-DFT
 //
-// The stop decision lives on the device: every kernel of an instance returns at once
-// after `done` is set, so the host can enqueue many iterations without reading back.
+// Every pass exists for FP32 fields (T = float) and FP64 fields (T = double). An
+// instance is processed by the passes of its current phase (0: FP32, 1: FP64) until it
+// is done, so the host can enqueue many iterations without reading anything back.
 #include <cfloat>
 #include <cmath>
 
@@ -21,29 +22,40 @@
 
 namespace lsb {
 
+template <typename T>
+__device__ __forceinline__ bool active(const InstanceState& s) {
+  return !s.done && s.phase == (sizeof(T) == 8 ? 1 : 0);
+}
+
 // ----------------------------------------------------------------------------- z pass
 // Lines l = x * ny + y; pair p of components (2p, 2p+1) shares one complex line
 // z = a + i b (two real transforms for the price of one complex transform).
-template <int VPT>
+// mode 0: eps = eps_bar (or eps0); mode 1: eps += r / N with r from the spectrum;
+// mode 2: keep eps (continuation of an instance in another precision).
+template <typename T, int VPT>
 __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode, int L,
-                                                     const float* __restrict__ lambda,
-                                                     const float* __restrict__ mu,
-                                                     float* __restrict__ eps,
-                                                     float2* __restrict__ spec,
-                                                     const float* __restrict__ eps_bar,
-                                                     const float* __restrict__ eps0,
-                                                     const InstanceState* __restrict__ st,
-                                                     SolveParams sp) {
-  extern __shared__ float2 zbuf[];
+                                                     const T* __restrict__ lambda,
+                                                     const T* __restrict__ mu,
+                                                     T* __restrict__ eps,
+                                                     cplx<T>* __restrict__ spec,
+                                                     const double* __restrict__ eps_bar,
+                                                     const T* __restrict__ eps0,
+                                                     InstanceState* __restrict__ st,
+                                                     const Medium* __restrict__ med) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char zraw[];
+  C* zbuf = reinterpret_cast<C*>(zraw);
   const int b = blockIdx.y;
-  if (mode == 1 && st[b].done) return;
+  if (!active<T>(st[b])) return;
   const int nz = g.nz, nzh = g.nzh;
   const long long nlines = (long long)g.nx * g.ny;
   const long long l0 = (long long)blockIdx.x * L;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int ldz = nz;
-  float* eb = eps + (size_t)b * 6 * g.nv;
-  float2* sb = spec + (size_t)b * 6 * g.nm;
+  T* eb = eps + (size_t)b * 6 * g.nv;
+  C* sb = spec + (size_t)b * 6 * g.nm;
+  const Plan1D& pz = g.pz;
+  const C* tw = twiddles<T>(pz);
 
   if (mode == 1) {
     // Build conj(Z) with Z[k] = A[k] + i B[k] on the full line (Hermitian extension);
@@ -55,172 +67,200 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
       int l = rem / nzh, k = rem - l * nzh;
       long long line = l0 + l;
       if (line >= nlines) continue;
-      float2 A = sb[((size_t)(2 * p) * nlines + line) * nzh + k];
-      float2 B = sb[((size_t)(2 * p + 1) * nlines + line) * nzh + k];
+      C A = sb[((size_t)(2 * p) * nlines + line) * nzh + k];
+      C B = sb[((size_t)(2 * p + 1) * nlines + line) * nzh + k];
       const bool selfconj = (k == 0) || (2 * k == nz);
-      if (selfconj) { A.y = 0.f; B.y = 0.f; }
-      float2* Z = zbuf + (size_t)(p * L + l) * ldz;
-      Z[k] = make_float2(A.x - B.y, -(A.y + B.x));
-      if (!selfconj) Z[nz - k] = make_float2(A.x + B.y, A.y - B.x);
+      if (selfconj) { A.y = 0; B.y = 0; }
+      C* Z = zbuf + (size_t)(p * L + l) * ldz;
+      Z[k] = mk<C>(A.x - B.y, -(A.y + B.x));
+      if (!selfconj) Z[nz - k] = mk<C>(A.x + B.y, A.y - B.x);
     }
     __syncthreads();
-    fft_lines<VPT, false>(zbuf, 3 * L, 1, ldz, g.pz);
+    fft_lines<VPT, false>(zbuf, 3 * L, 1, ldz, pz, tw);
+  }
+
+  // Shift of the forward transform: the current mean-stress estimate (see InstanceState).
+  T shift[6];
+  if (mode != 0) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) shift[c] = (T)st[b].shift[c];
+  } else {
+    // <sigma(eps_bar)> = <lambda> tr(eps_bar) I + 2 <mu> eps_bar
+    const double* e = eps_bar + 6 * b;
+    const double tr = e[0] + e[1] + e[2];
+    double sh[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) sh[c] = (c < 3 ? med->lmean * tr : 0.0) + 2.0 * med->mmean * e[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) shift[c] = (T)sh[c];
+    if (blockIdx.x == 0 && tid == 0) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) st[b].shift[c] = (double)shift[c];
+    }
   }
 
   // Pointwise stage: update the strain, evaluate the stress, pack pairs for the R2C.
   {
     const int work = L * nz;
-    const float inv_nv = sp.inv_nv;
+    const T inv_nv = (T)(1.0 / (double)g.nv);
     for (int idx = tid; idx < work; idx += nt) {
       int l = idx / nz, n = idx - l * nz;
       long long line = l0 + l;
       if (line >= nlines) continue;
       size_t v = (size_t)line * nz + n;
-      float e[6];
+      T e[6];
       if (mode == 1) {
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
-          float2 w = zbuf[(size_t)(p * L + l) * ldz + n];
+          C w = zbuf[(size_t)(p * L + l) * ldz + n];
           // z = conj(w): r_{2p} = Re z = w.x, r_{2p+1} = Im z = -w.y
           e[2 * p] = eb[(size_t)(2 * p) * g.nv + v] + w.x * inv_nv;
           e[2 * p + 1] = eb[(size_t)(2 * p + 1) * g.nv + v] - w.y * inv_nv;
         }
+      } else if (mode == 2) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * g.nv + v];
       } else if (eps0 != nullptr) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * g.nv + v];
       } else {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) e[c] = eps_bar[b * 6 + c];
+        for (int c = 0; c < 6; ++c) e[c] = (T)eps_bar[b * 6 + c];
       }
 #pragma unroll
       for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + v] = e[c];
-      const float lam = lambda[v], tmu = 2.f * mu[v];
-      const float ltr = lam * (e[0] + e[1] + e[2]);
-      float s[6];
+      const T lam = lambda[v], tmu = (T)2 * mu[v];
+      const T ltr = lam * (e[0] + e[1] + e[2]);
+      T s[6];
 #pragma unroll
       for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
 #pragma unroll
       for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
 #pragma unroll
       for (int p = 0; p < 3; ++p)
-        zbuf[(size_t)(p * L + l) * ldz + n] = make_float2(s[2 * p], s[2 * p + 1]);
+        zbuf[(size_t)(p * L + l) * ldz + n] =
+            mk<C>(s[2 * p] - shift[2 * p], s[2 * p + 1] - shift[2 * p + 1]);
     }
   }
   __syncthreads();
-  fft_lines<VPT, false>(zbuf, 3 * L, 1, ldz, g.pz);
+  fft_lines<VPT, false>(zbuf, 3 * L, 1, ldz, pz, tw);
 
   // Unpack the two real spectra: A = (Z[k] + conj Z[-k]) / 2, B = (Z[k] - conj Z[-k]) / 2i.
   {
     const int work = 3 * L * nzh;
+    const T h = (T)0.5;
     for (int idx = tid; idx < work; idx += nt) {
       int p = idx / (L * nzh);
       int rem = idx - p * L * nzh;
       int l = rem / nzh, k = rem - l * nzh;
       long long line = l0 + l;
       if (line >= nlines) continue;
-      const float2* Z = zbuf + (size_t)(p * L + l) * ldz;
-      float2 zk = Z[k];
-      float2 zm = Z[k == 0 ? 0 : nz - k];
-      float2 A = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-      float2 B = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-      sb[((size_t)(2 * p) * nlines + line) * nzh + k] = A;
-      sb[((size_t)(2 * p + 1) * nlines + line) * nzh + k] = B;
+      const C* Z = zbuf + (size_t)(p * L + l) * ldz;
+      C zk = Z[k];
+      C zm = Z[k == 0 ? 0 : nz - k];
+      sb[((size_t)(2 * p) * nlines + line) * nzh + k] = mk<C>(h * (zk.x + zm.x), h * (zk.y - zm.y));
+      sb[((size_t)(2 * p + 1) * nlines + line) * nzh + k] = mk<C>(h * (zk.y + zm.y), -h * (zk.x - zm.x));
     }
   }
 }
 
 // ----------------------------------------------------------------------------- y pass
-// Block = (kz tile, x, instance * 6 + component); smem holds ny rows of T columns.
-template <int VPT>
-__global__ void __launch_bounds__(kMaxThreads) ypass_kernel(GridDesc g, int inverse, int T,
-                                                     float2* __restrict__ spec,
+// Block = (kz tile, x, instance * 6 + component); smem holds ny rows of TT columns.
+template <typename T, int VPT>
+__global__ void __launch_bounds__(kMaxThreads) ypass_kernel(GridDesc g, int inverse, int TT,
+                                                     cplx<T>* __restrict__ spec,
                                                      const InstanceState* __restrict__ st) {
-  extern __shared__ float2 ybuf[];
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char yraw[];
+  C* ybuf = reinterpret_cast<C*>(yraw);
   const int bc = blockIdx.z;
   const int b = bc / 6;
-  if (st[b].done) return;
+  if (!active<T>(st[b])) return;
   const int x = blockIdx.y;
-  const int kz0 = blockIdx.x * T;
+  const int kz0 = blockIdx.x * TT;
   const int ny = g.ny, nzh = g.nzh;
   const int tid = threadIdx.x, nt = blockDim.x;
-  float2* base = spec + ((size_t)bc * g.nx + x) * (size_t)ny * nzh;
-  const int work = ny * T;
+  C* base = spec + ((size_t)bc * g.nx + x) * (size_t)ny * nzh;
+  const int work = ny * TT;
   for (int idx = tid; idx < work; idx += nt) {
-    int y = idx / T, t = idx - y * T;
+    int y = idx / TT, t = idx - y * TT;
     int kz = kz0 + t;
-    float2 v = make_float2(0.f, 0.f);
+    C v = mk<C>(0, 0);
     if (kz < nzh) v = base[(size_t)y * nzh + kz];
     if (inverse) v.y = -v.y;
     ybuf[idx] = v;
   }
   __syncthreads();
-  fft_lines<VPT, true>(ybuf, T, T, 1, g.py);
+  fft_lines<VPT, true>(ybuf, TT, TT, 1, g.py, twiddles<T>(g.py));
   for (int idx = tid; idx < work; idx += nt) {
-    int y = idx / T, t = idx - y * T;
+    int y = idx / TT, t = idx - y * TT;
     int kz = kz0 + t;
-    float2 v = ybuf[idx];
+    C v = ybuf[idx];
     if (inverse) v.y = -v.y;
     if (kz < nzh) base[(size_t)y * nzh + kz] = v;
   }
 }
 
 // ----------------------------------------------------------------------------- x pass
-// Block = (kz tile, ky, instance). Row kx of smem holds the 6*T values
-// (component c, column t) at c*T + t.
-template <int VPT>
-__global__ void __launch_bounds__(kMaxThreads) xpass_kernel(GridDesc g, int T,
-                                                     float2* __restrict__ spec,
+// Block = (kz tile, ky, instance). Row kx of smem holds the 6*TT values
+// (component c, column t) at c*TT + t.
+template <typename T, int VPT>
+__global__ void __launch_bounds__(kMaxThreads) xpass_kernel(GridDesc g, int TT,
+                                                     cplx<T>* __restrict__ spec,
                                                      const Medium* __restrict__ med,
                                                      InstanceState* __restrict__ st,
                                                      double* __restrict__ partials) {
-  extern __shared__ float2 xbuf[];
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char xraw[];
+  C* xbuf = reinterpret_cast<C*>(xraw);
   __shared__ double red[32];
   const int b = blockIdx.z;
-  if (st[b].done) return;
+  if (!active<T>(st[b])) return;
   const int ky = blockIdx.y;
-  const int kz0 = blockIdx.x * T;
+  const int kz0 = blockIdx.x * TT;
   const int nx = g.nx, ny = g.ny, nzh = g.nzh;
   const int tid = threadIdx.x, nt = blockDim.x;
-  const int W = 6 * T;  // values per row
-  float2* sb = spec + (size_t)b * 6 * g.nm;
+  const int W = 6 * TT;  // values per row
+  C* sb = spec + (size_t)b * 6 * g.nm;
   const size_t cstride = (size_t)g.nm;               // component stride
   const size_t xstride = (size_t)ny * nzh;           // x stride
+  const C* tw = twiddles<T>(g.px);
 
   const int work = nx * W;
   for (int idx = tid; idx < work; idx += nt) {
     int kx = idx / W, q = idx - kx * W;
-    int c = q / T, t = q - c * T;
+    int c = q / TT, t = q - c * TT;
     int kz = kz0 + t;
-    float2 v = make_float2(0.f, 0.f);
+    C v = mk<C>(0, 0);
     if (kz < nzh) v = sb[c * cstride + kx * xstride + (size_t)ky * nzh + kz];
     xbuf[idx] = v;
   }
   __syncthreads();
-  fft_lines<VPT, true>(xbuf, W, W, 1, g.px);
+  fft_lines<VPT, true>(xbuf, W, W, 1, g.px, tw);
 
   // Residual partials, zero mode and Gamma^0 (written conjugated for the inverse DFT).
-  const float c_a = med->c_a, c_b = med->c_b;
+  const T c_a = medium_ca<T>(*med), c_b = medium_cb<T>(*med);
   const double sxs = 2.0 * g.nx / g.Lx, sys = 2.0 * g.ny / g.Ly, szs = 2.0 * g.nz / g.Lz;
   double acc = 0.0;
-  const int modes = nx * T;
+  const int modes = nx * TT;
   for (int idx = tid; idx < modes; idx += nt) {
-    int kx = idx / T, t = idx - kx * T;
+    int kx = idx / TT, t = idx - kx * TT;
     int kz = kz0 + t;
     if (kz >= nzh) continue;
-    float2* row = xbuf + (size_t)kx * W + t;
-    float2 s[6];
+    C* row = xbuf + (size_t)kx * W + t;
+    C s[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) s[c] = row[c * T];
+    for (int c = 0; c < 6; ++c) s[c] = row[c * TT];
     // modified wave vector tilde(xi) in FP64 (fourier.py:9-58 order of products)
     const double x0 = sxs * g.sx[kx] * g.cy[ky] * g.cz[kz];
     const double x1 = sys * g.cx[kx] * g.sy[ky] * g.cz[kz];
     const double x2 = szs * g.cx[kx] * g.cy[ky] * g.sz[kz];
-    // divergence xi . sigma_hat in FP32, weighted |.|^2 in FP64
+    // divergence xi . sigma_hat in the field precision, weighted |.|^2 in FP64
     {
-      const float f0 = (float)x0, f1 = (float)x1, f2 = (float)x2;
-      float2 d0 = make_float2(f0 * s[0].x + f1 * s[3].x + f2 * s[4].x, f0 * s[0].y + f1 * s[3].y + f2 * s[4].y);
-      float2 d1 = make_float2(f0 * s[3].x + f1 * s[1].x + f2 * s[5].x, f0 * s[3].y + f1 * s[1].y + f2 * s[5].y);
-      float2 d2 = make_float2(f0 * s[4].x + f1 * s[5].x + f2 * s[2].x, f0 * s[4].y + f1 * s[5].y + f2 * s[2].y);
+      const T f0 = (T)x0, f1 = (T)x1, f2 = (T)x2;
+      C d0 = mk<C>(f0 * s[0].x + f1 * s[3].x + f2 * s[4].x, f0 * s[0].y + f1 * s[3].y + f2 * s[4].y);
+      C d1 = mk<C>(f0 * s[3].x + f1 * s[1].x + f2 * s[5].x, f0 * s[3].y + f1 * s[1].y + f2 * s[5].y);
+      C d2 = mk<C>(f0 * s[4].x + f1 * s[5].x + f2 * s[2].x, f0 * s[4].y + f1 * s[5].y + f2 * s[2].y);
       double m2 = (double)d0.x * d0.x + (double)d0.y * d0.y + (double)d1.x * d1.x +
                   (double)d1.y * d1.y + (double)d2.x * d2.x + (double)d2.y * d2.y;
       const double w = (kz == 0 || 2 * kz == g.nz) ? 1.0 : 2.0;
@@ -229,53 +269,48 @@ __global__ void __launch_bounds__(kMaxThreads) xpass_kernel(GridDesc g, int T,
     if (kx == 0 && ky == 0 && kz == 0) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        st[b].sig0[2 * c] = s[c].x;
-        st[b].sig0[2 * c + 1] = s[c].y;
+        st[b].sig0[2 * c] = (double)s[c].x + (double)g.nv * st[b].shift[c];
+        st[b].sig0[2 * c + 1] = (double)s[c].y;
       }
     }
-    // normalised wave vector (fourier.py:61-85): FP64 with the 1e-12 guard, then FP32
+    // normalised wave vector (fourier.py:61-85): FP64 with the 1e-12 guard
     double nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
     if (nrm < 1.0e-12) nrm = 1.0;
-    const float z0 = (float)(x0 / nrm), z1 = (float)(x1 / nrm), z2 = (float)(x2 / nrm);
+    const T z0 = (T)(x0 / nrm), z1 = (T)(x1 / nrm), z2 = (T)(x2 / nrm);
     // r_hat = C_A A(xi) sigma_hat + C_B (xi xi : sigma_hat) xi xi   (fourier.cu:268-327)
-    const float z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
-    const float z01 = z0 * z1, z02 = z0 * z2, z12 = z1 * z2;
-    float2 r[6];
+    const T z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
+    const T z01 = z0 * z1, z02 = z0 * z2, z12 = z1 * z2;
+    T o[2][6];
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
-      float t0 = part ? s[0].y : s[0].x, t1 = part ? s[1].y : s[1].x, t2 = part ? s[2].y : s[2].x;
-      float t3 = part ? s[3].y : s[3].x, t4 = part ? s[4].y : s[4].x, t5 = part ? s[5].y : s[5].x;
-      float rho = z00 * t0 + z11 * t1 + z22 * t2 + 2.f * (z01 * t3 + z02 * t4 + z12 * t5);
-      float a0 = z0 * (z0 * t0 + z2 * t4 + z1 * t3);
-      float a1 = z1 * (z1 * t1 + z2 * t5 + z0 * t3);
-      float a2 = z2 * (z2 * t2 + z1 * t5 + z0 * t4);
-      float a3 = 0.5f * (z01 * (t0 + t1) + (z00 + z11) * t3 + z2 * (z0 * t5 + z1 * t4));
-      float a4 = 0.5f * (z02 * (t0 + t2) + (z00 + z22) * t4 + z1 * (z0 * t5 + z2 * t3));
-      float a5 = 0.5f * (z12 * (t1 + t2) + (z11 + z22) * t5 + z0 * (z1 * t4 + z2 * t3));
-      float o0 = c_a * a0 + c_b * rho * z00;
-      float o1 = c_a * a1 + c_b * rho * z11;
-      float o2 = c_a * a2 + c_b * rho * z22;
-      float o3 = c_a * a3 + c_b * rho * z01;
-      float o4 = c_a * a4 + c_b * rho * z02;
-      float o5 = c_a * a5 + c_b * rho * z12;
-      if (part == 0) {
-        r[0].x = o0; r[1].x = o1; r[2].x = o2; r[3].x = o3; r[4].x = o4; r[5].x = o5;
-      } else {
-        r[0].y = -o0; r[1].y = -o1; r[2].y = -o2; r[3].y = -o3; r[4].y = -o4; r[5].y = -o5;
-      }
+      T t0 = part ? s[0].y : s[0].x, t1 = part ? s[1].y : s[1].x, t2 = part ? s[2].y : s[2].x;
+      T t3 = part ? s[3].y : s[3].x, t4 = part ? s[4].y : s[4].x, t5 = part ? s[5].y : s[5].x;
+      T rho = z00 * t0 + z11 * t1 + z22 * t2 + (T)2 * (z01 * t3 + z02 * t4 + z12 * t5);
+      T a0 = z0 * (z0 * t0 + z2 * t4 + z1 * t3);
+      T a1 = z1 * (z1 * t1 + z2 * t5 + z0 * t3);
+      T a2 = z2 * (z2 * t2 + z1 * t5 + z0 * t4);
+      T a3 = (T)0.5 * (z01 * (t0 + t1) + (z00 + z11) * t3 + z2 * (z0 * t5 + z1 * t4));
+      T a4 = (T)0.5 * (z02 * (t0 + t2) + (z00 + z22) * t4 + z1 * (z0 * t5 + z2 * t3));
+      T a5 = (T)0.5 * (z12 * (t1 + t2) + (z11 + z22) * t5 + z0 * (z1 * t4 + z2 * t3));
+      o[part][0] = c_a * a0 + c_b * rho * z00;
+      o[part][1] = c_a * a1 + c_b * rho * z11;
+      o[part][2] = c_a * a2 + c_b * rho * z22;
+      o[part][3] = c_a * a3 + c_b * rho * z01;
+      o[part][4] = c_a * a4 + c_b * rho * z02;
+      o[part][5] = c_a * a5 + c_b * rho * z12;
     }
 #pragma unroll
-    for (int c = 0; c < 6; ++c) row[c * T] = r[c];
+    for (int c = 0; c < 6; ++c) row[c * TT] = mk<C>(o[0][c], -o[1][c]);
   }
   __syncthreads();
-  fft_lines<VPT, true>(xbuf, W, W, 1, g.px);
+  fft_lines<VPT, true>(xbuf, W, W, 1, g.px, tw);
   for (int idx = tid; idx < work; idx += nt) {
     int kx = idx / W, q = idx - kx * W;
-    int c = q / T, t = q - c * T;
+    int c = q / TT, t = q - c * TT;
     int kz = kz0 + t;
     if (kz < nzh) {
-      float2 v = xbuf[idx];
-      sb[c * cstride + kx * xstride + (size_t)ky * nzh + kz] = make_float2(v.x, -v.y);
+      C v = xbuf[idx];
+      sb[c * cstride + kx * xstride + (size_t)ky * nzh + kz] = mk<C>(v.x, -v.y);
     }
   }
 
@@ -296,15 +331,17 @@ __global__ void __launch_bounds__(kMaxThreads) xpass_kernel(GridDesc g, int T,
 }
 
 // ----------------------------------------------------------------------------- finalize
-// Criterion (lippmann_schwinger.py:118-143 / lippmann_schwinger.cu:95-109) and the stop
-// rule (lippmann_schwinger.cu:201-206; lippmann_schwinger.py:196-206).
-__global__ void finalize_kernel(int nblk, InstanceState* __restrict__ st,
+// Criterion (lippmann_schwinger.py:118-143 / lippmann_schwinger.cu:95-109), the stop
+// rule (lippmann_schwinger.cu:201-206; lippmann_schwinger.py:196-206) and, for mixed
+// precision, the switch to FP64 fields once FP32 round-off stalls the criterion near
+// the tolerance.
+__global__ void finalize_kernel(int nblk, int phase, InstanceState* __restrict__ st,
                                 const double* __restrict__ partials, double* __restrict__ history,
                                 int history_len, SolveParams sp) {
   __shared__ double red[32];
   const int b = blockIdx.x;
   InstanceState& s = st[b];
-  if (s.done) return;
+  if (s.done || s.phase != phase) return;
   const int tid = threadIdx.x, nt = blockDim.x;
   double acc = 0.0;
   for (int i = tid; i < nblk; i += nt) acc += partials[(size_t)b * nblk + i];
@@ -312,122 +349,200 @@ __global__ void finalize_kernel(int nblk, InstanceState* __restrict__ st,
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if ((tid & 31) == 0) red[tid >> 5] = acc;
   __syncthreads();
-  if (tid == 0) {
-    double num2 = 0.0;
-    for (int w = 0; w < (nt + 31) / 32; ++w) num2 += red[w];
-    double den2 = 0.0;
-    for (int c = 0; c < 6; ++c) {
-      double m2 = s.sig0[2 * c] * s.sig0[2 * c] + s.sig0[2 * c + 1] * s.sig0[2 * c + 1];
-      den2 += (c < 3 ? 1.0 : 2.0) * m2;
-    }
-    double e = (num2 == 0.0) ? 0.0 : sqrt(num2) / sqrt(den2);
-    if (s.evals == 0) s.e0 = e;
-    if (history != nullptr && s.evals < history_len) history[(size_t)b * history_len + s.evals] = e;
-    s.evals += 1;
-    s.e = e;
-    const double thr = fmax((double)sp.rtol * s.e0, (double)sp.atol);
-    const bool conv = sp.rule == 0 ? (e < thr) : (e <= thr);
-    if (!isfinite(e)) {
-      s.done = 1;
-      s.status = kNonFinite;
-    } else if (conv) {
-      s.done = 1;
-      s.status = kConverged;
-    } else if (s.iter >= sp.maxiter) {
-      s.done = 1;
-      s.status = kMaxIter;
-    } else {
-      s.iter += 1;
-    }
+  if (tid != 0) return;
+  double num2 = 0.0;
+  for (int w = 0; w < (nt + 31) / 32; ++w) num2 += red[w];
+  double den2 = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    double m2 = s.sig0[2 * c] * s.sig0[2 * c] + s.sig0[2 * c + 1] * s.sig0[2 * c + 1];
+    den2 += (c < 3 ? 1.0 : 2.0) * m2;
   }
+  const double e = (num2 == 0.0) ? 0.0 : sqrt(num2) / sqrt(den2);
+  if (s.evals == 0) {
+    s.e0 = e;
+    s.best_e = e;
+    s.best_eval = 0;
+  }
+  if (history != nullptr && s.evals < history_len) history[(size_t)b * history_len + s.evals] = e;
+  s.evals += 1;
+  s.e = e;
+  const double thr = fmax(sp.rtol * s.e0, sp.atol);
+  const bool conv = sp.rule == 0 ? (e < thr) : (e <= thr);
+  // the next forward transform is shifted by the current mean stress
+  const double inv_nv = 1.0 / (double)sp.nv;
+  for (int c = 0; c < 6; ++c) s.shift[c] = s.sig0[2 * c] * inv_nv;
+  if (!isfinite(e)) {
+    s.done = 1;
+    s.status = kNonFinite;
+    return;
+  }
+  if (conv) {
+    s.done = 1;
+    s.status = kConverged;
+    return;
+  }
+  if (s.iter >= sp.maxiter) {
+    s.done = 1;
+    s.status = kMaxIter;
+    return;
+  }
+  if (e < sp.stall_improve * s.best_e) s.best_eval = s.evals;
+  if (e < s.best_e) s.best_e = e;
+  const bool stalled = phase == 0 && sp.precision != kPrecFP64 && sp.stall_window > 0 &&
+                       s.best_e < sp.stall_near * thr &&
+                       s.evals - s.best_eval >= sp.stall_window;
+  if (stalled) {
+    if (sp.precision == kPrecMixed) {
+      // continue from this iterate with FP64 fields; no FP32 update for this evaluation
+      s.phase = 1;
+      s.switched = 1;
+      s.best_eval = s.evals;
+    } else {
+      s.done = 1;
+      s.status = kStalled;
+    }
+    return;
+  }
+  s.iter += 1;
 }
 
-__global__ void reset_state_kernel(int batch, InstanceState* st) {
+__global__ void reset_state_kernel(int batch, int phase, InstanceState* st) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < batch) {
     InstanceState z = {};
+    z.phase = phase;
     st[b] = z;
   }
 }
 
 // ----------------------------------------------------------------------------- medium
-__global__ void minmax_partial_kernel(long long nv, const float* __restrict__ lambda,
-                                      const float* __restrict__ mu, float* __restrict__ scratch) {
-  __shared__ float sh[4][32];
-  float lmin = FLT_MAX, lmax = -FLT_MAX, mmin = FLT_MAX, mmax = -FLT_MAX;
+template <typename TL>
+__global__ void minmax_partial_kernel(long long nv, const TL* __restrict__ lambda,
+                                      const TL* __restrict__ mu, double* __restrict__ scratch) {
+  __shared__ double sh[6][32];
+  double lmin = DBL_MAX, lmax = -DBL_MAX, mmin = DBL_MAX, mmax = -DBL_MAX;
+  double lsum = 0.0, msum = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
        i += (long long)gridDim.x * blockDim.x) {
-    float l = lambda[i], m = mu[i];
-    lmin = fminf(lmin, l); lmax = fmaxf(lmax, l);
-    mmin = fminf(mmin, m); mmax = fmaxf(mmax, m);
+    double l = lambda[i], m = mu[i];
+    lmin = fmin(lmin, l); lmax = fmax(lmax, l);
+    mmin = fmin(mmin, m); mmax = fmax(mmax, m);
+    lsum += l;
+    msum += m;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    lmin = fminf(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
-    lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    mmin = fminf(mmin, __shfl_xor_sync(0xffffffffu, mmin, o));
-    mmax = fmaxf(mmax, __shfl_xor_sync(0xffffffffu, mmax, o));
+    lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+    lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    mmin = fmin(mmin, __shfl_xor_sync(0xffffffffu, mmin, o));
+    mmax = fmax(mmax, __shfl_xor_sync(0xffffffffu, mmax, o));
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    msum += __shfl_xor_sync(0xffffffffu, msum, o);
   }
   const int w = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) { sh[0][w] = lmin; sh[1][w] = lmax; sh[2][w] = mmin; sh[3][w] = mmax; }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][w] = lmin; sh[1][w] = lmax; sh[2][w] = mmin; sh[3][w] = mmax;
+    sh[4][w] = lsum; sh[5][w] = msum;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int i = 1; i < (blockDim.x + 31) / 32; ++i) {
-      lmin = fminf(lmin, sh[0][i]); lmax = fmaxf(lmax, sh[1][i]);
-      mmin = fminf(mmin, sh[2][i]); mmax = fmaxf(mmax, sh[3][i]);
+      lmin = fmin(lmin, sh[0][i]); lmax = fmax(lmax, sh[1][i]);
+      mmin = fmin(mmin, sh[2][i]); mmax = fmax(mmax, sh[3][i]);
+      lsum += sh[4][i];
+      msum += sh[5][i];
     }
-    scratch[4 * blockIdx.x + 0] = lmin;
-    scratch[4 * blockIdx.x + 1] = lmax;
-    scratch[4 * blockIdx.x + 2] = mmin;
-    scratch[4 * blockIdx.x + 3] = mmax;
+    double* o = scratch + 6 * blockIdx.x;
+    o[0] = lmin; o[1] = lmax; o[2] = mmin; o[3] = mmax; o[4] = lsum; o[5] = msum;
   }
 }
 
-__global__ void minmax_final_kernel(int nblk, const float* __restrict__ scratch, Medium* med) {
+__global__ void minmax_final_kernel(int nblk, long long nv, int fp64_fields,
+                                    const double* __restrict__ scratch, Medium* med) {
   if (threadIdx.x != 0) return;
-  float lmin = FLT_MAX, lmax = -FLT_MAX, mmin = FLT_MAX, mmax = -FLT_MAX;
+  double lmin = DBL_MAX, lmax = -DBL_MAX, mmin = DBL_MAX, mmax = -DBL_MAX;
+  double lsum = 0.0, msum = 0.0;
   for (int i = 0; i < nblk; ++i) {
-    lmin = fminf(lmin, scratch[4 * i + 0]); lmax = fmaxf(lmax, scratch[4 * i + 1]);
-    mmin = fminf(mmin, scratch[4 * i + 2]); mmax = fmaxf(mmax, scratch[4 * i + 3]);
+    const double* o = scratch + 6 * i;
+    lmin = fmin(lmin, o[0]); lmax = fmax(lmax, o[1]);
+    mmin = fmin(mmin, o[2]); mmax = fmax(mmax, o[3]);
+    lsum += o[4];
+    msum += o[5];
   }
   Medium m;
   m.lmin = lmin; m.lmax = lmax; m.mmin = mmin; m.mmax = mmax;
-  // lambda0 = 1/2 (min + max) in FP32 (lippmann_schwinger.py:171-172)
-  m.lambda0 = 0.5f * (lmin + lmax);
-  m.mu0 = 0.5f * (mmin + mmax);
-  const double l0 = m.lambda0, m0 = m.mu0;
-  m.c_a = (float)(-1.0 / m0);
-  m.c_b = (float)((l0 + m0) / (m0 * (l0 + 2.0 * m0)));
+  m.lmean = lsum / (double)nv;
+  m.mmean = msum / (double)nv;
+  // lambda0 = 1/2 (min + max) in the field precision (lippmann_schwinger.py:171-172)
+  m.lambda0 = 0.5f * ((float)lmin + (float)lmax);
+  m.mu0 = 0.5f * ((float)mmin + (float)mmax);
+  m.c_a = (float)(-1.0 / (double)m.mu0);
+  m.c_b = (float)(((double)m.lambda0 + m.mu0) / ((double)m.mu0 * ((double)m.lambda0 + 2.0 * m.mu0)));
+  if (fp64_fields) {
+    m.lambda0_64 = 0.5 * (lmin + lmax);
+    m.mu0_64 = 0.5 * (mmin + mmax);
+  } else {
+    m.lambda0_64 = m.lambda0;
+    m.mu0_64 = m.mu0;
+  }
+  m.c_a64 = -1.0 / m.mu0_64;
+  m.c_b64 = (m.lambda0_64 + m.mu0_64) / (m.mu0_64 * (m.lambda0_64 + 2.0 * m.mu0_64));
   *med = m;
 }
 
+// ----------------------------------------------------------------------------- conversions
+// out[b] = in[b] for every instance b with phase == 1 (and, if only_running, not done).
+template <typename Tin, typename Tout>
+__global__ void convert_fields_kernel(long long n_per_instance, int only_running,
+                                      const InstanceState* __restrict__ st,
+                                      const Tin* __restrict__ in, Tout* __restrict__ out) {
+  const int b = blockIdx.y;
+  if (st[b].phase != 1 || (only_running && st[b].done)) return;
+  const Tin* ib = in + (size_t)b * n_per_instance;
+  Tout* ob = out + (size_t)b * n_per_instance;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_per_instance;
+       i += (long long)gridDim.x * blockDim.x)
+    ob[i] = (Tout)ib[i];
+}
+
+template <typename Tin, typename Tout>
+__global__ void convert_plain_kernel(long long n, const Tin* __restrict__ in, Tout* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (Tout)in[i];
+}
+
 // ----------------------------------------------------------------------------- stress
-__global__ void stress_kernel(long long nv, int batch, const float* __restrict__ lambda,
-                              const float* __restrict__ mu, const float* __restrict__ eps,
-                              float* __restrict__ sigma, double* __restrict__ scratch) {
+// sigma = C : eps for every instance of the given phase; sigma is written in TS.
+template <typename T, typename TS>
+__global__ void stress_kernel(long long nv, int phase, const InstanceState* __restrict__ st,
+                              const T* __restrict__ lambda, const T* __restrict__ mu,
+                              const T* __restrict__ eps, TS* __restrict__ sigma,
+                              double* __restrict__ scratch) {
   __shared__ double sh[6][32];
   const int b = blockIdx.y;
-  const float* eb = eps + (size_t)b * 6 * nv;
-  float* sg = sigma ? sigma + (size_t)b * 6 * nv : nullptr;
+  if (st[b].phase != phase) return;
+  const T* eb = eps + (size_t)b * 6 * nv;
+  TS* sg = sigma ? sigma + (size_t)b * 6 * nv : nullptr;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
        i += (long long)gridDim.x * blockDim.x) {
-    float e[6];
+    T e[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * nv + i];
-    const float lam = lambda[i], tmu = 2.f * mu[i];
-    const float ltr = lam * (e[0] + e[1] + e[2]);
-    float s[6];
+    const T lam = lambda[i], tmu = (T)2 * mu[i];
+    const T ltr = lam * (e[0] + e[1] + e[2]);
+    T s[6];
 #pragma unroll
     for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
 #pragma unroll
     for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
     if (sg) {
 #pragma unroll
-      for (int c = 0; c < 6; ++c) sg[(size_t)c * nv + i] = s[c];
+      for (int c = 0; c < 6; ++c) sg[(size_t)c * nv + i] = (TS)s[c];
     }
 #pragma unroll
-    for (int c = 0; c < 6; ++c) acc[c] += s[c];
+    for (int c = 0; c < 6; ++c) acc[c] += (double)s[c];
   }
   if (scratch == nullptr) return;
 #pragma unroll
@@ -448,10 +563,11 @@ __global__ void stress_kernel(long long nv, int batch, const float* __restrict__
   }
 }
 
-__global__ void mean_final_kernel(int nblk, long long nv, const double* __restrict__ scratch,
-                                  double* __restrict__ mean) {
+__global__ void mean_final_kernel(int nblk, long long nv, int phase,
+                                  const InstanceState* __restrict__ st,
+                                  const double* __restrict__ scratch, double* __restrict__ mean) {
   const int bc = blockIdx.x;  // instance * 6 + component
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x != 0 || st[bc / 6].phase != phase) return;
   double v = 0.0;
   for (int i = 0; i < nblk; ++i) v += scratch[(size_t)bc * nblk + i];
   mean[bc] = v / (double)nv;
@@ -464,110 +580,157 @@ static int pick_pow2_leq(int v) {
   return p;
 }
 
-LaunchShape plan_launch(const GridDesc& g) {
+LaunchShape plan_launch(const GridDesc& g, int elem_bytes) {
   LaunchShape s;
-  const long long kElems = kPassElems;
+  const long long kElems = kPassBytes / elem_bytes;
   // z pass: 3 complex lines of nz per (x, y) line
   s.lines_per_block = (int)std::max<long long>(1, kElems / (3LL * g.nz));
-  s.lines_per_block = std::min<long long>(s.lines_per_block, (long long)g.nx * g.ny);
+  s.lines_per_block = (int)std::min<long long>(s.lines_per_block, (long long)g.nx * g.ny);
   s.z_threads = threads_for(g.pz, 3LL * s.lines_per_block * g.nz, kVPT);
   while (s.z_threads > kMaxThreads && s.lines_per_block > 1) {
     s.lines_per_block -= 1;
     s.z_threads = threads_for(g.pz, 3LL * s.lines_per_block * g.nz, kVPT);
   }
   s.z_blocks = (int)(((long long)g.nx * g.ny + s.lines_per_block - 1) / s.lines_per_block);
-  s.z_smem = (size_t)3 * s.lines_per_block * g.nz * sizeof(float2);
+  s.z_smem = (size_t)3 * s.lines_per_block * g.nz * elem_bytes;
   // y pass
   s.ty = std::max(1, std::min(16, (int)(kElems / g.ny)));
   s.ty = std::min(s.ty, g.nzh);
-  s.y_tiles = (g.nzh + s.ty - 1) / s.ty;
   s.y_threads = threads_for(g.py, (long long)g.ny * s.ty, kVPT);
   while (s.y_threads > kMaxThreads && s.ty > 1) {
     s.ty -= 1;
     s.y_threads = threads_for(g.py, (long long)g.ny * s.ty, kVPT);
   }
   s.y_tiles = (g.nzh + s.ty - 1) / s.ty;
-  s.y_smem = (size_t)g.ny * s.ty * sizeof(float2);
+  s.y_smem = (size_t)g.ny * s.ty * elem_bytes;
   // x pass
   s.tx = std::max(1, std::min(16, pick_pow2_leq((int)std::max<long long>(1, kElems / (6LL * g.nx)))));
   s.tx = std::min(s.tx, g.nzh);
-  s.x_tiles = (g.nzh + s.tx - 1) / s.tx;
   s.x_threads = threads_for(g.px, 6LL * g.nx * s.tx, kVPT);
   while (s.x_threads > kMaxThreads && s.tx > 1) {
     s.tx /= 2;
     s.x_threads = threads_for(g.px, 6LL * g.nx * s.tx, kVPT);
   }
   s.x_tiles = (g.nzh + s.tx - 1) / s.tx;
-  s.x_smem = (size_t)6 * g.nx * s.tx * sizeof(float2);
+  s.x_smem = (size_t)6 * g.nx * s.tx * elem_bytes;
   s.x_blocks_per_instance = s.x_tiles * g.ny;
   return s;
 }
 
-// Every pass is planned with at most kPassElems complex values of dynamic shared memory,
-// so one fixed opt-in serves all solvers alive in the process.
-cudaError_t configure_kernels(const LaunchShape& s) {
-  const int bytes = (int)(kPassElems * sizeof(float2));
-  if (s.z_smem > (size_t)bytes || s.y_smem > (size_t)bytes || s.x_smem > (size_t)bytes)
-    return cudaErrorInvalidValue;
+// Every pass is planned with at most kPassBytes of dynamic shared memory, so one fixed
+// opt-in serves all solvers alive in the process.
+template <typename T>
+static cudaError_t configure_for() {
+  const int bytes = (int)kPassBytes;
   cudaError_t e;
-  e = cudaFuncSetAttribute(zpass_kernel<kVPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  e = cudaFuncSetAttribute(zpass_kernel<T, kVPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(ypass_kernel<kVPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  e = cudaFuncSetAttribute(ypass_kernel<T, kVPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(xpass_kernel<kVPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  return e;
+  return cudaFuncSetAttribute(xpass_kernel<T, kVPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-void launch_zpass(const GridDesc& g, const LaunchShape& s, int mode, int batch, const float* lambda,
-                  const float* mu, float* eps, float2* spec, const float* eps_bar,
-                  const float* eps0, const InstanceState* st, const SolveParams& sp,
-                  cudaStream_t stream) {
+cudaError_t configure_kernels() {
+  cudaError_t e = configure_for<float>();
+  if (e != cudaSuccess) return e;
+  return configure_for<double>();
+}
+
+template <typename T>
+void launch_zpass(const GridDesc& g, const LaunchShape& s, int mode, int batch, const T* lambda,
+                  const T* mu, T* eps, cplx<T>* spec, const double* eps_bar, const T* eps0,
+                  InstanceState* st, const Medium* med, cudaStream_t stream) {
   dim3 grid(s.z_blocks, batch);
-  zpass_kernel<kVPT><<<grid, s.z_threads, s.z_smem, stream>>>(
-      g, mode, s.lines_per_block, lambda, mu, eps, spec, eps_bar, eps0, st, sp);
+  zpass_kernel<T, kVPT><<<grid, s.z_threads, s.z_smem, stream>>>(
+      g, mode, s.lines_per_block, lambda, mu, eps, spec, eps_bar, eps0, st, med);
 }
 
-void launch_ypass(const GridDesc& g, const LaunchShape& s, bool inverse, int batch, float2* spec,
+template <typename T>
+void launch_ypass(const GridDesc& g, const LaunchShape& s, bool inverse, int batch, cplx<T>* spec,
                   const InstanceState* st, cudaStream_t stream) {
   dim3 grid(s.y_tiles, g.nx, 6 * batch);
-  ypass_kernel<kVPT><<<grid, s.y_threads, s.y_smem, stream>>>(g, inverse ? 1 : 0, s.ty, spec, st);
+  ypass_kernel<T, kVPT><<<grid, s.y_threads, s.y_smem, stream>>>(g, inverse ? 1 : 0, s.ty, spec, st);
 }
 
-void launch_xpass(const GridDesc& g, const LaunchShape& s, int batch, float2* spec, const Medium* med,
+template <typename T>
+void launch_xpass(const GridDesc& g, const LaunchShape& s, int batch, cplx<T>* spec, const Medium* med,
                   InstanceState* st, double* partials, cudaStream_t stream) {
   dim3 grid(s.x_tiles, g.ny, batch);
-  xpass_kernel<kVPT><<<grid, s.x_threads, s.x_smem, stream>>>(g, s.tx, spec, med, st, partials);
+  xpass_kernel<T, kVPT><<<grid, s.x_threads, s.x_smem, stream>>>(g, s.tx, spec, med, st, partials);
 }
 
-void launch_finalize(const GridDesc& g, const LaunchShape& s, int batch, InstanceState* st,
+void launch_finalize(const LaunchShape& s, int phase, int batch, InstanceState* st,
                      const double* partials, double* history, int history_len,
                      const SolveParams& sp, cudaStream_t stream) {
-  (void)g;
-  finalize_kernel<<<batch, 256, 0, stream>>>(s.x_blocks_per_instance, st, partials, history,
+  finalize_kernel<<<batch, 256, 0, stream>>>(s.x_blocks_per_instance, phase, st, partials, history,
                                               history_len, sp);
 }
 
-void launch_reset_state(int batch, InstanceState* st, cudaStream_t stream) {
-  reset_state_kernel<<<(batch + 127) / 128, 128, 0, stream>>>(batch, st);
+void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t stream) {
+  reset_state_kernel<<<(batch + 127) / 128, 128, 0, stream>>>(batch, phase, st);
 }
 
-void launch_medium(long long nv, const float* lambda, const float* mu, float* scratch, Medium* med,
+template <typename TL>
+void launch_medium(long long nv, const TL* lambda, const TL* mu, double* scratch, Medium* med,
                    cudaStream_t stream) {
   int nblk = (int)std::min<long long>(1024, (nv + 255) / 256);
   if (nblk < 1) nblk = 1;
-  minmax_partial_kernel<<<nblk, 256, 0, stream>>>(nv, lambda, mu, scratch);
-  minmax_final_kernel<<<1, 32, 0, stream>>>(nblk, scratch, med);
+  minmax_partial_kernel<TL><<<nblk, 256, 0, stream>>>(nv, lambda, mu, scratch);
+  minmax_final_kernel<<<1, 32, 0, stream>>>(nblk, nv, sizeof(TL) == 8 ? 1 : 0, scratch, med);
 }
 
-void launch_stress(const GridDesc& g, int batch, const float* lambda, const float* mu,
-                   const float* eps, float* sigma, double* scratch, double* mean,
-                   cudaStream_t stream) {
+template <typename Tin, typename Tout>
+void launch_convert_fields(long long n_per_instance, int batch, int only_running,
+                           const InstanceState* st, const Tin* in, Tout* out, cudaStream_t stream) {
+  int nblk = (int)std::min<long long>(2048, (n_per_instance + 255) / 256);
+  dim3 grid(std::max(nblk, 1), batch);
+  convert_fields_kernel<Tin, Tout><<<grid, 256, 0, stream>>>(n_per_instance, only_running, st, in, out);
+}
+
+template <typename Tin, typename Tout>
+void launch_convert(long long n, const Tin* in, Tout* out, cudaStream_t stream) {
+  int nblk = (int)std::min<long long>(2048, (n + 255) / 256);
+  convert_plain_kernel<Tin, Tout><<<std::max(nblk, 1), 256, 0, stream>>>(n, in, out);
+}
+
+template <typename T, typename TS>
+void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState* st,
+                   const T* lambda, const T* mu, const T* eps, TS* sigma, double* scratch,
+                   double* mean, cudaStream_t stream) {
   int nblk = (int)std::min<long long>(1024, (g.nv + 255) / 256);
   if (nblk < 1) nblk = 1;
   dim3 grid(nblk, batch);
-  stress_kernel<<<grid, 256, 0, stream>>>(g.nv, batch, lambda, mu, eps, sigma,
-                                          mean ? scratch : nullptr);
-  if (mean) mean_final_kernel<<<6 * batch, 32, 0, stream>>>(nblk, g.nv, scratch, mean);
+  stress_kernel<T, TS><<<grid, 256, 0, stream>>>(g.nv, phase, st, lambda, mu, eps, sigma,
+                                                  mean ? scratch : nullptr);
+  if (mean) mean_final_kernel<<<6 * batch, 32, 0, stream>>>(nblk, g.nv, phase, st, scratch, mean);
 }
+
+// explicit instantiations
+#define LSB_INST(T)                                                                             \
+  template void launch_zpass<T>(const GridDesc&, const LaunchShape&, int, int, const T*,        \
+                                const T*, T*, cplx<T>*, const double*, const T*, InstanceState*, \
+                                const Medium*, cudaStream_t);                                   \
+  template void launch_ypass<T>(const GridDesc&, const LaunchShape&, bool, int, cplx<T>*,       \
+                                const InstanceState*, cudaStream_t);                            \
+  template void launch_xpass<T>(const GridDesc&, const LaunchShape&, int, cplx<T>*,             \
+                                const Medium*, InstanceState*, double*, cudaStream_t);          \
+  template void launch_medium<T>(long long, const T*, const T*, double*, Medium*, cudaStream_t);
+LSB_INST(float)
+LSB_INST(double)
+#undef LSB_INST
+template void launch_convert_fields<float, double>(long long, int, int, const InstanceState*,
+                                                   const float*, double*, cudaStream_t);
+template void launch_convert_fields<double, float>(long long, int, int, const InstanceState*,
+                                                   const double*, float*, cudaStream_t);
+template void launch_convert<float, double>(long long, const float*, double*, cudaStream_t);
+template void launch_stress<float, float>(const GridDesc&, int, int, const InstanceState*, const float*,
+                                          const float*, const float*, float*, double*, double*,
+                                          cudaStream_t);
+template void launch_stress<double, float>(const GridDesc&, int, int, const InstanceState*,
+                                           const double*, const double*, const double*, float*,
+                                           double*, double*, cudaStream_t);
+template void launch_stress<double, double>(const GridDesc&, int, int, const InstanceState*,
+                                            const double*, const double*, const double*, double*,
+                                            double*, double*, cudaStream_t);
 
 }  // namespace lsb

@@ -1,12 +1,14 @@
 // Kernel launchers of the Lippmann-Schwinger solver (implemented in ls_kernels.cu).
 #pragma once
 
+#include <algorithm>
+
 #include "ls_types.cuh"
 
 namespace lsb {
 
-constexpr int kVPT = 16;  // complex values per thread in the shared-memory FFTs
-constexpr long long kPassElems = 6144;  // complex values per block (48 KB of shared memory)
+constexpr int kVPT = 16;                 // complex values per thread in the shared-memory FFTs
+constexpr long long kPassBytes = 49152;  // dynamic shared memory of one FFT block
 
 struct LaunchShape {
   int lines_per_block = 1;  // z pass
@@ -18,30 +20,43 @@ struct LaunchShape {
   size_t z_smem = 0, y_smem = 0, x_smem = 0;
 };
 
-LaunchShape plan_launch(const GridDesc& g);
-cudaError_t configure_kernels(const LaunchShape& ls);
+// Tile and block sizes of the three passes for complex values of elem_bytes bytes.
+LaunchShape plan_launch(const GridDesc& g, int elem_bytes);
+cudaError_t configure_kernels();
 
-// eps/sigma/spec/state/partials are batch base pointers; `batch` instances run.
-// mode 0: eps = eps_bar (or eps0 if given); mode 1: eps += r / N from spec.
-void launch_zpass(const GridDesc& g, const LaunchShape& ls, int mode, int batch,
-                  const float* lambda, const float* mu, float* eps, float2* spec,
-                  const float* eps_bar, const float* eps0, const InstanceState* st,
-                  const SolveParams& sp, cudaStream_t s);
-void launch_ypass(const GridDesc& g, const LaunchShape& ls, bool inverse, int batch,
-                  float2* spec, const InstanceState* st, cudaStream_t s);
-void launch_xpass(const GridDesc& g, const LaunchShape& ls, int batch, float2* spec,
+// Pointers are batch base pointers; the kernels process instance b when it is not done
+// and its phase matches the precision T (float: phase 0, double: phase 1).
+// mode 0: eps = eps_bar (or eps0 if given); mode 1: eps += r / N from spec; mode 2: keep
+// eps and the stored shift (continuation in another precision).
+template <typename T>
+void launch_zpass(const GridDesc& g, const LaunchShape& ls, int mode, int batch, const T* lambda,
+                  const T* mu, T* eps, cplx<T>* spec, const double* eps_bar, const T* eps0,
+                  InstanceState* st, const Medium* med, cudaStream_t s);
+template <typename T>
+void launch_ypass(const GridDesc& g, const LaunchShape& ls, bool inverse, int batch, cplx<T>* spec,
+                  const InstanceState* st, cudaStream_t s);
+template <typename T>
+void launch_xpass(const GridDesc& g, const LaunchShape& ls, int batch, cplx<T>* spec,
                   const Medium* med, InstanceState* st, double* partials, cudaStream_t s);
-void launch_finalize(const GridDesc& g, const LaunchShape& ls, int batch, InstanceState* st,
+void launch_finalize(const LaunchShape& ls, int phase, int batch, InstanceState* st,
                      const double* partials, double* history, int history_len,
                      const SolveParams& sp, cudaStream_t s);
-void launch_reset_state(int batch, InstanceState* st, cudaStream_t s);
-// min/max of the Lame fields -> reference medium. `scratch` holds 4 * 1024 floats.
-void launch_medium(long long nv, const float* lambda, const float* mu, float* scratch,
-                   Medium* med, cudaStream_t s);
-// sigma = C : eps for every instance; if mean != nullptr also the FP64 mean of sigma
-// per instance and component ([batch][6]); `scratch` holds batch * 6 * 1024 doubles.
-void launch_stress(const GridDesc& g, int batch, const float* lambda, const float* mu,
-                   const float* eps, float* sigma, double* scratch, double* mean,
+void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t s);
+// min/max and FP64 means of the Lame fields -> reference medium; scratch: 6*1024 doubles.
+template <typename TL>
+void launch_medium(long long nv, const TL* lambda, const TL* mu, double* scratch, Medium* med,
                    cudaStream_t s);
+// out = in for instances in phase 1 (if only_running: and not done).
+template <typename Tin, typename Tout>
+void launch_convert_fields(long long n_per_instance, int batch, int only_running,
+                           const InstanceState* st, const Tin* in, Tout* out, cudaStream_t s);
+template <typename Tin, typename Tout>
+void launch_convert(long long n, const Tin* in, Tout* out, cudaStream_t s);
+// sigma = C : eps for the instances in `phase`; if mean != nullptr also the FP64 mean of
+// sigma per instance and component ([batch][6]); scratch: batch * 6 * 1024 doubles.
+template <typename T, typename TS>
+void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState* st,
+                   const T* lambda, const T* mu, const T* eps, TS* sigma, double* scratch,
+                   double* mean, cudaStream_t s);
 
 }  // namespace lsb

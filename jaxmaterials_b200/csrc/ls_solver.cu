@@ -1,9 +1,13 @@
 // Host side of liblippmannschwinger.so: plans, device buffers, the iteration driver and
 // the C ABI declared in include/lippmann_schwinger.h.
 //
-// The iteration never waits on the host per step: kernels read the per-instance stop flag
+// The iteration never waits on the host per step: kernels read the per-instance state
 // written by finalize_kernel, so the host enqueues iterations in growing chunks and reads
-// the 64-byte states back once per chunk.
+// the small states back once per chunk. Precision (lsb_set_precision):
+//   FP32   FP32 fields and FFTs throughout (FP64 norms); may stall at the FP32 floor;
+//   MIXED  FP32 until the criterion stalls near the tolerance, then the stalled
+//          instances continue from their iterate with FP64 fields and FFTs (default);
+//   FP64   FP64 fields and FFTs from the start.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -39,6 +43,12 @@ int fail(int code, const char* fmt, ...) {
       return fail(-2, "%s:%d: %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(_e)); \
   } while (0)
 
+#define LSB_TRY(expr)        \
+  do {                       \
+    int _rc = (expr);        \
+    if (_rc != 0) return _rc; \
+  } while (0)
+
 // Radices for a length-n Stockham plan: 8s first, then 4, 2, 3, 5, then remaining primes.
 bool factorize(int n, Plan1D& p) {
   p.n = n;
@@ -61,46 +71,50 @@ bool factorize(int n, Plan1D& p) {
   return true;
 }
 
+bool shape_fits(const LaunchShape& sh) {
+  return sh.z_threads <= kMaxThreads && sh.y_threads <= kMaxThreads && sh.x_threads <= kMaxThreads;
+}
+
 }  // namespace
 
 struct lsb_solver {
   int device = 0;
   int batch_cap = 0;
   int depth = 0;
+  int precision = kPrecMixed;
+  int stall_window = 8;
   GridDesc g{};
-  LaunchShape shape{};
+  LaunchShape sh32{}, sh64{};
   cudaStream_t stream = nullptr;
-  // device buffers
-  float* d_eps = nullptr;          // [batch][6][nv] working strain (when caller gives none)
-  float2* d_spec = nullptr;        // [batch][6][nm]
-  double* d_partials = nullptr;    // [batch][x blocks]
+  // FP32 work buffers
+  float* d_eps32 = nullptr;      // [batch][6][nv] (used when the caller passes no strain buffer)
+  float2* d_spec32 = nullptr;    // [batch][6][nm]
+  // FP64 work buffers, allocated on first use
+  double* d_eps64 = nullptr;
+  double2* d_spec64 = nullptr;
+  double* d_lame64 = nullptr;    // [2][nv]
+  // shared
+  double* d_partials = nullptr;  // [batch][x blocks]
   InstanceState* d_state = nullptr;
   Medium* d_medium = nullptr;
-  float* d_epsbar = nullptr;       // [batch][6]
-  float* d_mm_scratch = nullptr;   // min/max partials
+  double* d_epsbar = nullptr;    // [batch][6]
+  double* d_scratch = nullptr;   // 6 * 1024
   double* d_mean_scratch = nullptr;
-  double* d_mean = nullptr;        // [batch][6]
-  double* d_history = nullptr;     // [batch][history_len]
+  double* d_mean = nullptr;      // [batch][6]
+  double* d_history = nullptr;   // [batch][history_len]
   int history_len = 0;
   int last_batch = 0;
-  float2* d_tw = nullptr;
+  float2* d_tw32 = nullptr;
+  double2* d_tw64 = nullptr;
   double* d_tables = nullptr;
   InstanceState* h_state = nullptr;  // pinned
   long long launches = 0;            // kernels enqueued by this solver
 
   ~lsb_solver() {
-    cudaFree(d_eps);
-    cudaFree(d_spec);
-    cudaFree(d_partials);
-    cudaFree(d_state);
-    cudaFree(d_medium);
-    cudaFree(d_epsbar);
-    cudaFree(d_mm_scratch);
-    cudaFree(d_mean_scratch);
-    cudaFree(d_mean);
-    cudaFree(d_history);
-    cudaFree(d_tw);
-    cudaFree(d_tables);
+    void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
+                    d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
+                    d_tables};
+    for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
   }
 };
@@ -116,7 +130,16 @@ int ensure_history(lsb_solver* s, int len) {
   return 0;
 }
 
-int create_impl(lsb_solver** out, const int voxels[3], const float extents[3], int batch, int depth) {
+int ensure_fp64(lsb_solver* s) {
+  if (s->d_spec64) return 0;
+  const size_t B = (size_t)s->batch_cap;
+  LSB_CUDA(cudaMalloc(&s->d_eps64, sizeof(double) * B * 6 * s->g.nv));
+  LSB_CUDA(cudaMalloc(&s->d_spec64, sizeof(double2) * B * 6 * s->g.nm));
+  LSB_CUDA(cudaMalloc(&s->d_lame64, sizeof(double) * 2 * s->g.nv));
+  return 0;
+}
+
+int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], int batch, int depth) {
   if (!out || !voxels || !extents) return fail(-1, "null argument");
   *out = nullptr;
   for (int d = 0; d < 3; ++d) {
@@ -145,9 +168,9 @@ int create_impl(lsb_solver** out, const int voxels[3], const float extents[3], i
     delete s;
     return fail(-1, "grid extent has too many prime factors");
   }
-  s->shape = plan_launch(g);
-  const LaunchShape& sh = s->shape;
-  if (sh.z_threads > kMaxThreads || sh.y_threads > kMaxThreads || sh.x_threads > kMaxThreads) {
+  s->sh32 = plan_launch(g, sizeof(float2));
+  s->sh64 = plan_launch(g, sizeof(double2));
+  if (!shape_fits(s->sh32) || !shape_fits(s->sh64)) {
     delete s;
     return fail(-1, "grid %dx%dx%d needs FFT blocks above %d threads", g.nx, g.ny, g.nz, kMaxThreads);
   }
@@ -158,16 +181,19 @@ int create_impl(lsb_solver** out, const int voxels[3], const float extents[3], i
     return e == cudaSuccess;
   };
   const size_t B = (size_t)batch;
-  bool ok = alloc((void**)&s->d_eps, sizeof(float) * B * 6 * g.nv) &&
-            alloc((void**)&s->d_spec, sizeof(float2) * B * 6 * g.nm) &&
-            alloc((void**)&s->d_partials, sizeof(double) * B * sh.x_blocks_per_instance) &&
+  const size_t xblk = (size_t)std::max(s->sh32.x_blocks_per_instance, s->sh64.x_blocks_per_instance);
+  const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
+  bool ok = alloc((void**)&s->d_eps32, sizeof(float) * B * 6 * g.nv) &&
+            alloc((void**)&s->d_spec32, sizeof(float2) * B * 6 * g.nm) &&
+            alloc((void**)&s->d_partials, sizeof(double) * B * xblk) &&
             alloc((void**)&s->d_state, sizeof(InstanceState) * B) &&
             alloc((void**)&s->d_medium, sizeof(Medium)) &&
-            alloc((void**)&s->d_epsbar, sizeof(float) * B * 6) &&
-            alloc((void**)&s->d_mm_scratch, sizeof(float) * 4 * 1024) &&
+            alloc((void**)&s->d_epsbar, sizeof(double) * B * 6) &&
+            alloc((void**)&s->d_scratch, sizeof(double) * 6 * 1024) &&
             alloc((void**)&s->d_mean_scratch, sizeof(double) * B * 6 * 1024) &&
             alloc((void**)&s->d_mean, sizeof(double) * B * 6) &&
-            alloc((void**)&s->d_tw, sizeof(float2) * (size_t)(g.nx + g.ny + g.nz)) &&
+            alloc((void**)&s->d_tw32, sizeof(float2) * ntw) &&
+            alloc((void**)&s->d_tw64, sizeof(double2) * ntw) &&
             alloc((void**)&s->d_tables, sizeof(double) * 2 * (size_t)(g.nx + g.ny + g.nzh));
   if (!ok) {
     delete s;
@@ -179,11 +205,14 @@ int create_impl(lsb_solver** out, const int voxels[3], const float extents[3], i
   }
   // twiddles exp(-2 pi i k / n) and the sin/cos tables of the modified wave vectors,
   // both evaluated in FP64 (fourier.py:29-31: xi_d / 2 = pi k_d / N_d)
-  std::vector<float2> tw;
+  std::vector<float2> tw32;
+  std::vector<double2> tw64;
   for (int n : {g.nx, g.ny, g.nz})
     for (int k = 0; k < n; ++k) {
       double a = -2.0 * M_PI * (double)k / (double)n;
-      tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+      double c = std::cos(a), sn = std::sin(a);
+      tw32.push_back(make_float2((float)c, (float)sn));
+      tw64.push_back(make_double2(c, sn));
     }
   std::vector<double> tab;
   auto add_tab = [&](int n, int count) {
@@ -193,21 +222,25 @@ int create_impl(lsb_solver** out, const int voxels[3], const float extents[3], i
   add_tab(g.nx, g.nx);
   add_tab(g.ny, g.ny);
   add_tab(g.nz, g.nzh);
-  if (cudaMemcpy(s->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+  if (cudaMemcpy(s->d_tw32, tw32.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->d_tw64, tw64.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(s->d_tables, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
     delete s;
     return fail(-2, "upload of twiddle tables failed");
   }
-  g.px.tw = s->d_tw;
-  g.py.tw = s->d_tw + g.nx;
-  g.pz.tw = s->d_tw + g.nx + g.ny;
+  g.px.tw = s->d_tw32;
+  g.py.tw = s->d_tw32 + g.nx;
+  g.pz.tw = s->d_tw32 + g.nx + g.ny;
+  g.px.tw64 = s->d_tw64;
+  g.py.tw64 = s->d_tw64 + g.nx;
+  g.pz.tw64 = s->d_tw64 + g.nx + g.ny;
   g.sx = s->d_tables;
   g.cx = g.sx + g.nx;
   g.sy = g.cx + g.nx;
   g.cy = g.sy + g.ny;
   g.sz = g.cy + g.ny;
   g.cz = g.sz + g.nzh;
-  cudaError_t e = configure_kernels(sh);
+  cudaError_t e = configure_kernels();
   if (e != cudaSuccess) {
     delete s;
     return fail(-2, "kernel configuration: %s", cudaGetErrorString(e));
@@ -216,66 +249,154 @@ int create_impl(lsb_solver** out, const int voxels[3], const float extents[3], i
   return 0;
 }
 
-int solve_impl(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
-               const float* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,
-               double* mean_sigma, float rtol, float atol, int maxiter, int rule, int* iters,
-               int* status, double* residual) {
-  if (!s) return fail(-1, "null solver");
-  if (batch < 1 || batch > s->batch_cap) return fail(-1, "batch %d outside [1, %d]", batch, s->batch_cap);
-  if (!d_lambda || !d_mu || !eps_bar || !iters || !status) return fail(-1, "null argument");
-  if (maxiter < 0) return fail(-1, "maxiter must be >= 0");
-  int cur = 0;
-  cudaGetDevice(&cur);
-  if (cur != s->device) return fail(-1, "solver was created on device %d, current is %d", s->device, cur);
-  const GridDesc& g = s->g;
-  const LaunchShape& sh = s->shape;
-  cudaStream_t st = s->stream;
-  float* eps = d_eps ? d_eps : s->d_eps;
-  if (ensure_history(s, maxiter + 1)) return -3;
+SolveParams make_params(const lsb_solver* s, double rtol, double atol, int maxiter, int rule) {
   SolveParams sp;
   sp.rtol = rtol;
   sp.atol = atol;
   sp.maxiter = maxiter;
   sp.rule = rule;
-  sp.inv_nv = (float)(1.0 / (double)g.nv);
+  sp.nv = s->g.nv;
+  sp.precision = s->precision;
+  sp.stall_window = s->stall_window;
+  sp.stall_improve = 0.98;
+  sp.stall_near = 4.0;
+  return sp;
+}
 
-  LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(float) * 6 * batch, cudaMemcpyHostToDevice, st));
-  LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
-  launch_reset_state(batch, s->d_state, st);
-  launch_medium(g.nv, d_lambda, d_mu, s->d_mm_scratch, s->d_medium, st);
-  launch_zpass(g, sh, 0, batch, d_lambda, d_mu, eps, s->d_spec, s->d_epsbar, d_eps0, s->d_state, sp, st);
-  launch_ypass(g, sh, false, batch, s->d_spec, s->d_state, st);
-  s->launches += 5;
+// Runs the loop of precision T for every instance in its phase until none is left there.
+// init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
+template <typename T>
+int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
+              const T* eps0, int init_mode, const SolveParams& sp) {
+  const GridDesc& g = s->g;
+  const LaunchShape& sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
+  const int phase = sizeof(T) == 8 ? 1 : 0;
+  cudaStream_t st = s->stream;
+  launch_zpass<T>(g, sh, init_mode, batch, lam, mu, eps, spec, s->d_epsbar, eps0, s->d_state,
+                  s->d_medium, st);
+  launch_ypass<T>(g, sh, false, batch, spec, s->d_state, st);
+  s->launches += 2;
   LSB_CUDA(cudaGetLastError());
-
   long long launched = 0;
-  const long long max_evals = (long long)maxiter + 1;
+  const long long max_evals = (long long)sp.maxiter + 2;
   int chunk = 1;
   for (;;) {
     int n = (int)std::min<long long>(chunk, max_evals - launched);
     for (int i = 0; i < n; ++i) {
-      launch_xpass(g, sh, batch, s->d_spec, s->d_medium, s->d_state, s->d_partials, st);
-      launch_finalize(g, sh, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
-      launch_ypass(g, sh, true, batch, s->d_spec, s->d_state, st);
-      launch_zpass(g, sh, 1, batch, d_lambda, d_mu, eps, s->d_spec, s->d_epsbar, nullptr, s->d_state, sp, st);
-      launch_ypass(g, sh, false, batch, s->d_spec, s->d_state, st);
+      launch_xpass<T>(g, sh, batch, spec, s->d_medium, s->d_state, s->d_partials, st);
+      launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
+      launch_ypass<T>(g, sh, true, batch, spec, s->d_state, st);
+      launch_zpass<T>(g, sh, 1, batch, lam, mu, eps, spec, s->d_epsbar, nullptr, s->d_state,
+                      s->d_medium, st);
+      launch_ypass<T>(g, sh, false, batch, spec, s->d_state, st);
     }
     launched += n;
     s->launches += 5LL * n;
     LSB_CUDA(cudaGetLastError());
-    LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch, cudaMemcpyDeviceToHost, st));
+    LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch,
+                             cudaMemcpyDeviceToHost, st));
     LSB_CUDA(cudaStreamSynchronize(st));
-    bool all = true;
-    for (int b = 0; b < batch; ++b) all = all && s->h_state[b].done;
-    if (all) break;
+    bool left = false;
+    for (int b = 0; b < batch; ++b) left = left || (!s->h_state[b].done && s->h_state[b].phase == phase);
+    if (!left) return 0;
     if (launched >= max_evals) return fail(-4, "internal: iteration driver did not terminate");
     chunk = std::min(chunk * 2, 32);
   }
-  launch_stress(g, batch, d_lambda, d_mu, eps, d_sigma, s->d_mean_scratch, mean_sigma ? s->d_mean : nullptr, st);
-  s->launches += mean_sigma ? 2 : 1;
+}
+
+// Full solve with FP32 inputs/outputs. d_eps (FP32) is the FP32 work buffer and output.
+int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
+              const double* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,
+              double* mean_sigma, double rtol, double atol, int maxiter, int rule, int* iters,
+              int* status, double* residual) {
+  if (!s) return fail(-1, "null solver");
+  if (batch < 1 || batch > s->batch_cap) return fail(-1, "batch %d outside [1, %d]", batch, s->batch_cap);
+  if (!d_lambda || !d_mu || !eps_bar || !iters || !status || !d_eps) return fail(-1, "null argument");
+  if (maxiter < 0) return fail(-1, "maxiter must be >= 0");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != s->device) return fail(-1, "solver was created on device %d, current is %d", s->device, cur);
+  const GridDesc& g = s->g;
+  cudaStream_t st = s->stream;
+  LSB_TRY(ensure_history(s, maxiter + 8));
+  const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
+  const bool fp64_start = s->precision == kPrecFP64;
+  if (s->precision != kPrecFP32) LSB_TRY(ensure_fp64(s));
+
+  LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
+  LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
+  launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st);
+  launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  s->launches += 3;
+  bool any64 = fp64_start;
+  if (!fp64_start) {
+    LSB_TRY(run_phase<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, d_eps0, 0, sp));
+    for (int b = 0; b < batch; ++b) any64 = any64 || (s->h_state[b].phase == 1 && !s->h_state[b].done);
+  }
+  if (any64) {
+    const long long n6 = 6 * g.nv;
+    launch_convert<float, double>(g.nv, d_lambda, s->d_lame64, st);
+    launch_convert<float, double>(g.nv, d_mu, s->d_lame64 + g.nv, st);
+    s->launches += 2;
+    if (fp64_start && d_eps0) {
+      launch_convert_fields<float, double>(n6, batch, 1, s->d_state, d_eps0, s->d_eps64, st);
+      s->launches += 1;
+    } else if (!fp64_start) {
+      launch_convert_fields<float, double>(n6, batch, 1, s->d_state, d_eps, s->d_eps64, st);
+      s->launches += 1;
+    }
+    const int init_mode = fp64_start ? (d_eps0 ? 2 : 0) : 2;
+    LSB_TRY(run_phase<double>(s, batch, s->d_lame64, s->d_lame64 + g.nv, s->d_eps64, s->d_spec64,
+                              nullptr, init_mode, sp));
+    launch_convert_fields<double, float>(n6, batch, 0, s->d_state, s->d_eps64, d_eps, st);
+    launch_stress<double, float>(g, 1, batch, s->d_state, s->d_lame64, s->d_lame64 + g.nv, s->d_eps64,
+                                 d_sigma, s->d_mean_scratch, s->d_mean, st);
+    s->launches += 3;
+  }
+  launch_stress<float, float>(g, 0, batch, s->d_state, d_lambda, d_mu, d_eps, d_sigma,
+                              s->d_mean_scratch, s->d_mean, st);
+  s->launches += 2;
   LSB_CUDA(cudaGetLastError());
   if (mean_sigma)
     LSB_CUDA(cudaMemcpyAsync(mean_sigma, s->d_mean, sizeof(double) * 6 * batch, cudaMemcpyDeviceToHost, st));
+  LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch, cudaMemcpyDeviceToHost, st));
+  LSB_CUDA(cudaStreamSynchronize(st));
+  for (int b = 0; b < batch; ++b) {
+    iters[b] = s->h_state[b].iter;
+    status[b] = s->h_state[b].status;
+    if (residual) residual[b] = s->h_state[b].e;
+  }
+  s->last_batch = batch;
+  return 0;
+}
+
+// Full solve with FP64 inputs/outputs (FP64 fields throughout).
+int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_mu,
+              const double* eps_bar, const double* d_eps0, double* d_eps, double* d_sigma,
+              double* mean_sigma, double rtol, double atol, int maxiter, int rule, int* iters,
+              int* status, double* residual) {
+  if (!s) return fail(-1, "null solver");
+  if (batch < 1 || batch > s->batch_cap) return fail(-1, "batch %d outside [1, %d]", batch, s->batch_cap);
+  if (!d_lambda || !d_mu || !eps_bar || !iters || !status || !d_eps) return fail(-1, "null argument");
+  if (maxiter < 0) return fail(-1, "maxiter must be >= 0");
+  const GridDesc& g = s->g;
+  cudaStream_t st = s->stream;
+  LSB_TRY(ensure_history(s, maxiter + 8));
+  LSB_TRY(ensure_fp64(s));
+  const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
+  LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
+  LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
+  launch_reset_state(batch, 1, s->d_state, st);
+  launch_medium<double>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  s->launches += 3;
+  LSB_TRY(run_phase<double>(s, batch, d_lambda, d_mu, d_eps, s->d_spec64, d_eps0, 0, sp));
+  launch_stress<double, double>(g, 1, batch, s->d_state, d_lambda, d_mu, d_eps, d_sigma,
+                                s->d_mean_scratch, s->d_mean, st);
+  s->launches += 2;
+  LSB_CUDA(cudaGetLastError());
+  if (mean_sigma)
+    LSB_CUDA(cudaMemcpyAsync(mean_sigma, s->d_mean, sizeof(double) * 6 * batch, cudaMemcpyDeviceToHost, st));
+  LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch, cudaMemcpyDeviceToHost, st));
   LSB_CUDA(cudaStreamSynchronize(st));
   for (int b = 0; b < batch; ++b) {
     iters[b] = s->h_state[b].iter;
@@ -291,7 +412,7 @@ struct AbiCache {
   std::mutex mu;
   lsb_solver* solver = nullptr;
   int voxels[3] = {0, 0, 0};
-  float extents[3] = {0, 0, 0};
+  double extents[3] = {0, 0, 0};
   float* d_lame = nullptr;   // [2][nv]
   float* d_fields = nullptr; // [2][6][nv] eps, sigma
   size_t nv = 0;
@@ -314,11 +435,11 @@ AbiCache& abi_cache() {
 
 extern "C" {
 
-int lsb_version(void) { return 1; }
+int lsb_version(void) { return 2; }
 
 const char* lsb_last_error(void) { return g_last_error.c_str(); }
 
-int lsb_create(lsb_solver** out, const int voxels[3], const float extents[3], int batch, int depth) {
+int lsb_create(lsb_solver** out, const int voxels[3], const double extents[3], int batch, int depth) {
   g_last_error.clear();
   return create_impl(out, voxels, extents, batch, depth);
 }
@@ -331,14 +452,34 @@ int lsb_set_stream(lsb_solver* solver, void* stream) {
   return 0;
 }
 
+int lsb_set_precision(lsb_solver* solver, int precision, int stall_window) {
+  if (!solver) return fail(-1, "null solver");
+  if (precision < LSB_PREC_FP32 || precision > LSB_PREC_FP64) return fail(-1, "unknown precision %d", precision);
+  if (stall_window < 0) return fail(-1, "stall_window must be >= 0");
+  solver->precision = precision;
+  solver->stall_window = stall_window;
+  return 0;
+}
+
 int lsb_solve(lsb_solver* solver, int batch, const float* d_lambda, const float* d_mu,
               const float* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,
               double* mean_sigma, float rtol, float atol, int maxiter, int rule, int* iters,
               int* status, double* residual) {
   g_last_error.clear();
-  if (!d_eps) return fail(-1, "d_eps must not be null");
-  return solve_impl(solver, batch, d_lambda, d_mu, eps_bar, d_eps0, d_eps, d_sigma, mean_sigma,
-                    rtol, atol, maxiter, rule, iters, status, residual);
+  if (!eps_bar) return fail(-1, "null argument");
+  if (batch < 1 || (solver && batch > solver->batch_cap)) return fail(-1, "batch %d out of range", batch);
+  std::vector<double> eb(eps_bar, eps_bar + 6 * batch);
+  return solve_f32(solver, batch, d_lambda, d_mu, eb.data(), d_eps0, d_eps, d_sigma, mean_sigma,
+                   rtol, atol, maxiter, rule, iters, status, residual);
+}
+
+int lsb_solve_f64(lsb_solver* solver, int batch, const double* d_lambda, const double* d_mu,
+                  const double* eps_bar, const double* d_eps0, double* d_eps, double* d_sigma,
+                  double* mean_sigma, double rtol, double atol, int maxiter, int rule, int* iters,
+                  int* status, double* residual) {
+  g_last_error.clear();
+  return solve_f64(solver, batch, d_lambda, d_mu, eps_bar, d_eps0, d_eps, d_sigma, mean_sigma,
+                   rtol, atol, maxiter, rule, iters, status, residual);
 }
 
 long long lsb_kernel_launches(lsb_solver* solver) { return solver ? solver->launches : -1; }
@@ -350,36 +491,35 @@ int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const fl
   if (batch < 1 || batch > s->batch_cap) return fail(-1, "batch %d outside [1, %d]", batch, s->batch_cap);
   if (reps < 1) return fail(-1, "reps must be >= 1");
   const GridDesc& g = s->g;
-  const LaunchShape& sh = s->shape;
+  const LaunchShape& sh = s->sh32;
   cudaStream_t st = s->stream;
-  SolveParams sp;
-  sp.rtol = 0.f;
-  sp.atol = 0.f;  // never converges: every pass does its full work
-  sp.maxiter = 0x3fffffff;
-  sp.rule = LSB_RULE_CUDA;
-  sp.inv_nv = (float)(1.0 / (double)g.nv);
-  std::vector<float> eb(6 * batch, 0.f);
-  for (int b = 0; b < batch; ++b) eb[6 * b + (b % 6)] = 1.f;
-  if (ensure_history(s, 1)) return -3;
-  LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eb.data(), sizeof(float) * eb.size(), cudaMemcpyHostToDevice, st));
-  launch_reset_state(batch, s->d_state, st);
-  launch_medium(g.nv, d_lambda, d_mu, s->d_mm_scratch, s->d_medium, st);
-  launch_zpass(g, sh, 0, batch, d_lambda, d_mu, d_eps, s->d_spec, s->d_epsbar, nullptr, s->d_state, sp, st);
-  launch_ypass(g, sh, false, batch, s->d_spec, s->d_state, st);
+  // tolerances 0 and no stall detection: every pass does its full work
+  SolveParams sp = make_params(s, 0.0, 0.0, 0x3fffffff, LSB_RULE_CUDA);
+  sp.precision = kPrecFP32;
+  sp.stall_window = 0;
+  std::vector<double> eb(6 * batch, 0.0);
+  for (int b = 0; b < batch; ++b) eb[6 * b + (b % 6)] = 1.0;
+  LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eb.data(), sizeof(double) * eb.size(), cudaMemcpyHostToDevice, st));
+  launch_reset_state(batch, 0, s->d_state, st);
+  launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  launch_zpass<float>(g, sh, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, s->d_epsbar, nullptr,
+                      s->d_state, s->d_medium, st);
+  launch_ypass<float>(g, sh, false, batch, s->d_spec32, s->d_state, st);
   cudaEvent_t ev[6];
   for (auto& e : ev) LSB_CUDA(cudaEventCreate(&e));
   double acc[5] = {0, 0, 0, 0, 0};
   for (int r = 0; r < reps; ++r) {
     cudaEventRecord(ev[0], st);
-    launch_xpass(g, sh, batch, s->d_spec, s->d_medium, s->d_state, s->d_partials, st);
+    launch_xpass<float>(g, sh, batch, s->d_spec32, s->d_medium, s->d_state, s->d_partials, st);
     cudaEventRecord(ev[1], st);
-    launch_finalize(g, sh, batch, s->d_state, s->d_partials, nullptr, 0, sp, st);
+    launch_finalize(sh, 0, batch, s->d_state, s->d_partials, nullptr, 0, sp, st);
     cudaEventRecord(ev[2], st);
-    launch_ypass(g, sh, true, batch, s->d_spec, s->d_state, st);
+    launch_ypass<float>(g, sh, true, batch, s->d_spec32, s->d_state, st);
     cudaEventRecord(ev[3], st);
-    launch_zpass(g, sh, 1, batch, d_lambda, d_mu, d_eps, s->d_spec, s->d_epsbar, nullptr, s->d_state, sp, st);
+    launch_zpass<float>(g, sh, 1, batch, d_lambda, d_mu, d_eps, s->d_spec32, s->d_epsbar, nullptr,
+                        s->d_state, s->d_medium, st);
     cudaEventRecord(ev[4], st);
-    launch_ypass(g, sh, false, batch, s->d_spec, s->d_state, st);
+    launch_ypass<float>(g, sh, false, batch, s->d_spec32, s->d_state, st);
     cudaEventRecord(ev[5], st);
     LSB_CUDA(cudaEventSynchronize(ev[5]));
     for (int k = 0; k < 5; ++k) {
@@ -403,7 +543,7 @@ int lsb_history(lsb_solver* solver, double* out, int len) {
   return 0;
 }
 
-int lsb_c_eff(const float* lambda, const float* mu, const int voxels[3], const float extents[3],
+int lsb_c_eff(const float* lambda, const float* mu, const int voxels[3], const double extents[3],
               float rtol, float atol, int maxiter, int depth, double* c_eff, int* iters) {
   g_last_error.clear();
   if (!lambda || !mu || !c_eff || !iters) return fail(-1, "null argument");
@@ -423,11 +563,11 @@ int lsb_c_eff(const float* lambda, const float* mu, const int voxels[3], const f
   }
   cudaMemcpy(d_l, lambda, sizeof(float) * nv, cudaMemcpyHostToDevice);
   cudaMemcpy(d_m, mu, sizeof(float) * nv, cudaMemcpyHostToDevice);
-  float eb[36] = {0};
-  for (int k = 0; k < 6; ++k) eb[6 * k + k] = 1.f;
+  double eb[36] = {0};
+  for (int k = 0; k < 6; ++k) eb[6 * k + k] = 1.0;
   int status[6];
-  rc = solve_impl(s, 6, d_l, d_m, eb, nullptr, s->d_eps, nullptr, c_eff, rtol, atol, maxiter,
-                  LSB_RULE_CUDA, iters, status, nullptr);
+  rc = solve_f32(s, 6, d_l, d_m, eb, nullptr, s->d_eps32, nullptr, c_eff, rtol, atol, maxiter,
+                 LSB_RULE_CUDA, iters, status, nullptr);
   cleanup();
   return rc;
 }
@@ -448,15 +588,16 @@ int lippmann_schwinger_solve(float* lambda, float* mu, float* epsilon_bar, float
   std::lock_guard<std::mutex> lock(c.mu);
   int dev = 0;
   cudaGetDevice(&dev);
+  const double ext[3] = {extents[0], extents[1], extents[2]};
   bool same = c.solver && c.solver->device == dev &&
               std::memcmp(c.voxels, voxels, sizeof(c.voxels)) == 0 &&
-              std::memcmp(c.extents, extents, sizeof(c.extents)) == 0;
+              std::memcmp(c.extents, ext, sizeof(c.extents)) == 0;
   if (!same) {
     c.release();
-    int rc = create_impl(&c.solver, voxels, extents, 1, 0);
+    int rc = create_impl(&c.solver, voxels, ext, 1, 0);
     if (rc) return rc;
     std::memcpy(c.voxels, voxels, sizeof(c.voxels));
-    std::memcpy(c.extents, extents, sizeof(c.extents));
+    std::memcpy(c.extents, ext, sizeof(c.extents));
     c.nv = (size_t)c.solver->g.nv;
     if (cudaMalloc(&c.d_lame, sizeof(float) * 2 * c.nv) != cudaSuccess ||
         cudaMalloc(&c.d_fields, sizeof(float) * 12 * c.nv) != cudaSuccess) {
@@ -470,9 +611,11 @@ int lippmann_schwinger_solve(float* lambda, float* mu, float* epsilon_bar, float
   LSB_CUDA(cudaMemcpyAsync(c.d_lame + nv, mu, sizeof(float) * nv, cudaMemcpyHostToDevice, st));
   int it = 0, status = 0;
   double e = 0.0;
-  int rc = solve_impl(c.solver, 1, c.d_lame, c.d_lame + nv, epsilon_bar, nullptr, c.d_fields,
-                      c.d_fields + 6 * nv, nullptr, rtol, atol, maxiter, LSB_RULE_CUDA, &it,
-                      &status, &e);
+  double eb[6];
+  for (int k = 0; k < 6; ++k) eb[k] = epsilon_bar[k];
+  int rc = solve_f32(c.solver, 1, c.d_lame, c.d_lame + nv, eb, nullptr, c.d_fields,
+                     c.d_fields + 6 * nv, nullptr, rtol, atol, maxiter, LSB_RULE_CUDA, &it,
+                     &status, &e);
   if (rc) return rc;
   LSB_CUDA(cudaMemcpyAsync(epsilon, c.d_fields, sizeof(float) * 6 * nv, cudaMemcpyDeviceToHost, st));
   LSB_CUDA(cudaMemcpyAsync(sigma, c.d_fields + 6 * nv, sizeof(float) * 6 * nv, cudaMemcpyDeviceToHost, st));
@@ -484,7 +627,7 @@ int lippmann_schwinger_solve(float* lambda, float* mu, float* epsilon_bar, float
     if (verbose > 1) {
       printf("==== Lippmann Schwinger solver ====\n");
       printf("  iteration           ||r||   ||r||/||r_0||\n");
-      for (int i = 0; i <= it && i < (int)hist.size(); ++i)
+      for (int i = 0; i < (int)hist.size() && (i == 0 || hist[i] != 0.0); ++i)
         printf("     %4d          %8.4e  %8.4e\n", i, hist[i], hist[i] / e0);
       printf("  ");
     } else {

@@ -1,9 +1,9 @@
 // Shared host/device types of the Lippmann-Schwinger solver library.
 //
 // Layouts (all row-major, last index fastest):
-//   real fields      eps, sigma, r       [batch][6][nx][ny][nz]            float
-//   Lame fields      lambda, mu          [nx][ny][nz]                      float
-//   spectrum         S                   [batch][6][nx][ny][nzh], nzh = nz/2+1   float2
+//   real fields      eps, sigma, r       [batch][6][nx][ny][nz]            float or double
+//   Lame fields      lambda, mu          [nx][ny][nz]                      float or double
+//   spectrum         S                   [batch][6][nx][ny][nzh], nzh = nz/2+1   float2 or double2
 // The spectrum layout is that of a cuFFT R2C transform of batch 6 over z-fastest
 // fields (cuda/src/lippmann_schwinger.cu:117-120 in the reference). Voigt order is
 // (xx, yy, zz, xy, xz, yz) with tensor shear entries.
@@ -15,18 +15,40 @@
 
 namespace lsb {
 
-constexpr int kMaxStages = 20;   // radix stages of one 1-D transform
-constexpr int kMaxDim = 1024;    // largest supported extent along any axis
-constexpr int kMaxThreads = 384;  // largest block of the FFT passes (6144 values / 16 per thread)
+constexpr int kMaxStages = 20;    // radix stages of one 1-D transform
+constexpr int kMaxDim = 1024;     // largest supported extent along any axis
+constexpr int kMaxThreads = 384;  // largest block of the FFT passes
+
+template <typename T>
+struct Complex;
+template <>
+struct Complex<float> {
+  using type = float2;
+};
+template <>
+struct Complex<double> {
+  using type = double2;
+};
+template <typename T>
+using cplx = typename Complex<T>::type;
 
 // Mixed-radix Stockham plan for complex transforms of length n.
-// tw[k] = exp(-2 pi i k / n), k in [0, n), computed in FP64 on the host.
+// tw[k] = exp(-2 pi i k / n), k in [0, n), computed in FP64 on the host and stored in
+// both precisions.
 struct Plan1D {
   int n;
   int nst;
   int radix[kMaxStages];
   const float2* tw;
+  const double2* tw64;
 };
+
+template <typename T>
+__host__ __device__ inline const cplx<T>* twiddles(const Plan1D& p);
+template <>
+__host__ __device__ inline const float2* twiddles<float>(const Plan1D& p) { return p.tw; }
+template <>
+__host__ __device__ inline const double2* twiddles<double>(const Plan1D& p) { return p.tw64; }
 
 struct GridDesc {
   int nx, ny, nz, nzh;
@@ -43,38 +65,69 @@ struct GridDesc {
   const double* cz;
 };
 
-// Reference medium, derived on the device from min/max of the Lame fields.
+// Reference medium, derived on the device from min/max of the Lame fields
+// (lambda0 = (min + max) / 2, evaluated in the precision of the iteration).
 struct Medium {
-  float lambda0, mu0;
-  float c_a;   // -1/mu0
-  float c_b;   // (lambda0+mu0) / (mu0 (lambda0 + 2 mu0))
-  float lmin, lmax, mmin, mmax;
+  double lmin, lmax, mmin, mmax;
+  double lmean, mmean;    // FP64 means of the Lame fields
+  float lambda0, mu0;     // FP32 iteration
+  float c_a, c_b;         // -1/mu0 and (lambda0+mu0) / (mu0 (lambda0 + 2 mu0))
+  double lambda0_64, mu0_64, c_a64, c_b64;  // FP64 iteration
 };
+
+template <typename T>
+__device__ inline T medium_ca(const Medium& m);
+template <>
+__device__ inline float medium_ca<float>(const Medium& m) { return m.c_a; }
+template <>
+__device__ inline double medium_ca<double>(const Medium& m) { return m.c_a64; }
+template <typename T>
+__device__ inline T medium_cb(const Medium& m);
+template <>
+__device__ inline float medium_cb<float>(const Medium& m) { return m.c_b; }
+template <>
+__device__ inline double medium_cb<double>(const Medium& m) { return m.c_b64; }
 
 enum Status : int {
   kRunning = 0,
   kConverged = 1,
   kMaxIter = 2,
   kNonFinite = 3,
+  kStalled = 4,   // FP32 round-off floor reached above the tolerance (FP32-only mode)
 };
 
 // Per-instance iteration state, owned by the device.
 struct InstanceState {
-  int iter;      // updates performed
-  int done;      // nonzero once the instance has stopped
-  int status;    // Status
-  int evals;     // criterion evaluations performed
-  double e0;     // criterion at the first iterate
-  double e;      // last criterion value
+  int iter;       // updates performed
+  int done;       // nonzero once the instance has stopped
+  int status;     // Status
+  int evals;      // criterion evaluations performed
+  int phase;      // 0: FP32 fields, 1: FP64 fields
+  int best_eval;  // evaluation at which best_e last improved significantly
+  int switched;   // 1 once the instance moved from FP32 to FP64
+  int pad;
+  double e0;      // criterion at the first iterate
+  double e;       // last criterion value
+  double best_e;  // smallest criterion value seen in the current phase
   double sig0[12];  // zero mode of sigma_hat (6 complex) at the last evaluation
+  // Per-component constant subtracted from sigma before the forward transform. Keeping
+  // the near-mean out of the transform keeps the round-off of the lines that carry the
+  // zero frequency at the level of the stress fluctuation; the zero mode is restored in
+  // FP64 (sig0), and Gamma^0 and xi vanish there, so nothing else depends on it.
+  double shift[6];
 };
 
+enum Precision : int { kPrecFP32 = 0, kPrecMixed = 1, kPrecFP64 = 2 };
+
 struct SolveParams {
-  float rtol, atol;
+  double rtol, atol;
   int maxiter;
-  int rule;       // 0: stop when e <  max(rtol e0, atol)  (C ABI rule)
-                  // 1: stop when e <= max(rtol e0, atol)  (jax-signature rule)
-  float inv_nv;   // 1 / voxels
+  int rule;         // 0: stop when e <  max(rtol e0, atol); 1: stop when e <= ...
+  long long nv;     // voxels
+  int precision;    // Precision
+  int stall_window;       // evaluations without a significant improvement => stalled
+  double stall_improve;   // significant improvement: e < stall_improve * best_e
+  double stall_near;      // stall is only declared while best_e < stall_near * threshold
 };
 
 }  // namespace lsb

@@ -1,3 +1,3 @@
 from .lippmann_schwinger import (  # noqa: F401
-    CONVERGED, MAXITER, NONFINITE, RULE_CUDA, RULE_JAX, Solver, SolveResult, c_eff,
+    CONVERGED, MAXITER, NONFINITE, PRECISIONS, STALLED, RULE_CUDA, RULE_JAX, Solver, SolveResult, c_eff,
     lippmann_schwinger, lippmann_schwinger_cuda, lippmann_schwinger_jax)

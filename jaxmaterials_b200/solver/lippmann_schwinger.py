@@ -35,12 +35,14 @@ __all__ = [
     "CONVERGED",
     "MAXITER",
     "NONFINITE",
+    "STALLED",
     "RULE_CUDA",
     "RULE_JAX",
 ]
 
-CONVERGED, MAXITER, NONFINITE = 1, 2, 3
+CONVERGED, MAXITER, NONFINITE, STALLED = 1, 2, 3, 4
 RULE_CUDA, RULE_JAX = 0, 1
+PRECISIONS = {"fp32": 0, "mixed": 1, "fp64": 2}
 
 
 def _fptr(a):
@@ -103,7 +105,7 @@ class Solver:
     optionally the warm start). Uses the current CUDA device and torch's current stream.
     """
 
-    def __init__(self, grid_spec, batch=1, depth=0):
+    def __init__(self, grid_spec, batch=1, depth=0, precision="mixed", stall_window=8):
         import torch
 
         if not torch.cuda.is_available():
@@ -113,13 +115,23 @@ class Solver:
         self.batch = int(batch)
         self.depth = int(depth)
         self.device = torch.device("cuda", torch.cuda.current_device())
-        voxels, extents = _grid_args(grid_spec)
+        voxels, _ = _grid_args(grid_spec)
+        extents = np.array([grid_spec.Lx, grid_spec.Ly, grid_spec.Lz], dtype=np.float64)
         h = ctypes.c_void_p()
         _lib.check(self._lib.lsb_create(ctypes.byref(h), voxels.ctypes.data_as(_lib.c_int_p),
-                                        _fptr(extents), self.batch, self.depth), "lsb_create")
+                                        extents.ctypes.data_as(_lib.c_double_p), self.batch,
+                                        self.depth), "lsb_create")
         self._h = h
         self._last_batch = 0
         self._last_maxiter = 0
+        self.set_precision(precision, stall_window)
+
+    def set_precision(self, precision="mixed", stall_window=8):
+        """Field precision: "fp32", "mixed" (FP32, FP64 once FP32 round-off stalls the
+        criterion near the tolerance) or "fp64"."""
+        _lib.check(self._lib.lsb_set_precision(self._h, PRECISIONS[precision], int(stall_window)),
+                   "lsb_set_precision")
+        self.precision = precision
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -132,32 +144,38 @@ class Solver:
         except Exception:
             pass
 
-    def _as_device(self, a, shape):
+    def _as_device(self, a, shape, dtype=None):
         import torch
 
-        t = torch.as_tensor(a, dtype=torch.float32, device=self.device)
+        t = torch.as_tensor(a, dtype=dtype or torch.float32, device=self.device)
         t = t.contiguous()
         if tuple(t.shape) != tuple(shape):
             raise ValueError(f"expected shape {tuple(shape)}, got {tuple(t.shape)}")
         return t
 
     def solve(self, lmbda, mu, epsilon_bar, rtol=1e-6, atol=1e-20, maxiter=32,
-              rule=RULE_CUDA, epsilon0=None, want_sigma=True, out=None):
-        """Run the fixed point for every row of ``epsilon_bar`` (shape (B, 6) or (6,))."""
+              rule=RULE_CUDA, epsilon0=None, want_sigma=True, out=None, dtype=np.float32):
+        """Run the fixed point for every row of ``epsilon_bar`` (shape (B, 6) or (6,)).
+
+        ``dtype=np.float64`` runs FP64 fields end to end (inputs and outputs in FP64)."""
         import torch
 
+        f64 = np.dtype(dtype) == np.float64
+        tdt = torch.float64 if f64 else torch.float32
         g = self.grid_spec
         nshape = (g.nx, g.ny, g.nz)
-        eb = np.ascontiguousarray(np.atleast_2d(np.asarray(epsilon_bar, dtype=np.float32)))
+        eb = np.ascontiguousarray(np.atleast_2d(np.asarray(
+            epsilon_bar.cpu() if isinstance(epsilon_bar, torch.Tensor) else epsilon_bar,
+            dtype=np.float64 if f64 else np.float32)))
         b = eb.shape[0]
         if eb.shape[1] != 6 or b < 1 or b > self.batch:
             raise ValueError(f"epsilon_bar must have shape (B, 6) with 1 <= B <= {self.batch}")
-        lm = self._as_device(lmbda, nshape)
-        m = self._as_device(mu, nshape)
+        lm = self._as_device(lmbda, nshape, tdt)
+        m = self._as_device(mu, nshape, tdt)
         e0 = None
         if epsilon0 is not None:
-            e0 = self._as_device(epsilon0, (b, 6) + nshape)
-        eps = out if out is not None else torch.empty((b, 6) + nshape, dtype=torch.float32,
+            e0 = self._as_device(epsilon0, (b, 6) + nshape, tdt)
+        eps = out if out is not None else torch.empty((b, 6) + nshape, dtype=tdt,
                                                       device=self.device)
         sig = torch.empty_like(eps) if want_sigma else None
         iters = np.zeros(b, dtype=np.int32)
@@ -166,15 +184,17 @@ class Solver:
         mean = np.zeros((b, 6), dtype=np.float64)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._lib.lsb_set_stream(self._h, ctypes.c_void_p(stream)), "lsb_set_stream")
-        rc = self._lib.lsb_solve(
+        fn = self._lib.lsb_solve_f64 if f64 else self._lib.lsb_solve
+        ebp = eb.ctypes.data_as(_lib.c_double_p) if f64 else _fptr(eb)
+        rc = fn(
             self._h, b, ctypes.c_void_p(lm.data_ptr()), ctypes.c_void_p(m.data_ptr()),
-            _fptr(eb), ctypes.c_void_p(e0.data_ptr() if e0 is not None else 0),
+            ebp, ctypes.c_void_p(e0.data_ptr() if e0 is not None else 0),
             ctypes.c_void_p(eps.data_ptr()),
             ctypes.c_void_p(sig.data_ptr() if sig is not None else 0),
             mean.ctypes.data_as(_lib.c_double_p), float(rtol), float(atol), int(maxiter),
             int(rule), iters.ctypes.data_as(_lib.c_int_p), status.ctypes.data_as(_lib.c_int_p),
             resid.ctypes.data_as(_lib.c_double_p))
-        _lib.check(rc, "lsb_solve")
+        _lib.check(rc, "lsb_solve_f64" if f64 else "lsb_solve")
         self._last_batch = b
         self._last_maxiter = int(maxiter)
         return SolveResult(eps, sig, iters, status, resid, mean)
@@ -229,27 +249,29 @@ def _cached_solver(grid_spec, batch, depth):
 
 
 def lippmann_schwinger(lmbda, mu, epsilon_bar, grid_spec, rtol=1e-6, atol=1e-20, depth=0,
-                       maxiter=32, dtype=np.float32, epsilon0=None):
+                       maxiter=32, dtype=np.float32, epsilon0=None, precision=None):
     """Signature of the reference ``lippmann_schwinger_jax`` (``:146-265``).
 
     Returns ``(epsilon, sigma, iter)`` with fields of shape (6, nx, ny, nz): NumPy arrays
     for NumPy input, CUDA tensors for torch input. Stops when
     e <= max(rtol e0, atol) or after ``maxiter`` updates, without raising (as the
-    reference). Fields are FP32; norms and the stop decision are FP64.
+    reference). ``dtype`` float32 runs FP32 fields (mixed precision: FP64 fields take
+    over if FP32 round-off stalls the criterion near the tolerance; ``precision="fp32"``
+    disables that); float64 runs FP64 fields. Norms and the stop decision are FP64.
     """
-    if np.dtype(dtype) != np.float32:
-        raise NotImplementedError("the CUDA solver carries FP32 fields (dtype=float32)")
     import torch
 
+    f64 = np.dtype(dtype) == np.float64
     as_torch = isinstance(lmbda, torch.Tensor)
     s = _cached_solver(grid_spec, 1, depth)
+    s.set_precision(precision or ("fp64" if f64 else "mixed"))
     e0 = None if epsilon0 is None else (
         epsilon0.reshape((1, 6) + grid_spec.shape) if as_torch
-        else np.asarray(epsilon0, np.float32).reshape((1, 6) + grid_spec.shape))
+        else np.asarray(epsilon0).reshape((1, 6) + grid_spec.shape))
     eb = np.asarray(epsilon_bar.cpu() if isinstance(epsilon_bar, torch.Tensor) else epsilon_bar,
-                    dtype=np.float32).reshape(1, 6)
+                    dtype=np.float64).reshape(1, 6)
     r = s.solve(lmbda, mu, eb, rtol=rtol, atol=atol, maxiter=maxiter, rule=RULE_JAX,
-                epsilon0=e0)
+                epsilon0=e0, dtype=np.float64 if f64 else np.float32)
     eps, sig = r.epsilon[0], r.sigma[0]
     if not as_torch:
         eps, sig = eps.cpu().numpy(), sig.cpu().numpy()
@@ -259,11 +281,14 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid_spec, rtol=1e-6, atol=1e-20,
 lippmann_schwinger_jax = lippmann_schwinger
 
 
-def c_eff(lmbda, mu, grid_spec, rtol=1e-6, atol=1e-20, maxiter=1000, depth=0, solver=None):
+def c_eff(lmbda, mu, grid_spec, rtol=1e-6, atol=1e-20, maxiter=1000, depth=0, solver=None,
+          precision="mixed"):
     """Effective stiffness: row k = mean stress for the unit strain e_k (tensor shear).
 
     Solves the six load cases as one batch. Returns ``(C, iters, result)``."""
     s = solver if solver is not None else _cached_solver(grid_spec, 6, depth)
+    if solver is None:
+        s.set_precision(precision)
     r = s.solve(lmbda, mu, np.eye(6, dtype=np.float32), rtol=rtol, atol=atol,
                 maxiter=maxiter, rule=RULE_CUDA, want_sigma=False)
     return r.mean_sigma.copy(), r.iters.copy(), r

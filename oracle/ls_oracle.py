@@ -88,6 +88,25 @@ def get_xizero(grid, dtype=np.float64):
     return (xi / nrm).astype(dtype)
 
 
+def get_xizero_cuda32(grid, dtype=np.float32):
+    """Normalised wave vectors as the reference CUDA library builds them: FP32 sin/cos of
+    pi k/N, FP32 norm, norms below 1e-6 replaced by 1 (``cuda/src/fourier.cu:47-77``).
+    On even grids the modes with two Nyquist indices get |xi| ~ 1e-5 from FP32 round-off
+    and pass this guard, so the reference CUDA applies a nonzero Gamma^0 there, unlike
+    the Python path (``get_xizero``)."""
+    # xi_d / 2 = M_PI * k / N evaluated in double and stored as float
+    h = [(np.pi * np.arange(m) / m).astype(np.float32) for m in grid.shape]
+    x = np.meshgrid(*h, indexing="ij")
+    s = [np.sin(v).astype(np.float32) for v in x]
+    c = [np.cos(v).astype(np.float32) for v in x]
+    sc = [np.float32(2 * n) / np.float32(ln)
+          for n, ln in zip(grid.shape, (grid.Lx, grid.Ly, grid.Lz))]
+    t = [sc[0] * s[0] * c[1] * c[2], sc[1] * c[0] * s[1] * c[2], sc[2] * c[0] * c[1] * s[2]]
+    nrm = np.sqrt(t[0] ** 2 + t[1] ** 2 + t[2] ** 2).astype(np.float32)
+    nrm[nrm < 1.0e-6] = 1.0
+    return np.stack([v / nrm for v in t]).astype(dtype)
+
+
 def half(a, grid):
     """Restrict a full-spectrum array to the R2C half spectrum k_z in [0, nz/2]."""
     return a[..., : grid.nz // 2 + 1]
@@ -234,7 +253,7 @@ def lame_reference(lmbda, mu):
 
 def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, depth=0,
                        maxiter=32, dtype=np.float32, spectrum="half", workers=None,
-                       epsilon0=None, history=None):
+                       epsilon0=None, history=None, xizero_fn=None):
     """Moulinec-Suquet fixed point with Anderson acceleration of depth ``depth``
     (``src/jaxmaterials/solver/lippmann_schwinger.py:146-265``).
 
@@ -242,6 +261,8 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
     ``spectrum="half"`` uses R2C/C2R transforms (same fixed point, half the work).
     ``epsilon0`` optionally replaces the cold start eps = epsilon_bar by a warm start.
     ``history``, if a list, receives the criterion value after every evaluation.
+    ``xizero_fn(grid, dtype)`` replaces ``get_xizero`` (e.g. ``get_xizero_cuda32`` for
+    the reference CUDA library's construction).
 
     Returns ``(epsilon, sigma, iterations)`` with sigma = sigma(epsilon); the loop stops
     when e <= atol or e <= rtol * e0 (e0 at the first iterate) or after maxiter updates.
@@ -252,7 +273,7 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
     lmbda = np.asarray(lmbda, dtype=dtype)
     mu = np.asarray(mu, dtype=dtype)
     lmbda0, mu0 = lame_reference(lmbda, mu)
-    xizero = get_xizero(grid, dtype=dtype)
+    xizero = (xizero_fn or get_xizero)(grid, dtype=dtype)
     xi = get_xi(grid, dtype=dtype)
     if spectrum == "half":
         xizero = half(xizero, grid)
