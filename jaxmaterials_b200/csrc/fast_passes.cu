@@ -1,0 +1,487 @@
+// FP32 passes for power-of-two axis lengths (16..256) with compile-time sizes.
+//
+// Each 1-D transform of length N = E * P is a four-step FFT spread over P threads:
+// thread p holds x[p + P e] (e < E), does the E-point DFT in registers, multiplies by
+// exp(-2 pi i p k1 / N), writes its E values to shared memory transposed, and after one
+// barrier each thread gathers P values of one k1 and finishes with the P-point DFT,
+// producing X[k1 + E k2]. One shared-memory round trip per transform, no runtime index
+// division, and the y and x passes read and write global memory in coalesced rows.
+// Semantics are those of the generic passes in ls_kernels.cu (same layouts, shift of the
+// forward transform, criterion partials, Gamma^0), which remain the path for every other
+// size and for FP64 fields.
+#include <cmath>
+
+#include "fast_passes.cuh"
+#include "fft_smem.cuh"
+
+namespace lsb {
+namespace fast {
+
+template <int N>
+struct Split;
+template <>
+struct Split<16> { static constexpr int E = 4, P = 4; };
+template <>
+struct Split<32> { static constexpr int E = 8, P = 4; };
+template <>
+struct Split<64> { static constexpr int E = 8, P = 8; };
+template <>
+struct Split<128> { static constexpr int E = 16, P = 8; };
+template <>
+struct Split<256> { static constexpr int E = 16, P = 16; };
+
+__device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y); }
+
+__device__ __forceinline__ bool active32(const InstanceState& s) { return !s.done && s.phase == 0; }
+
+// Step A of the four-step transform: DFT over e of v[e] = x[p + P e], then the twiddle.
+template <int N>
+__device__ __forceinline__ void step_a(float2* v, int p, const float2* __restrict__ tw) {
+  constexpr int E = Split<N>::E;
+  Bfly<E>::run(v);
+  if (p > 0) {
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) v[k1] = cmul(v[k1], __ldg(tw + p * k1));
+  }
+}
+
+// ----------------------------------------------------------------------------- y pass
+// Block = (16 kz columns, x, instance * 6 + component); thread (p, t), t fastest.
+constexpr int kYT = 16;
+
+template <int NY>
+__global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (kYT * Split<NY>::P)) ypass_fast(GridDesc g, int inverse,
+                                                               float2* __restrict__ spec,
+                                                               const InstanceState* __restrict__ st) {
+  constexpr int E = Split<NY>::E, P = Split<NY>::P;
+  __shared__ float2 buf[NY * kYT];
+  const int bc = blockIdx.z;
+  if (!active32(st[bc / 6])) return;
+  const int t = threadIdx.x % kYT, p = threadIdx.x / kYT;
+  const int nzh = g.nzh;
+  const int kz = blockIdx.x * kYT + t;
+  const bool valid = kz < nzh;
+  float2* base = spec + ((size_t)bc * g.nx + blockIdx.y) * (size_t)NY * nzh + kz;
+  const float2* tw = g.py.tw;
+  float2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    float2 a = valid ? base[(size_t)(p + P * e) * nzh] : make_float2(0.f, 0.f);
+    v[e] = inverse ? conj2(a) : a;
+  }
+  step_a<NY>(v, p, tw);
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) buf[(k1 * P + p) * kYT + t] = v[k1];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < E / P; ++j) {
+    const int k1 = p + P * j;
+    float2 w[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) w[q] = buf[(k1 * P + q) * kYT + t];
+    Bfly<P>::run(w);
+    if (valid) {
+#pragma unroll
+      for (int k2 = 0; k2 < P; ++k2) base[(size_t)(k1 + E * k2) * nzh] = inverse ? conj2(w[k2]) : w[k2];
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- x pass
+// Block = (TX kz columns, ky, instance); thread (c, p, t) with t fastest.
+template <int NX>
+__host__ __device__ constexpr int x_cols() { return NX <= 32 ? 16 : (NX == 256 ? 4 : 8); }
+
+template <int NX>
+__global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast(
+    GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
+    InstanceState* __restrict__ st, double* __restrict__ partials) {
+  constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols<NX>();
+  extern __shared__ __align__(16) unsigned char xfraw[];
+  float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 * NX * T values
+  __shared__ double red[32];
+  const int b = blockIdx.z;
+  if (!active32(st[b])) return;
+  const int tid = threadIdx.x;
+  const int t = tid % T, p = (tid / T) % P, c = tid / (T * P);
+  const int ky = blockIdx.y;
+  const int kz0 = blockIdx.x * T;
+  const int kz = kz0 + t;
+  const int nzh = g.nzh;
+  const bool valid = kz < nzh;
+  const size_t xstride = (size_t)g.ny * nzh;
+  float2* gcol = spec + (size_t)b * 6 * g.nm + (size_t)c * g.nm + (size_t)ky * nzh + kz;
+  const float2* tw = g.px.tw;
+  float2* tr = buf + (size_t)c * NX * T;   // this component's region
+
+  // forward: load, step A, transpose
+  float2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = valid ? gcol[(size_t)(p + P * e) * xstride] : make_float2(0.f, 0.f);
+  step_a<NX>(v, p, tw);
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) tr[(k1 * P + p) * T + t] = v[k1];
+  __syncthreads();
+  float2 o[E];  // outputs X[k1 + E k2] for k1 = p + P j: o[j * P + k2]
+#pragma unroll
+  for (int j = 0; j < E / P; ++j) {
+    const int k1 = p + P * j;
+    float2 w[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) w[q] = tr[(k1 * P + q) * T + t];
+    Bfly<P>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) o[j * P + k2] = w[k2];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < E / P; ++j)
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) tr[((p + P * j) + E * k2) * T + t] = o[j * P + k2];
+  __syncthreads();
+
+  // residual partials, zero mode, Gamma^0 (written conjugated for the inverse transform)
+  const float c_a = med->c_a, c_b = med->c_b;
+  const double sxs = 2.0 * g.nx / g.Lx, sys = 2.0 * g.ny / g.Ly, szs = 2.0 * g.nz / g.Lz;
+  double acc = 0.0;
+  for (int idx = tid; idx < NX * T; idx += blockDim.x) {
+    const int kx = idx / T, tt = idx % T;
+    const int kzz = kz0 + tt;
+    if (kzz >= nzh) continue;
+    float2 s[6];
+#pragma unroll
+    for (int cc = 0; cc < 6; ++cc) s[cc] = buf[((size_t)cc * NX + kx) * T + tt];
+    const double x0 = sxs * g.sx[kx] * g.cy[ky] * g.cz[kzz];
+    const double x1 = sys * g.cx[kx] * g.sy[ky] * g.cz[kzz];
+    const double x2 = szs * g.cx[kx] * g.cy[ky] * g.sz[kzz];
+    {
+      const float f0 = (float)x0, f1 = (float)x1, f2 = (float)x2;
+      float2 d0 = make_float2(f0 * s[0].x + f1 * s[3].x + f2 * s[4].x, f0 * s[0].y + f1 * s[3].y + f2 * s[4].y);
+      float2 d1 = make_float2(f0 * s[3].x + f1 * s[1].x + f2 * s[5].x, f0 * s[3].y + f1 * s[1].y + f2 * s[5].y);
+      float2 d2 = make_float2(f0 * s[4].x + f1 * s[5].x + f2 * s[2].x, f0 * s[4].y + f1 * s[5].y + f2 * s[2].y);
+      double m2 = (double)d0.x * d0.x + (double)d0.y * d0.y + (double)d1.x * d1.x +
+                  (double)d1.y * d1.y + (double)d2.x * d2.x + (double)d2.y * d2.y;
+      acc += ((kzz == 0 || 2 * kzz == g.nz) ? 1.0 : 2.0) * m2;
+    }
+    if (kx == 0 && ky == 0 && kzz == 0) {
+#pragma unroll
+      for (int cc = 0; cc < 6; ++cc) {
+        st[b].sig0[2 * cc] = (double)s[cc].x + (double)g.nv * st[b].shift[cc];
+        st[b].sig0[2 * cc + 1] = (double)s[cc].y;
+      }
+    }
+    double nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+    if (nrm < 1.0e-12) nrm = 1.0;
+    const float z0 = (float)(x0 / nrm), z1 = (float)(x1 / nrm), z2 = (float)(x2 / nrm);
+    const float z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
+    const float z01 = z0 * z1, z02 = z0 * z2, z12 = z1 * z2;
+    float r[2][6];
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      float t0 = part ? s[0].y : s[0].x, t1 = part ? s[1].y : s[1].x, t2 = part ? s[2].y : s[2].x;
+      float t3 = part ? s[3].y : s[3].x, t4 = part ? s[4].y : s[4].x, t5 = part ? s[5].y : s[5].x;
+      float rho = z00 * t0 + z11 * t1 + z22 * t2 + 2.f * (z01 * t3 + z02 * t4 + z12 * t5);
+      float a0 = z0 * (z0 * t0 + z2 * t4 + z1 * t3);
+      float a1 = z1 * (z1 * t1 + z2 * t5 + z0 * t3);
+      float a2 = z2 * (z2 * t2 + z1 * t5 + z0 * t4);
+      float a3 = 0.5f * (z01 * (t0 + t1) + (z00 + z11) * t3 + z2 * (z0 * t5 + z1 * t4));
+      float a4 = 0.5f * (z02 * (t0 + t2) + (z00 + z22) * t4 + z1 * (z0 * t5 + z2 * t3));
+      float a5 = 0.5f * (z12 * (t1 + t2) + (z11 + z22) * t5 + z0 * (z1 * t4 + z2 * t3));
+      r[part][0] = c_a * a0 + c_b * rho * z00;
+      r[part][1] = c_a * a1 + c_b * rho * z11;
+      r[part][2] = c_a * a2 + c_b * rho * z22;
+      r[part][3] = c_a * a3 + c_b * rho * z01;
+      r[part][4] = c_a * a4 + c_b * rho * z02;
+      r[part][5] = c_a * a5 + c_b * rho * z12;
+    }
+#pragma unroll
+    for (int cc = 0; cc < 6; ++cc) buf[((size_t)cc * NX + kx) * T + tt] = make_float2(r[0][cc], -r[1][cc]);
+  }
+  __syncthreads();
+
+  // inverse (forward transform of the conjugate): step A from the natural layout
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = tr[(p + P * e) * T + t];
+  step_a<NX>(v, p, tw);
+  __syncthreads();
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) tr[(k1 * P + p) * T + t] = v[k1];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < E / P; ++j) {
+    const int k1 = p + P * j;
+    float2 w[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) w[q] = tr[(k1 * P + q) * T + t];
+    Bfly<P>::run(w);
+    if (valid) {
+#pragma unroll
+      for (int k2 = 0; k2 < P; ++k2) gcol[(size_t)(k1 + E * k2) * xstride] = conj2(w[k2]);
+    }
+  }
+
+  // deterministic block reduction of the residual partial
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((tid & 31) == 0) red[tid >> 5] = acc;
+  __syncthreads();
+  if (tid < 32) {
+    double w = (tid < (int)(blockDim.x + 31) / 32) ? red[tid] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) w += __shfl_xor_sync(0xffffffffu, w, off);
+    if (tid == 0) {
+      const int nblk = gridDim.x * gridDim.y;
+      partials[(size_t)b * nblk + blockIdx.y * gridDim.x + blockIdx.x] = w;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- z pass
+// Block = L (x, y) lines = 3L complex pair lines; thread (line q, p), p fastest.
+template <int NZ>
+__host__ __device__ constexpr int z_lines() { return 128 / Split<NZ>::P; }
+template <int NZ>
+__host__ __device__ constexpr int z_ld() { return NZ + (Split<NZ>::P == 4 ? 4 : 8); }
+
+// In-place four-step FFT of the 3L lines of zbuf (natural order in and out).
+template <int NZ>
+__device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const float2* __restrict__ tw) {
+  constexpr int E = Split<NZ>::E, P = Split<NZ>::P, LD = z_ld<NZ>();
+  float2* line = zbuf + (size_t)q * LD;
+  float2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = line[p + P * e];
+  step_a<NZ>(v, p, tw);
+  __syncthreads();
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) line[k1 * P + p] = v[k1];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < E / P; ++j) {
+    const int k1 = p + P * j;
+    float2 w[P];
+#pragma unroll
+    for (int qq = 0; qq < P; ++qq) w[qq] = line[k1 * P + qq];
+    Bfly<P>::run(w);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) v[j * P + k2] = w[k2];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < E / P; ++j)
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) line[(p + P * j) + E * k2] = v[j * P + k2];
+  __syncthreads();
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fast(
+    GridDesc g, int mode, const float* __restrict__ lambda, const float* __restrict__ mu,
+    float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
+    const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med) {
+  constexpr int P = Split<NZ>::P, L = z_lines<NZ>(), LD = z_ld<NZ>(), NZH = NZ / 2 + 1;
+  extern __shared__ __align__(16) unsigned char zfraw[];
+  float2* zbuf = reinterpret_cast<float2*>(zfraw);   // 3L lines of LD values
+  const int b = blockIdx.y;
+  if (!active32(st[b])) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int p = tid % P, q = tid / P;
+  const long long nlines = (long long)g.nx * g.ny;
+  const long long l0 = (long long)blockIdx.x * L;
+  float* eb = eps + (size_t)b * 6 * g.nv;
+  float2* sb = spec + (size_t)b * 6 * g.nm;
+  const float2* tw = g.pz.tw;
+
+  if (mode == 1) {
+    for (int idx = tid; idx < 3 * L * NZH; idx += nt) {
+      const int pr = idx / (L * NZH);
+      const int rem = idx - pr * (L * NZH);
+      const int l = rem / NZH, k = rem - l * NZH;
+      const long long line = l0 + l;
+      if (line >= nlines) continue;
+      float2 A = sb[((size_t)(2 * pr) * nlines + line) * NZH + k];
+      float2 B = sb[((size_t)(2 * pr + 1) * nlines + line) * NZH + k];
+      const bool selfconj = (k == 0) || (2 * k == NZ);
+      if (selfconj) { A.y = 0.f; B.y = 0.f; }
+      float2* Z = zbuf + (size_t)(pr * L + l) * LD;
+      Z[k] = make_float2(A.x - B.y, -(A.y + B.x));
+      if (!selfconj) Z[NZ - k] = make_float2(A.x + B.y, A.y - B.x);
+    }
+    __syncthreads();
+    zline_fft<NZ>(zbuf, q, p, tw);
+  }
+
+  float shift[6];
+  if (mode != 0) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) shift[c] = (float)st[b].shift[c];
+  } else {
+    const double* e = eps_bar + 6 * b;
+    const double tr = e[0] + e[1] + e[2];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+      shift[c] = (float)((c < 3 ? med->lmean * tr : 0.0) + 2.0 * med->mmean * e[c]);
+    if (blockIdx.x == 0 && tid == 0) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) st[b].shift[c] = (double)shift[c];
+    }
+  }
+
+  {
+    const float inv_nv = (float)(1.0 / (double)g.nv);
+    for (int idx = tid; idx < L * NZ; idx += nt) {
+      const int l = idx / NZ, n = idx % NZ;
+      const long long line = l0 + l;
+      if (line >= nlines) continue;
+      const size_t vx = (size_t)line * NZ + n;
+      float e[6];
+      if (mode == 1) {
+#pragma unroll
+        for (int pr = 0; pr < 3; ++pr) {
+          float2 w = zbuf[(size_t)(pr * L + l) * LD + n];
+          e[2 * pr] = eb[(size_t)(2 * pr) * g.nv + vx] + w.x * inv_nv;
+          e[2 * pr + 1] = eb[(size_t)(2 * pr + 1) * g.nv + vx] - w.y * inv_nv;
+        }
+      } else if (mode == 2) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * g.nv + vx];
+      } else if (eps0 != nullptr) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * g.nv + vx];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) e[c] = (float)eps_bar[b * 6 + c];
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + vx] = e[c];
+      const float lam = lambda[vx], tmu = 2.f * mu[vx];
+      const float ltr = lam * (e[0] + e[1] + e[2]);
+      float s[6];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
+#pragma unroll
+      for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+#pragma unroll
+      for (int pr = 0; pr < 3; ++pr)
+        zbuf[(size_t)(pr * L + l) * LD + n] =
+            make_float2(s[2 * pr] - shift[2 * pr], s[2 * pr + 1] - shift[2 * pr + 1]);
+    }
+  }
+  __syncthreads();
+  zline_fft<NZ>(zbuf, q, p, tw);
+
+  for (int idx = tid; idx < 3 * L * NZH; idx += nt) {
+    const int pr = idx / (L * NZH);
+    const int rem = idx - pr * (L * NZH);
+    const int l = rem / NZH, k = rem - l * NZH;
+    const long long line = l0 + l;
+    if (line >= nlines) continue;
+    const float2* Z = zbuf + (size_t)(pr * L + l) * LD;
+    const float2 zk = Z[k];
+    const float2 zm = Z[k == 0 ? 0 : NZ - k];
+    sb[((size_t)(2 * pr) * nlines + line) * NZH + k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    sb[((size_t)(2 * pr + 1) * nlines + line) * NZH + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+  }
+}
+
+// ----------------------------------------------------------------------------- host side
+static bool pow2_supported(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256; }
+
+bool supported(const GridDesc& g) {
+  return pow2_supported(g.nx) && pow2_supported(g.ny) && pow2_supported(g.nz);
+}
+
+template <int N>
+static int x_blocks(const GridDesc& g) { return (g.nzh + x_cols<N>() - 1) / x_cols<N>(); }
+
+int x_tiles(const GridDesc& g) {
+  switch (g.nx) {
+    case 16: return x_blocks<16>(g);
+    case 32: return x_blocks<32>(g);
+    case 64: return x_blocks<64>(g);
+    case 128: return x_blocks<128>(g);
+    default: return x_blocks<256>(g);
+  }
+}
+
+template <int N>
+static size_t zsmem() { return (size_t)3 * z_lines<N>() * z_ld<N>() * sizeof(float2); }
+template <int N>
+static size_t xsmem() { return (size_t)6 * N * x_cols<N>() * sizeof(float2); }
+
+template <int N>
+static cudaError_t configure_n() {
+  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(xpass_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N>());
+}
+
+cudaError_t configure() {
+  cudaError_t e;
+  if ((e = configure_n<16>()) != cudaSuccess) return e;
+  if ((e = configure_n<32>()) != cudaSuccess) return e;
+  if ((e = configure_n<64>()) != cudaSuccess) return e;
+  if ((e = configure_n<128>()) != cudaSuccess) return e;
+  return configure_n<256>();
+}
+
+template <int N>
+static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
+                    float* eps, float2* spec, const double* eps_bar, const float* eps0,
+                    InstanceState* st, const Medium* med, cudaStream_t s) {
+  const long long nlines = (long long)g.nx * g.ny;
+  dim3 grid((unsigned)((nlines + z_lines<N>() - 1) / z_lines<N>()), batch);
+  zpass_fast<N><<<grid, 3 * z_lines<N>() * Split<N>::P, zsmem<N>(), s>>>(g, mode, lambda, mu, eps, spec,
+                                                                          eps_bar, eps0, st, med);
+}
+
+void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
+                  float* eps, float2* spec, const double* eps_bar, const float* eps0,
+                  InstanceState* st, const Medium* med, cudaStream_t s) {
+  switch (g.nz) {
+    case 16: zlaunch<16>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
+    case 32: zlaunch<32>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
+    case 64: zlaunch<64>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
+    case 128: zlaunch<128>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
+    default: zlaunch<256>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
+  }
+}
+
+template <int N>
+static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
+                    cudaStream_t s) {
+  dim3 grid((g.nzh + kYT - 1) / kYT, g.nx, 6 * batch);
+  ypass_fast<N><<<grid, kYT * Split<N>::P, 0, s>>>(g, inverse ? 1 : 0, spec, st);
+}
+
+void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
+                  cudaStream_t s) {
+  switch (g.ny) {
+    case 16: ylaunch<16>(g, inverse, batch, spec, st, s); break;
+    case 32: ylaunch<32>(g, inverse, batch, spec, st, s); break;
+    case 64: ylaunch<64>(g, inverse, batch, spec, st, s); break;
+    case 128: ylaunch<128>(g, inverse, batch, spec, st, s); break;
+    default: ylaunch<256>(g, inverse, batch, spec, st, s); break;
+  }
+}
+
+template <int N>
+static void xlaunch(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
+                    double* partials, cudaStream_t s) {
+  dim3 grid(x_blocks<N>(g), g.ny, batch);
+  xpass_fast<N><<<grid, 6 * Split<N>::P * x_cols<N>(), xsmem<N>(), s>>>(g, spec, med, st, partials);
+}
+
+void launch_xpass(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
+                  double* partials, cudaStream_t s) {
+  switch (g.nx) {
+    case 16: xlaunch<16>(g, batch, spec, med, st, partials, s); break;
+    case 32: xlaunch<32>(g, batch, spec, med, st, partials, s); break;
+    case 64: xlaunch<64>(g, batch, spec, med, st, partials, s); break;
+    case 128: xlaunch<128>(g, batch, spec, med, st, partials, s); break;
+    default: xlaunch<256>(g, batch, spec, med, st, partials, s); break;
+  }
+}
+
+}  // namespace fast
+}  // namespace lsb

@@ -1,0 +1,23 @@
+// FP32 passes with compile-time power-of-two lengths (implemented in fast_passes.cu).
+#pragma once
+
+#include "ls_types.cuh"
+
+namespace lsb {
+namespace fast {
+
+// True when every extent is one of 16, 32, 64, 128, 256.
+bool supported(const GridDesc& g);
+// x-pass blocks per (ky) row: the number of kz tiles.
+int x_tiles(const GridDesc& g);
+cudaError_t configure();
+void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
+                  float* eps, float2* spec, const double* eps_bar, const float* eps0,
+                  InstanceState* st, const Medium* med, cudaStream_t s);
+void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
+                  cudaStream_t s);
+void launch_xpass(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
+                  double* partials, cudaStream_t s);
+
+}  // namespace fast
+}  // namespace lsb

@@ -89,6 +89,42 @@ struct Bfly<8> {
   }
 };
 
+// 16-point DFT as 4 x 4 with the twiddles exp(-2 pi i k / 16) in between.
+template <>
+struct Bfly<16> {
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(C::x);
+    const R c = (R)0.92387953251128675613;  // cos(pi/8)
+    const R s = (R)0.38268343236508977173;  // sin(pi/8)
+    const R h = (R)0.70710678118654752440;  // cos(pi/4)
+    C a[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) a[p][e] = v[p + 4 * e];
+      Bfly<4>::run(a[p]);
+    }
+    // a[p][k] *= W16^(p k)
+    a[1][1] = mk<C>(c * a[1][1].x + s * a[1][1].y, c * a[1][1].y - s * a[1][1].x);   // W^1
+    a[1][2] = mk<C>(h * (a[1][2].x + a[1][2].y), h * (a[1][2].y - a[1][2].x));       // W^2
+    a[1][3] = mk<C>(s * a[1][3].x + c * a[1][3].y, s * a[1][3].y - c * a[1][3].x);   // W^3
+    a[2][1] = mk<C>(h * (a[2][1].x + a[2][1].y), h * (a[2][1].y - a[2][1].x));       // W^2
+    a[2][2] = cmul_mi(a[2][2]);                                                       // W^4
+    a[2][3] = mk<C>(h * (a[2][3].y - a[2][3].x), -h * (a[2][3].x + a[2][3].y));      // W^6
+    a[3][1] = mk<C>(s * a[3][1].x + c * a[3][1].y, s * a[3][1].y - c * a[3][1].x);   // W^3
+    a[3][2] = mk<C>(h * (a[3][2].y - a[3][2].x), -h * (a[3][2].x + a[3][2].y));      // W^6
+    a[3][3] = mk<C>(-c * a[3][3].x - s * a[3][3].y, s * a[3][3].x - c * a[3][3].y);  // W^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      C b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+      Bfly<4>::run(b);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
+    }
+  }
+};
+
 template <>
 struct Bfly<3> {
   template <typename C>

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/lippmann_schwinger.h"
+#include "fast_passes.cuh"
 #include "ls_kernels.cuh"
 
 using namespace lsb;
@@ -83,6 +84,7 @@ struct lsb_solver {
   int depth = 0;
   int precision = kPrecMixed;
   int stall_window = 8;
+  bool fast32 = false;   // FP32 passes with compile-time power-of-two lengths
   GridDesc g{};
   LaunchShape sh32{}, sh64{};
   cudaStream_t stream = nullptr;
@@ -170,6 +172,8 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   }
   s->sh32 = plan_launch(g, sizeof(float2));
   s->sh64 = plan_launch(g, sizeof(double2));
+  s->fast32 = fast::supported(g);
+  if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g) * g.ny;
   if (!shape_fits(s->sh32) || !shape_fits(s->sh64)) {
     delete s;
     return fail(-1, "grid %dx%dx%d needs FFT blocks above %d threads", g.nx, g.ny, g.nz, kMaxThreads);
@@ -241,6 +245,7 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   g.sz = g.cy + g.ny;
   g.cz = g.sz + g.nzh;
   cudaError_t e = configure_kernels();
+  if (e == cudaSuccess) e = fast::configure();
   if (e != cudaSuccess) {
     delete s;
     return fail(-2, "kernel configuration: %s", cudaGetErrorString(e));
@@ -263,18 +268,55 @@ SolveParams make_params(const lsb_solver* s, double rtol, double atol, int maxit
   return sp;
 }
 
+// Pass dispatch: FP32 fields use the compile-time-size passes when every extent is a
+// supported power of two, the generic passes otherwise.
+template <typename T>
+void pass_z(lsb_solver* s, int mode, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
+            const T* eps0) {
+  if constexpr (sizeof(T) == 4) {
+    if (s->fast32) {
+      fast::launch_zpass(s->g, mode, batch, lam, mu, eps, spec, s->d_epsbar, eps0, s->d_state,
+                         s->d_medium, s->stream);
+      return;
+    }
+  }
+  launch_zpass<T>(s->g, sizeof(T) == 8 ? s->sh64 : s->sh32, mode, batch, lam, mu, eps, spec,
+                  s->d_epsbar, eps0, s->d_state, s->d_medium, s->stream);
+}
+
+template <typename T>
+void pass_y(lsb_solver* s, bool inverse, int batch, cplx<T>* spec) {
+  if constexpr (sizeof(T) == 4) {
+    if (s->fast32) {
+      fast::launch_ypass(s->g, inverse, batch, spec, s->d_state, s->stream);
+      return;
+    }
+  }
+  launch_ypass<T>(s->g, sizeof(T) == 8 ? s->sh64 : s->sh32, inverse, batch, spec, s->d_state, s->stream);
+}
+
+template <typename T>
+void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
+  if constexpr (sizeof(T) == 4) {
+    if (s->fast32) {
+      fast::launch_xpass(s->g, batch, spec, s->d_medium, s->d_state, s->d_partials, s->stream);
+      return;
+    }
+  }
+  launch_xpass<T>(s->g, sizeof(T) == 8 ? s->sh64 : s->sh32, batch, spec, s->d_medium, s->d_state,
+                  s->d_partials, s->stream);
+}
+
 // Runs the loop of precision T for every instance in its phase until none is left there.
 // init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
 template <typename T>
 int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
               const T* eps0, int init_mode, const SolveParams& sp) {
-  const GridDesc& g = s->g;
   const LaunchShape& sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
   const int phase = sizeof(T) == 8 ? 1 : 0;
   cudaStream_t st = s->stream;
-  launch_zpass<T>(g, sh, init_mode, batch, lam, mu, eps, spec, s->d_epsbar, eps0, s->d_state,
-                  s->d_medium, st);
-  launch_ypass<T>(g, sh, false, batch, spec, s->d_state, st);
+  pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0);
+  pass_y<T>(s, false, batch, spec);
   s->launches += 2;
   LSB_CUDA(cudaGetLastError());
   long long launched = 0;
@@ -283,12 +325,11 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   for (;;) {
     int n = (int)std::min<long long>(chunk, max_evals - launched);
     for (int i = 0; i < n; ++i) {
-      launch_xpass<T>(g, sh, batch, spec, s->d_medium, s->d_state, s->d_partials, st);
+      pass_x<T>(s, batch, spec);
       launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
-      launch_ypass<T>(g, sh, true, batch, spec, s->d_state, st);
-      launch_zpass<T>(g, sh, 1, batch, lam, mu, eps, spec, s->d_epsbar, nullptr, s->d_state,
-                      s->d_medium, st);
-      launch_ypass<T>(g, sh, false, batch, spec, s->d_state, st);
+      pass_y<T>(s, true, batch, spec);
+      pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr);
+      pass_y<T>(s, false, batch, spec);
     }
     launched += n;
     s->launches += 5LL * n;
@@ -502,24 +543,22 @@ int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const fl
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eb.data(), sizeof(double) * eb.size(), cudaMemcpyHostToDevice, st));
   launch_reset_state(batch, 0, s->d_state, st);
   launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
-  launch_zpass<float>(g, sh, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, s->d_epsbar, nullptr,
-                      s->d_state, s->d_medium, st);
-  launch_ypass<float>(g, sh, false, batch, s->d_spec32, s->d_state, st);
+  pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr);
+  pass_y<float>(s, false, batch, s->d_spec32);
   cudaEvent_t ev[6];
   for (auto& e : ev) LSB_CUDA(cudaEventCreate(&e));
   double acc[5] = {0, 0, 0, 0, 0};
   for (int r = 0; r < reps; ++r) {
     cudaEventRecord(ev[0], st);
-    launch_xpass<float>(g, sh, batch, s->d_spec32, s->d_medium, s->d_state, s->d_partials, st);
+    pass_x<float>(s, batch, s->d_spec32);
     cudaEventRecord(ev[1], st);
     launch_finalize(sh, 0, batch, s->d_state, s->d_partials, nullptr, 0, sp, st);
     cudaEventRecord(ev[2], st);
-    launch_ypass<float>(g, sh, true, batch, s->d_spec32, s->d_state, st);
+    pass_y<float>(s, true, batch, s->d_spec32);
     cudaEventRecord(ev[3], st);
-    launch_zpass<float>(g, sh, 1, batch, d_lambda, d_mu, d_eps, s->d_spec32, s->d_epsbar, nullptr,
-                        s->d_state, s->d_medium, st);
+    pass_z<float>(s, 1, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr);
     cudaEventRecord(ev[4], st);
-    launch_ypass<float>(g, sh, false, batch, s->d_spec32, s->d_state, st);
+    pass_y<float>(s, false, batch, s->d_spec32);
     cudaEventRecord(ev[5], st);
     LSB_CUDA(cudaEventSynchronize(ev[5]));
     for (int k = 0; k < 5; ++k) {

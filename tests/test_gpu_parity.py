@@ -50,7 +50,9 @@ def oracle_fixed_iters(lm, mu, eb, g, iters):
 
 @pytest.mark.parametrize("tag,n", [("even", (12, 10, 8)), ("odd", (11, 9, 7)),
                                    ("prime", (37, 47, 61)), ("mixed", (48, 20, 30)),
-                                   ("line", (1, 1, 16)), ("flat", (16, 8, 1))])
+                                   ("line", (1, 1, 16)), ("flat", (16, 8, 1)),
+                                   ("pow2a", (64, 32, 16)), ("pow2b", (16, 128, 256)),
+                                   ("pow2c", (256, 16, 32))])
 def test_fields_match_oracle(ls, tag, n):
     from jaxmaterials_b200 import GridSpec
 
