@@ -114,7 +114,11 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, which):
+        """Record the wall time of the start/end of the timed region."""
+        setattr(self, which, time.time())
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -127,7 +131,11 @@ class ClockSampler:
     def summary(self):
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        t0, t1 = getattr(self, "start", None), getattr(self, "end", None)
+        lines = [l for ts, l in self.lines if t0 is None or t1 is None or t0 - 0.25 <= ts <= t1 + 0.25]
+        if not lines:
+            lines = [l for _, l in self.lines]
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -245,6 +253,7 @@ def own_arm(args):
     def step(lm_t, mu_t):
         return s.solve(lm_t, mu_t, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
 
+    clocks = ClockSampler(local).__enter__()
     for _ in range(max(args.warmup, 3)):
         r = step(lm_d, mu_d)
     converged = bool(np.all(r.status == CONVERGED))
@@ -258,17 +267,19 @@ def own_arm(args):
     launches0 = s.kernel_launches()
     iters_total = 0
     c_eff = None
-    with ClockSampler(local) as clocks:
-        barrier()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        for _ in range(args.steps):
-            r = step(lm_d, mu_d)
-            iters_total += int(r.iters.sum())
-            c_eff = r.mean_sigma
-        t1.record(stream)
-        barrier()
+    barrier()
+    clocks.mark("start")
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        r = step(lm_d, mu_d)
+        iters_total += int(r.iters.sum())
+        c_eff = r.mean_sigma
+    t1.record(stream)
+    barrier()
+    clocks.mark("end")
+    clocks.__exit__(None, None, None)
     launches = s.kernel_launches() - launches0
     ms = t0.elapsed_time(t1)
     ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
