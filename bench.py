@@ -39,7 +39,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--depth", type=int, default=0)
+    p.add_argument("--depth", type=int, default=5)
+    p.add_argument("--no-plain", action="store_true", help="skip the plain-iteration comparison")
     p.add_argument("--cpu-sample-s", type=float, default=12.0)
     return p.parse_args()
 
@@ -163,14 +164,14 @@ def cpu_sample(lm, mu, g, depth, budget_s, threads):
     eb = np.zeros(6)
     eb[0] = 1.0
     total_t, total_it = 0.0, 0
-    chunk = 2
+    chunk = 1
     while total_t < budget_s:
         t0 = time.perf_counter()
         _, _, it = O.lippmann_schwinger(lm, mu, eb, og, rtol=0.0, atol=0.0, depth=depth,
                                         maxiter=chunk, dtype=np.float32, workers=threads)
         total_t += time.perf_counter() - t0
         total_it += it
-        chunk = min(chunk * 2, 16)
+        chunk = min(chunk * 2, 4)
     return total_t / (total_it * g.number_of_voxels), total_it
 
 
@@ -282,6 +283,32 @@ def own_arm(args):
     clocks.__exit__(None, None, None)
     launches = s.kernel_launches() - launches0
     ms = t0.elapsed_time(t1)
+
+    # ---- the plain Moulinec-Suquet iteration on the same structure, same timing rules
+    plain = None
+    if args.depth > 0 and not args.no_plain:
+        sp_ = Solver(g, batch=6, depth=0)
+        for _ in range(3):
+            sp_.solve(lm_d, mu_d, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
+        barrier()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        pits = 0
+        for _ in range(args.steps):
+            rp = sp_.solve(lm_d, mu_d, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
+            pits += int(rp.iters.sum())
+        p1.record(stream)
+        barrier()
+        pms = torch.tensor([p0.elapsed_time(p1)], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(pms, op=dist.ReduceOp.MAX)
+        pms = float(pms.item())
+        plain = {"value": 6.0 * args.steps * world / (pms / 1000.0), "unit": "solves/s",
+                 "iters_per_solve": pits / (6 * args.steps),
+                 "voxel_iter_per_s": pits * world * g.number_of_voxels / (pms / 1000.0),
+                 "all_converged": bool(np.all(rp.status == CONVERGED))}
+        sp_.close()
     ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
     it_t = torch.tensor([iters_total], device=dev, dtype=torch.float64)
     if world > 1:
@@ -311,7 +338,8 @@ def own_arm(args):
         dist.all_reduce(ems, op=dist.ReduceOp.MAX)
     e2e = 6.0 * args.steps * world / (float(ems.item()) / 1000.0)
 
-    # ---- per-pass timing for the roofline (same stream, CUDA events, full workload)
+    # ---- per-pass timing for the roofline (same stream, CUDA events, full workload); the
+    # passes shared by the plain and the Anderson iteration
     passes = s.profile_passes(lm_d, mu_d, batch=6, reps=5)
     nv, nm, b = g.number_of_voxels, g.number_of_modes, 6
     spec = 6 * nm * 8
@@ -352,6 +380,7 @@ def own_arm(args):
             "voxel_iter_per_s": vips,
             "iters_per_solve": float(iters_total) / (6 * args.steps),
             "all_converged": converged,
+            "plain": plain,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "gpu_launches": int(launches),
             "roofline": {

@@ -274,14 +274,18 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
   __syncthreads();
 }
 
+// Modes as the generic z pass: 0 init from eps_bar/eps0, 1 plain update, 2 keep eps,
+// 3 Anderson residual (rings + Gram-row partials), 4 Anderson combine.
 template <int NZ>
 __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fast(
     GridDesc g, int mode, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
-    const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med) {
+    const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med,
+    AndersonArgs<float> aa) {
   constexpr int P = Split<NZ>::P, L = z_lines<NZ>(), LD = z_ld<NZ>(), NZH = NZ / 2 + 1;
   extern __shared__ __align__(16) unsigned char zfraw[];
   float2* zbuf = reinterpret_cast<float2*>(zfraw);   // 3L lines of LD values
+  __shared__ double gred[kMaxDepth + 1][32];
   const int b = blockIdx.y;
   if (!active32(st[b])) return;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
   float2* sb = spec + (size_t)b * 6 * g.nm;
   const float2* tw = g.pz.tw;
 
-  if (mode == 1) {
+  if (mode == 1 || mode == 3) {
     for (int idx = tid; idx < 3 * L * NZH; idx += nt) {
       const int pr = idx / (L * NZH);
       const int rem = idx - pr * (L * NZH);
@@ -309,6 +313,64 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
     }
     __syncthreads();
     zline_fft<NZ>(zbuf, q, p, tw);
+  }
+
+  int slot = 0, filled = 0;
+  const int M1 = aa.depth + 1;
+  const size_t ring = (size_t)6 * g.nv;
+  if (mode >= 3) {
+    const int j = st[b].iter - 1 - st[b].aa_base;
+    slot = j % M1;
+    filled = j + 1 < M1 ? j + 1 : M1;
+  }
+  if (mode == 3) {
+    float* rb = aa.r + (size_t)b * M1 * ring;
+    float* gb = aa.g + (size_t)b * M1 * ring;
+    double dots[kMaxDepth + 1];
+#pragma unroll
+    for (int qq = 0; qq <= kMaxDepth; ++qq) dots[qq] = 0.0;
+    const float inv_nv = (float)(1.0 / (double)g.nv);
+    for (int idx = tid; idx < L * NZ; idx += nt) {
+      const int l = idx / NZ, n = idx % NZ;
+      const long long line = l0 + l;
+      if (line >= nlines) continue;
+      const size_t vx = (size_t)line * NZ + n;
+      float r[6];
+#pragma unroll
+      for (int pr = 0; pr < 3; ++pr) {
+        float2 w = zbuf[(size_t)(pr * L + l) * LD + n];
+        r[2 * pr] = w.x * inv_nv;
+        r[2 * pr + 1] = -w.y * inv_nv;
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const size_t o = (size_t)c * g.nv + vx;
+        rb[slot * ring + o] = r[c];
+        gb[slot * ring + o] = eb[o] + r[c];
+      }
+      for (int qq = 0; qq < filled; ++qq) {
+        double d = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const float rs = qq == slot ? r[c] : rb[qq * ring + (size_t)c * g.nv + vx];
+          d += (c < 3 ? 1.0 : 2.0) * (double)r[c] * (double)rs;
+        }
+        dots[qq] += d;
+      }
+    }
+    for (int qq = 0; qq < filled; ++qq) {
+      double a = dots[qq];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      if ((tid & 31) == 0) gred[qq][tid >> 5] = a;
+    }
+    __syncthreads();
+    if (tid < filled) {
+      double a = 0.0;
+      for (int w = 0; w < nt / 32; ++w) a += gred[tid][w];
+      aa.partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + tid] = a;
+    }
+    return;
   }
 
   float shift[6];
@@ -345,6 +407,16 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
       } else if (mode == 2) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * g.nv + vx];
+      } else if (mode == 4) {
+        const float* gb = aa.g + (size_t)b * M1 * ring;
+        const double* al = aa.alpha + (size_t)b * M1;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) e[c] = 0.f;
+        for (int qq = 0; qq < filled; ++qq) {
+          const float a = (float)al[qq];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) e[c] += a * gb[qq * ring + (size_t)c * g.nv + vx];
+        }
       } else if (eps0 != nullptr) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * g.nv + vx];
@@ -407,6 +479,10 @@ int x_tiles(const GridDesc& g) {
 template <int N>
 static size_t zsmem() { return (size_t)3 * z_lines<N>() * z_ld<N>() * sizeof(float2); }
 template <int N>
+static int z_blocks_for(const GridDesc& g) {
+  return (int)(((long long)g.nx * g.ny + z_lines<N>() - 1) / z_lines<N>());
+}
+template <int N>
 static size_t xsmem() { return (size_t)6 * N * x_cols<N>() * sizeof(float2); }
 
 template <int N>
@@ -428,22 +504,34 @@ cudaError_t configure() {
 template <int N>
 static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
                     float* eps, float2* spec, const double* eps_bar, const float* eps0,
-                    InstanceState* st, const Medium* med, cudaStream_t s) {
-  const long long nlines = (long long)g.nx * g.ny;
-  dim3 grid((unsigned)((nlines + z_lines<N>() - 1) / z_lines<N>()), batch);
+                    InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s) {
+  dim3 grid((unsigned)z_blocks_for<N>(g), batch);
   zpass_fast<N><<<grid, 3 * z_lines<N>() * Split<N>::P, zsmem<N>(), s>>>(g, mode, lambda, mu, eps, spec,
-                                                                          eps_bar, eps0, st, med);
+                                                                          eps_bar, eps0, st, med, aa);
 }
 
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
                   float* eps, float2* spec, const double* eps_bar, const float* eps0,
-                  InstanceState* st, const Medium* med, cudaStream_t s) {
+                  InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s) {
   switch (g.nz) {
-    case 16: zlaunch<16>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
-    case 32: zlaunch<32>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
-    case 64: zlaunch<64>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
-    case 128: zlaunch<128>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
-    default: zlaunch<256>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, s); break;
+    case 16: zlaunch<16>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+    case 32: zlaunch<32>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+    case 64: zlaunch<64>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+    case 128: zlaunch<128>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+    default: zlaunch<256>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+  }
+}
+
+template <int N>
+static int z_blocks_n(const GridDesc& g) { return z_blocks_for<N>(g); }
+
+int z_blocks(const GridDesc& g) {
+  switch (g.nz) {
+    case 16: return z_blocks_n<16>(g);
+    case 32: return z_blocks_n<32>(g);
+    case 64: return z_blocks_n<64>(g);
+    case 128: return z_blocks_n<128>(g);
+    default: return z_blocks_n<256>(g);
   }
 }
 

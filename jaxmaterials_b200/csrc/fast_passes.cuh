@@ -11,9 +11,11 @@ bool supported(const GridDesc& g);
 // x-pass blocks per (ky) row: the number of kz tiles.
 int x_tiles(const GridDesc& g);
 cudaError_t configure();
+// z-pass blocks per instance (number of Gram-row partials in the Anderson residual mode).
+int z_blocks(const GridDesc& g);
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
                   float* eps, float2* spec, const double* eps_bar, const float* eps0,
-                  InstanceState* st, const Medium* med, cudaStream_t s);
+                  InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s);
 void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
                   cudaStream_t s);
 void launch_xpass(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,

@@ -31,7 +31,34 @@ __device__ __forceinline__ bool active(const InstanceState& s) {
 // Lines l = x * ny + y; pair p of components (2p, 2p+1) shares one complex line
 // z = a + i b (two real transforms for the price of one complex transform).
 // mode 0: eps = eps_bar (or eps0); mode 1: eps += r / N with r from the spectrum;
-// mode 2: keep eps (continuation of an instance in another precision).
+// mode 2: keep eps (continuation of an instance in another precision);
+// mode 3: Anderson residual: r from the spectrum into the rings, g = eps + r, FP64
+//         Gram-row partials <r_j, r_s>_w (no stress, no forward transform);
+// mode 4: Anderson combine: eps = sum_s alpha_s g_s, then stress and forward transform.
+template <typename T>
+__device__ __forceinline__ void anderson_slots(const InstanceState& s, int depth, int& slot, int& filled) {
+  const int j = s.iter - 1 - s.aa_base;
+  slot = j % (depth + 1);
+  filled = j + 1 < depth + 1 ? j + 1 : depth + 1;
+}
+
+// Block-wide FP64 sums of v[0..n) (n <= kMaxDepth + 1) written to out[0..n).
+__device__ __forceinline__ void block_sum_slots(double* v, int n, double (*red)[32], double* out) {
+  const int tid = threadIdx.x;
+  for (int s = 0; s < n; ++s) {
+    double a = v[s];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((tid & 31) == 0) red[s][tid >> 5] = a;
+  }
+  __syncthreads();
+  if (tid < n) {
+    double a = 0.0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) a += red[tid][w];
+    out[tid] = a;
+  }
+}
+
 template <typename T, int VPT>
 __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode, int L,
                                                      const T* __restrict__ lambda,
@@ -41,10 +68,12 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
                                                      const double* __restrict__ eps_bar,
                                                      const T* __restrict__ eps0,
                                                      InstanceState* __restrict__ st,
-                                                     const Medium* __restrict__ med) {
+                                                     const Medium* __restrict__ med,
+                                                     AndersonArgs<T> aa) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char zraw[];
   C* zbuf = reinterpret_cast<C*>(zraw);
+  __shared__ double gred[kMaxDepth + 1][32];
   const int b = blockIdx.y;
   if (!active<T>(st[b])) return;
   const int nz = g.nz, nzh = g.nzh;
@@ -57,7 +86,7 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
   const Plan1D& pz = g.pz;
   const C* tw = twiddles<T>(pz);
 
-  if (mode == 1) {
+  if (mode == 1 || mode == 3) {
     // Build conj(Z) with Z[k] = A[k] + i B[k] on the full line (Hermitian extension);
     // DC and (even nz) Nyquist terms are taken as real, as a C2R transform does.
     const int work = 3 * L * nzh;
@@ -77,6 +106,52 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
     }
     __syncthreads();
     fft_lines<VPT, false>(zbuf, 3 * L, 1, ldz, pz, tw);
+  }
+
+  if (mode == 3) {
+    // Anderson residual: rings and Gram-row partials, then done.
+    int slot, filled;
+    anderson_slots<T>(st[b], aa.depth, slot, filled);
+    const int M1 = aa.depth + 1;
+    const size_t ring = (size_t)6 * g.nv;   // one slot
+    T* rb = aa.r + (size_t)b * M1 * ring;
+    T* gb = aa.g + (size_t)b * M1 * ring;
+    double dots[kMaxDepth + 1];
+#pragma unroll
+    for (int q = 0; q <= kMaxDepth; ++q) dots[q] = 0.0;
+    const T inv_nv = (T)(1.0 / (double)g.nv);
+    for (int idx = tid; idx < L * nz; idx += nt) {
+      int l = idx / nz, n = idx - l * nz;
+      long long line = l0 + l;
+      if (line >= nlines) continue;
+      size_t v = (size_t)line * nz + n;
+      T r[6];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        C w = zbuf[(size_t)(p * L + l) * ldz + n];
+        r[2 * p] = w.x * inv_nv;
+        r[2 * p + 1] = -w.y * inv_nv;
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const size_t o = (size_t)c * g.nv + v;
+        rb[slot * ring + o] = r[c];
+        gb[slot * ring + o] = eb[o] + r[c];
+      }
+      for (int q = 0; q < filled; ++q) {
+        double d = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const T rs = q == slot ? r[c] : rb[q * ring + (size_t)c * g.nv + v];
+          d += (c < 3 ? 1.0 : 2.0) * (double)r[c] * (double)rs;
+        }
+        dots[q] += d;
+      }
+    }
+    double out[kMaxDepth + 1];
+    block_sum_slots(dots, filled, gred, out);
+    if (tid < filled) aa.partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + tid] = out[tid];
+    return;
   }
 
   // Shift of the forward transform: the current mean-stress estimate (see InstanceState).
@@ -120,6 +195,20 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
       } else if (mode == 2) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * g.nv + v];
+      } else if (mode == 4) {
+        int slot, filled;
+        anderson_slots<T>(st[b], aa.depth, slot, filled);
+        const int M1 = aa.depth + 1;
+        const size_t ring = (size_t)6 * g.nv;
+        const T* gb = aa.g + (size_t)b * M1 * ring;
+        const double* al = aa.alpha + (size_t)b * M1;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) e[c] = 0;
+        for (int q = 0; q < filled; ++q) {
+          const T a = (T)al[q];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) e[c] += a * gb[q * ring + (size_t)c * g.nv + v];
+        }
       } else if (eps0 != nullptr) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * g.nv + v];
@@ -406,6 +495,74 @@ __global__ void finalize_kernel(int nblk, int phase, InstanceState* __restrict__
   s.iter += 1;
 }
 
+// Anderson mixing coefficients (lippmann_schwinger.py:219-228): the new Gram row
+// <r_j, r_s>_w replaces row and column `slot` of A (the reference's roll of A is a
+// relabelling of the ring), A v = 1 is solved over the filled slots in FP64 by Gaussian
+// elimination with partial pivoting, alpha = v / sum(v). A singular or non-finite solve
+// falls back to the plain update alpha = e_slot.
+__global__ void anderson_solve_kernel(int nzblk, int depth, int phase, const InstanceState* __restrict__ st,
+                                      const double* __restrict__ partials, double* __restrict__ amat,
+                                      double* __restrict__ alpha) {
+  __shared__ double dot[kMaxDepth + 1];
+  const int b = blockIdx.x;
+  const InstanceState& s = st[b];
+  if (s.done || s.phase != phase) return;
+  const int M1 = depth + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int slot, filled;
+  anderson_slots<double>(s, depth, slot, filled);
+  if (warp < filled) {
+    double a = 0.0;
+    for (int i = lane; i < nzblk; i += 32) a += partials[((size_t)b * nzblk + i) * M1 + warp];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) dot[warp] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double* A = amat + (size_t)b * M1 * M1;
+  for (int q = 0; q < filled; ++q) {
+    A[slot * M1 + q] = dot[q];
+    A[q * M1 + slot] = dot[q];
+  }
+  double m[kMaxDepth + 1][kMaxDepth + 2];
+  for (int i = 0; i < filled; ++i) {
+    for (int j = 0; j < filled; ++j) m[i][j] = A[i * M1 + j];
+    m[i][filled] = 1.0;
+  }
+  bool ok = true;
+  for (int c = 0; c < filled && ok; ++c) {
+    int piv = c;
+    for (int i = c + 1; i < filled; ++i)
+      if (fabs(m[i][c]) > fabs(m[piv][c])) piv = i;
+    if (!(fabs(m[piv][c]) > 0.0)) { ok = false; break; }
+    if (piv != c)
+      for (int j = c; j <= filled; ++j) { double t = m[c][j]; m[c][j] = m[piv][j]; m[piv][j] = t; }
+    for (int i = c + 1; i < filled; ++i) {
+      const double f = m[i][c] / m[c][c];
+      for (int j = c; j <= filled; ++j) m[i][j] -= f * m[c][j];
+    }
+  }
+  double v[kMaxDepth + 1];
+  double sum = 0.0;
+  if (ok) {
+    for (int i = filled - 1; i >= 0; --i) {
+      double t = m[i][filled];
+      for (int j = i + 1; j < filled; ++j) t -= m[i][j] * v[j];
+      v[i] = t / m[i][i];
+      sum += v[i];
+    }
+    ok = isfinite(sum) && sum != 0.0;
+  }
+  double* al = alpha + (size_t)b * M1;
+  for (int q = 0; q < M1; ++q) al[q] = 0.0;
+  if (ok) {
+    for (int q = 0; q < filled; ++q) al[q] = v[q] / sum;
+  } else {
+    al[slot] = 1.0;
+  }
+}
+
 __global__ void reset_state_kernel(int batch, int phase, InstanceState* st) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < batch) {
@@ -639,10 +796,17 @@ cudaError_t configure_kernels() {
 template <typename T>
 void launch_zpass(const GridDesc& g, const LaunchShape& s, int mode, int batch, const T* lambda,
                   const T* mu, T* eps, cplx<T>* spec, const double* eps_bar, const T* eps0,
-                  InstanceState* st, const Medium* med, cudaStream_t stream) {
+                  InstanceState* st, const Medium* med, const AndersonArgs<T>& aa,
+                  cudaStream_t stream) {
   dim3 grid(s.z_blocks, batch);
   zpass_kernel<T, kVPT><<<grid, s.z_threads, s.z_smem, stream>>>(
-      g, mode, s.lines_per_block, lambda, mu, eps, spec, eps_bar, eps0, st, med);
+      g, mode, s.lines_per_block, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa);
+}
+
+void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
+                           const double* partials, double* amat, double* alpha, cudaStream_t stream) {
+  anderson_solve_kernel<<<batch, 32 * (depth + 1), 0, stream>>>(nzblk, depth, phase, st, partials,
+                                                                 amat, alpha);
 }
 
 template <typename T>
@@ -709,7 +873,7 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
 #define LSB_INST(T)                                                                             \
   template void launch_zpass<T>(const GridDesc&, const LaunchShape&, int, int, const T*,        \
                                 const T*, T*, cplx<T>*, const double*, const T*, InstanceState*, \
-                                const Medium*, cudaStream_t);                                   \
+                                const Medium*, const AndersonArgs<T>&, cudaStream_t);           \
   template void launch_ypass<T>(const GridDesc&, const LaunchShape&, bool, int, cplx<T>*,       \
                                 const InstanceState*, cudaStream_t);                            \
   template void launch_xpass<T>(const GridDesc&, const LaunchShape&, int, cplx<T>*,             \

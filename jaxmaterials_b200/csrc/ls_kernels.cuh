@@ -28,10 +28,14 @@ cudaError_t configure_kernels();
 // and its phase matches the precision T (float: phase 0, double: phase 1).
 // mode 0: eps = eps_bar (or eps0 if given); mode 1: eps += r / N from spec; mode 2: keep
 // eps and the stored shift (continuation in another precision).
+// modes 3/4: Anderson residual / combine (see ls_kernels.cu).
 template <typename T>
 void launch_zpass(const GridDesc& g, const LaunchShape& ls, int mode, int batch, const T* lambda,
                   const T* mu, T* eps, cplx<T>* spec, const double* eps_bar, const T* eps0,
-                  InstanceState* st, const Medium* med, cudaStream_t s);
+                  InstanceState* st, const Medium* med, const AndersonArgs<T>& aa, cudaStream_t s);
+// Anderson coefficients of every instance in `phase` from the Gram-row partials.
+void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
+                           const double* partials, double* amat, double* alpha, cudaStream_t s);
 template <typename T>
 void launch_ypass(const GridDesc& g, const LaunchShape& ls, bool inverse, int batch, cplx<T>* spec,
                   const InstanceState* st, cudaStream_t s);

@@ -95,6 +95,15 @@ struct lsb_solver {
   double* d_eps64 = nullptr;
   double2* d_spec64 = nullptr;
   double* d_lame64 = nullptr;    // [2][nv]
+  // Anderson acceleration (depth > 0): rings of g = eps + r and r, Gram matrices, coefficients
+  float* d_aa_g32 = nullptr;     // [batch][m+1][6][nv]
+  float* d_aa_r32 = nullptr;
+  double* d_aa_g64 = nullptr;    // FP64 rings, allocated for FP64 runs
+  double* d_aa_r64 = nullptr;
+  double* d_aa_partials = nullptr;  // [batch][z blocks][m+1]
+  double* d_aa_mat = nullptr;    // [batch][m+1][m+1]
+  double* d_aa_alpha = nullptr;  // [batch][m+1]
+  int aa_zblocks = 0;
   // shared
   double* d_partials = nullptr;  // [batch][x blocks]
   InstanceState* d_state = nullptr;
@@ -115,7 +124,8 @@ struct lsb_solver {
   ~lsb_solver() {
     void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
                     d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
-                    d_tables};
+                    d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
+                    d_aa_alpha};
     for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
   }
@@ -133,12 +143,37 @@ int ensure_history(lsb_solver* s, int len) {
 }
 
 int ensure_fp64(lsb_solver* s) {
-  if (s->d_spec64) return 0;
   const size_t B = (size_t)s->batch_cap;
-  LSB_CUDA(cudaMalloc(&s->d_eps64, sizeof(double) * B * 6 * s->g.nv));
-  LSB_CUDA(cudaMalloc(&s->d_spec64, sizeof(double2) * B * 6 * s->g.nm));
-  LSB_CUDA(cudaMalloc(&s->d_lame64, sizeof(double) * 2 * s->g.nv));
+  if (!s->d_spec64) {
+    LSB_CUDA(cudaMalloc(&s->d_eps64, sizeof(double) * B * 6 * s->g.nv));
+    LSB_CUDA(cudaMalloc(&s->d_spec64, sizeof(double2) * B * 6 * s->g.nm));
+    LSB_CUDA(cudaMalloc(&s->d_lame64, sizeof(double) * 2 * s->g.nv));
+  }
   return 0;
+}
+
+int ensure_fp64_rings(lsb_solver* s) {
+  if (s->depth == 0 || s->d_aa_g64) return 0;
+  const size_t n = (size_t)s->batch_cap * (s->depth + 1) * 6 * s->g.nv;
+  LSB_CUDA(cudaMalloc(&s->d_aa_g64, sizeof(double) * n));
+  LSB_CUDA(cudaMalloc(&s->d_aa_r64, sizeof(double) * n));
+  return 0;
+}
+
+template <typename T>
+AndersonArgs<T> anderson_args(lsb_solver* s, bool on) {
+  AndersonArgs<T> a;
+  a.depth = on ? s->depth : 0;
+  if constexpr (sizeof(T) == 4) {
+    a.g = s->d_aa_g32;
+    a.r = s->d_aa_r32;
+  } else {
+    a.g = s->d_aa_g64;
+    a.r = s->d_aa_r64;
+  }
+  a.partials = s->d_aa_partials;
+  a.alpha = s->d_aa_alpha;
+  return a;
 }
 
 int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], int batch, int depth) {
@@ -151,7 +186,7 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
       return fail(-1, "extents[%d] must be positive and finite", d);
   }
   if (batch < 1) return fail(-1, "batch must be >= 1");
-  if (depth != 0) return fail(-1, "Anderson depth %d not supported by this build", depth);
+  if (depth < 0 || depth > kMaxDepth) return fail(-1, "Anderson depth %d outside [0, %d]", depth, kMaxDepth);
   auto* s = new lsb_solver();
   s->batch_cap = batch;
   s->depth = depth;
@@ -202,6 +237,20 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   if (!ok) {
     delete s;
     return rc;
+  }
+  if (depth > 0) {
+    const size_t M1 = (size_t)depth + 1;
+    s->aa_zblocks = std::max(std::max(s->sh32.z_blocks, s->sh64.z_blocks),
+                             s->fast32 ? fast::z_blocks(g) : 0);
+    ok = alloc((void**)&s->d_aa_g32, sizeof(float) * B * M1 * 6 * g.nv) &&
+         alloc((void**)&s->d_aa_r32, sizeof(float) * B * M1 * 6 * g.nv) &&
+         alloc((void**)&s->d_aa_partials, sizeof(double) * B * s->aa_zblocks * M1) &&
+         alloc((void**)&s->d_aa_mat, sizeof(double) * B * M1 * M1) &&
+         alloc((void**)&s->d_aa_alpha, sizeof(double) * B * M1);
+    if (!ok) {
+      delete s;
+      return rc;
+    }
   }
   if (cudaMallocHost(&s->h_state, sizeof(InstanceState) * B) != cudaSuccess) {
     delete s;
@@ -272,16 +321,25 @@ SolveParams make_params(const lsb_solver* s, double rtol, double atol, int maxit
 // supported power of two, the generic passes otherwise.
 template <typename T>
 void pass_z(lsb_solver* s, int mode, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
-            const T* eps0) {
+            const T* eps0, const AndersonArgs<T>& aa) {
   if constexpr (sizeof(T) == 4) {
     if (s->fast32) {
       fast::launch_zpass(s->g, mode, batch, lam, mu, eps, spec, s->d_epsbar, eps0, s->d_state,
-                         s->d_medium, s->stream);
+                         s->d_medium, aa, s->stream);
       return;
     }
   }
   launch_zpass<T>(s->g, sizeof(T) == 8 ? s->sh64 : s->sh32, mode, batch, lam, mu, eps, spec,
-                  s->d_epsbar, eps0, s->d_state, s->d_medium, s->stream);
+                  s->d_epsbar, eps0, s->d_state, s->d_medium, aa, s->stream);
+}
+
+template <typename T>
+int z_blocks_of(const lsb_solver* s) {
+  if constexpr (sizeof(T) == 4) {
+    if (s->fast32) return fast::z_blocks(s->g);
+    return s->sh32.z_blocks;
+  }
+  return s->sh64.z_blocks;
 }
 
 template <typename T>
@@ -309,13 +367,16 @@ void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
 
 // Runs the loop of precision T for every instance in its phase until none is left there.
 // init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
+// With `anderson` the update is Anderson mixing of depth s->depth (rings of precision T).
 template <typename T>
 int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
-              const T* eps0, int init_mode, const SolveParams& sp) {
+              const T* eps0, int init_mode, const SolveParams& sp, bool anderson) {
   const LaunchShape& sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
   const int phase = sizeof(T) == 8 ? 1 : 0;
   cudaStream_t st = s->stream;
-  pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0);
+  const AndersonArgs<T> aa = anderson_args<T>(s, anderson && s->depth > 0);
+  const bool mix = aa.depth > 0;
+  pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0, aa);
   pass_y<T>(s, false, batch, spec);
   s->launches += 2;
   LSB_CUDA(cudaGetLastError());
@@ -328,11 +389,18 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
       pass_x<T>(s, batch, spec);
       launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
       pass_y<T>(s, true, batch, spec);
-      pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr);
+      if (mix) {
+        pass_z<T>(s, 3, batch, lam, mu, eps, spec, nullptr, aa);
+        launch_anderson_solve(z_blocks_of<T>(s), s->depth, phase, batch, s->d_state,
+                              s->d_aa_partials, s->d_aa_mat, s->d_aa_alpha, st);
+        pass_z<T>(s, 4, batch, lam, mu, eps, spec, nullptr, aa);
+      } else {
+        pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
+      }
       pass_y<T>(s, false, batch, spec);
     }
     launched += n;
-    s->launches += 5LL * n;
+    s->launches += (mix ? 7LL : 5LL) * n;
     LSB_CUDA(cudaGetLastError());
     LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch,
                              cudaMemcpyDeviceToHost, st));
@@ -371,7 +439,7 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   s->launches += 3;
   bool any64 = fp64_start;
   if (!fp64_start) {
-    LSB_TRY(run_phase<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, d_eps0, 0, sp));
+    LSB_TRY(run_phase<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, d_eps0, 0, sp, true));
     for (int b = 0; b < batch; ++b) any64 = any64 || (s->h_state[b].phase == 1 && !s->h_state[b].done);
   }
   if (any64) {
@@ -387,8 +455,11 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
       s->launches += 1;
     }
     const int init_mode = fp64_start ? (d_eps0 ? 2 : 0) : 2;
+    // FP64 from the start runs Anderson in FP64; the continuation after an FP32 stall is
+    // a few plain updates from the FP32 iterate.
+    if (fp64_start) LSB_TRY(ensure_fp64_rings(s));
     LSB_TRY(run_phase<double>(s, batch, s->d_lame64, s->d_lame64 + g.nv, s->d_eps64, s->d_spec64,
-                              nullptr, init_mode, sp));
+                              nullptr, init_mode, sp, fp64_start));
     launch_convert_fields<double, float>(n6, batch, 0, s->d_state, s->d_eps64, d_eps, st);
     launch_stress<double, float>(g, 1, batch, s->d_state, s->d_lame64, s->d_lame64 + g.nv, s->d_eps64,
                                  d_sigma, s->d_mean_scratch, s->d_mean, st);
@@ -430,7 +501,8 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   launch_reset_state(batch, 1, s->d_state, st);
   launch_medium<double>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
-  LSB_TRY(run_phase<double>(s, batch, d_lambda, d_mu, d_eps, s->d_spec64, d_eps0, 0, sp));
+  LSB_TRY(ensure_fp64_rings(s));
+  LSB_TRY(run_phase<double>(s, batch, d_lambda, d_mu, d_eps, s->d_spec64, d_eps0, 0, sp, true));
   launch_stress<double, double>(g, 1, batch, s->d_state, d_lambda, d_mu, d_eps, d_sigma,
                                 s->d_mean_scratch, s->d_mean, st);
   s->launches += 2;
@@ -543,7 +615,8 @@ int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const fl
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eb.data(), sizeof(double) * eb.size(), cudaMemcpyHostToDevice, st));
   launch_reset_state(batch, 0, s->d_state, st);
   launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
-  pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr);
+  const AndersonArgs<float> aa0 = anderson_args<float>(s, false);
+  pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa0);
   pass_y<float>(s, false, batch, s->d_spec32);
   cudaEvent_t ev[6];
   for (auto& e : ev) LSB_CUDA(cudaEventCreate(&e));
@@ -556,7 +629,7 @@ int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const fl
     cudaEventRecord(ev[2], st);
     pass_y<float>(s, true, batch, s->d_spec32);
     cudaEventRecord(ev[3], st);
-    pass_z<float>(s, 1, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr);
+    pass_z<float>(s, 1, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa0);
     cudaEventRecord(ev[4], st);
     pass_y<float>(s, false, batch, s->d_spec32);
     cudaEventRecord(ev[5], st);

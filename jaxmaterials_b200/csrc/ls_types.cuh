@@ -105,7 +105,7 @@ struct InstanceState {
   int phase;      // 0: FP32 fields, 1: FP64 fields
   int best_eval;  // evaluation at which best_e last improved significantly
   int switched;   // 1 once the instance moved from FP32 to FP64
-  int pad;
+  int aa_base;    // iteration count when the Anderson history (re)started
   double e0;      // criterion at the first iterate
   double e;       // last criterion value
   double best_e;  // smallest criterion value seen in the current phase
@@ -118,6 +118,21 @@ struct InstanceState {
 };
 
 enum Precision : int { kPrecFP32 = 0, kPrecMixed = 1, kPrecFP64 = 2 };
+
+constexpr int kMaxDepth = 8;  // largest Anderson depth m (ring of m+1 slots)
+
+// Anderson acceleration state of one batch (lippmann_schwinger.py:217-231). For update j
+// of an instance (j = iter - 1 - aa_base), slot j mod (m+1) of the rings receives
+// r_j = -Gamma^0 sigma_j (real space, normalised) and g_j = eps_j + r_j; the next
+// iterate is eps = sum_s alpha_s g_s over the filled slots.
+template <typename T>
+struct AndersonArgs {
+  int depth;             // m (0: plain iteration)
+  T* g;                  // [batch][m+1][6][nv]
+  T* r;                  // [batch][m+1][6][nv]
+  double* partials;      // [batch][z blocks][m+1] Gram-row partials
+  const double* alpha;   // [batch][m+1] mixing coefficients of the current update
+};
 
 struct SolveParams {
   double rtol, atol;

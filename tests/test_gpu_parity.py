@@ -315,3 +315,65 @@ def test_mixed_precision_reaches_tolerance_at_128(ls):
         ref = np.load(fx)["ceff_d0"]
         assert np.linalg.norm(r.mean_sigma - ref) / np.linalg.norm(ref) < 1e-5
     s.close()
+
+
+# ------------------------------------------------------------------ Anderson acceleration
+@pytest.mark.parametrize("depth", [1, 2, 4, 5])
+@pytest.mark.parametrize("n", [(12, 10, 8), (32, 16, 64), (37, 47, 61)])
+def test_anderson_fields_match_oracle(ls, depth, n):
+    """Same number of Anderson updates (lippmann_schwinger.py:217-231) as the FP64 oracle."""
+    from jaxmaterials_b200 import GridSpec
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    s = ls.Solver(g, batch=1, depth=depth)
+    r = s.solve(lm, mu, EPS_BAR, rtol=0.0, atol=0.0, maxiter=6)
+    e64, s64, it64 = O.lippmann_schwinger(lm, mu, EPS_BAR, O.Grid(*n, *EXT), rtol=0.0, atol=0.0,
+                                          depth=depth, maxiter=6, dtype=np.float64)
+    assert int(r.iters[0]) == it64 == 6
+    assert relmax(r.epsilon[0].cpu().numpy(), e64) < 5e-5
+    assert relmax(r.sigma[0].cpu().numpy(), s64) < 5e-5
+    s.close()
+
+
+@pytest.mark.parametrize("depth", [2, 4])
+@pytest.mark.parametrize("tag", ["even", "odd"])
+def test_reference_convergence_suite_anderson(ls, golden, tag, depth):
+    """tests/test_lippmann_schwinger.py:64-99 with Anderson depth 2 and 4, FP32 and FP64."""
+    from jaxmaterials_b200 import GridSpec
+
+    n = PY_SIZES[tag]
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    og = O.Grid(*n, *EXT)
+    _, sig, it = ls.lippmann_schwinger(lm, mu, EPS_BAR, g, rtol=1e-20, atol=1e-5, depth=depth,
+                                       maxiter=32)
+    assert it < 8
+    assert O.relative_divergence(sig.astype(np.float64), og) < 1e-5
+    assert abs(it - int(golden[f"big_{tag}_f32_d{depth}_iter"])) <= 1
+    eb64 = np.array([2.1, 0.9, 0.8, 0.4, 0.9, 0.5])
+    _, sig, it = ls.lippmann_schwinger(lm, mu, eb64, g, rtol=1e-20, atol=1e-12, depth=depth,
+                                       maxiter=32, dtype=np.float64)
+    assert it < {2: 14, 4: 13}[depth]
+    assert O.relative_divergence(sig, og) < 1e-12
+    assert it == int(golden[f"big_{tag}_f64_d{depth}_iter"])
+
+
+def test_anderson_ceff_at_128(ls):
+    """Config 2: 128^3, Anderson m=5, tol 1e-6: every load converges and C_eff is within
+    1e-5 of the FP64 oracle (Anderson m=5 run of the same structure)."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+
+    st = fibres.config_structure("c2_128", seed=0)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(128, 128, 128, 128.0, 128.0, 128.0)
+    s = ls.Solver(g, batch=6, depth=5)
+    r = s.solve(lm, mu, np.eye(6, dtype=np.float32), rtol=1e-6, atol=1e-20, maxiter=2000,
+                want_sigma=False)
+    assert np.all(r.status == ls.CONVERGED), r.status
+    fx = np.load(os.path.join(ROOT, "tests", "golden", "bench_c2_128.npz"))
+    ref = fx["ceff_d5"]
+    assert np.linalg.norm(r.mean_sigma - ref) / np.linalg.norm(ref) < 1e-5
+    assert np.all(r.iters <= 1.25 * fx["iters_d5"]), (r.iters, fx["iters_d5"])
+    s.close()
