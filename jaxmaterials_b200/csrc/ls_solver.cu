@@ -18,14 +18,16 @@
 #include <vector>
 
 #include "../../include/lippmann_schwinger.h"
-#include "fast_passes.cuh"
-#include "ls_kernels.cuh"
+#include "ls_solver_impl.cuh"
 
 using namespace lsb;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace lsb {
+namespace detail {
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -76,65 +78,17 @@ bool shape_fits(const LaunchShape& sh) {
   return sh.z_threads <= kMaxThreads && sh.y_threads <= kMaxThreads && sh.x_threads <= kMaxThreads;
 }
 
-}  // namespace
+}  // namespace detail
+}  // namespace lsb
 
-struct lsb_solver {
-  int device = 0;
-  int batch_cap = 0;
-  int depth = 0;
-  int precision = kPrecMixed;
-  int stall_window = 8;
-  bool fast32 = false;   // FP32 passes with compile-time power-of-two lengths
-  GridDesc g{};
-  LaunchShape sh32{}, sh64{};
-  cudaStream_t stream = nullptr;
-  // FP32 work buffers
-  float* d_eps32 = nullptr;      // [batch][6][nv] (used when the caller passes no strain buffer)
-  float2* d_spec32 = nullptr;    // [batch][6][nm]
-  // FP64 work buffers, allocated on first use
-  double* d_eps64 = nullptr;
-  double2* d_spec64 = nullptr;
-  double* d_lame64 = nullptr;    // [2][nv]
-  // Anderson acceleration (depth > 0): rings of g = eps + r and r, Gram matrices, coefficients
-  float* d_aa_g32 = nullptr;     // [batch][m+1][6][nv]
-  float* d_aa_r32 = nullptr;
-  double* d_aa_g64 = nullptr;    // FP64 rings, allocated for FP64 runs
-  double* d_aa_r64 = nullptr;
-  double* d_aa_partials = nullptr;  // [batch][z blocks][m+1]
-  double* d_aa_mat = nullptr;    // [batch][m+1][m+1]
-  double* d_aa_alpha = nullptr;  // [batch][m+1]
-  int aa_zblocks = 0;
-  // shared
-  double* d_partials = nullptr;  // [batch][x blocks]
-  InstanceState* d_state = nullptr;
-  Medium* d_medium = nullptr;
-  double* d_epsbar = nullptr;    // [batch][6]
-  double* d_scratch = nullptr;   // 6 * 1024
-  double* d_mean_scratch = nullptr;
-  double* d_mean = nullptr;      // [batch][6]
-  double* d_history = nullptr;   // [batch][history_len]
-  int history_len = 0;
-  int last_batch = 0;
-  float2* d_tw32 = nullptr;
-  double2* d_tw64 = nullptr;
-  double* d_tables = nullptr;
-  InstanceState* h_state = nullptr;  // pinned
-  long long launches = 0;            // kernels enqueued by this solver
+using namespace lsb::detail;
 
-  ~lsb_solver() {
-    void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
-                    d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
-                    d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
-                    d_aa_alpha};
-    for (void* p : bufs) cudaFree(p);
-    if (h_state) cudaFreeHost(h_state);
-  }
-};
+
 
 namespace {
 
 int ensure_history(lsb_solver* s, int len) {
-  if (len <= s->history_len) return 0;
+  if (len <= s->history_len || !s->owns_memory) return 0;
   cudaFree(s->d_history);
   s->d_history = nullptr;
   LSB_CUDA(cudaMalloc(&s->d_history, sizeof(double) * (size_t)s->batch_cap * len));
@@ -176,21 +130,18 @@ AndersonArgs<T> anderson_args(lsb_solver* s, bool on) {
   return a;
 }
 
-int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], int batch, int depth) {
-  if (!out || !voxels || !extents) return fail(-1, "null argument");
-  *out = nullptr;
+}  // namespace
+
+namespace lsb {
+namespace detail {
+
+int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]) {
   for (int d = 0; d < 3; ++d) {
     if (voxels[d] < 1 || voxels[d] > kMaxDim)
       return fail(-1, "voxels[%d] = %d outside [1, %d]", d, voxels[d], kMaxDim);
-    if (!(extents[d] > 0.f) || !std::isfinite(extents[d]))
+    if (!(extents[d] > 0.0) || !std::isfinite(extents[d]))
       return fail(-1, "extents[%d] must be positive and finite", d);
   }
-  if (batch < 1) return fail(-1, "batch must be >= 1");
-  if (depth < 0 || depth > kMaxDepth) return fail(-1, "Anderson depth %d outside [0, %d]", depth, kMaxDepth);
-  auto* s = new lsb_solver();
-  s->batch_cap = batch;
-  s->depth = depth;
-  cudaGetDevice(&s->device);
   GridDesc& g = s->g;
   g.nx = voxels[0];
   g.ny = voxels[1];
@@ -201,19 +152,81 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   g.Lx = extents[0];
   g.Ly = extents[1];
   g.Lz = extents[2];
-  if (!factorize(g.nx, g.px) || !factorize(g.ny, g.py) || !factorize(g.nz, g.pz)) {
-    delete s;
+  if (!factorize(g.nx, g.px) || !factorize(g.ny, g.py) || !factorize(g.nz, g.pz))
     return fail(-1, "grid extent has too many prime factors");
-  }
   s->sh32 = plan_launch(g, sizeof(float2));
   s->sh64 = plan_launch(g, sizeof(double2));
   s->fast32 = fast::supported(g);
   if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g) * g.ny;
-  if (!shape_fits(s->sh32) || !shape_fits(s->sh64)) {
-    delete s;
+  if (!shape_fits(s->sh32) || !shape_fits(s->sh64))
     return fail(-1, "grid %dx%dx%d needs FFT blocks above %d threads", g.nx, g.ny, g.nz, kMaxThreads);
+  cudaError_t e = configure_kernels();
+  if (e == cudaSuccess) e = fast::configure();
+  if (e != cudaSuccess) return fail(-2, "kernel configuration: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+int upload_tables(lsb_solver* s) {
+  GridDesc& g = s->g;
+  const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
+  // twiddles exp(-2 pi i k / n) and the sin/cos tables of the modified wave vectors,
+  // both evaluated in FP64 (fourier.py:29-31: xi_d / 2 = pi k_d / N_d)
+  std::vector<float2> tw32;
+  std::vector<double2> tw64;
+  for (int n : {g.nx, g.ny, g.nz})
+    for (int k = 0; k < n; ++k) {
+      double a = -2.0 * M_PI * (double)k / (double)n;
+      double c = std::cos(a), sn = std::sin(a);
+      tw32.push_back(make_float2((float)c, (float)sn));
+      tw64.push_back(make_double2(c, sn));
+    }
+  std::vector<double> tab;
+  auto add_tab = [&](int n, int count) {
+    for (int k = 0; k < count; ++k) tab.push_back(std::sin((2.0 * M_PI * k / n) / 2.0));
+    for (int k = 0; k < count; ++k) tab.push_back(std::cos((2.0 * M_PI * k / n) / 2.0));
+  };
+  add_tab(g.nx, g.nx);
+  add_tab(g.ny, g.ny);
+  add_tab(g.nz, g.nzh);
+  if (cudaMemcpy(s->d_tw32, tw32.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->d_tw64, tw64.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->d_tables, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(-2, "upload of twiddle tables failed");
+  g.px.tw = s->d_tw32;
+  g.py.tw = s->d_tw32 + g.nx;
+  g.pz.tw = s->d_tw32 + g.nx + g.ny;
+  g.px.tw64 = s->d_tw64;
+  g.py.tw64 = s->d_tw64 + g.nx;
+  g.pz.tw64 = s->d_tw64 + g.nx + g.ny;
+  g.sx = s->d_tables;
+  g.cx = g.sx + g.nx;
+  g.sy = g.cx + g.nx;
+  g.cy = g.sy + g.ny;
+  g.sz = g.cy + g.ny;
+  g.cz = g.sz + g.nzh;
+  return 0;
+}
+
+}  // namespace detail
+}  // namespace lsb
+
+namespace {
+
+int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], int batch, int depth) {
+  if (!out || !voxels || !extents) return fail(-1, "null argument");
+  *out = nullptr;
+  if (batch < 1) return fail(-1, "batch must be >= 1");
+  if (depth < 0 || depth > kMaxDepth) return fail(-1, "Anderson depth %d outside [0, %d]", depth, kMaxDepth);
+  auto* s = new lsb_solver();
+  s->batch_cap = batch;
+  s->depth = depth;
+  cudaGetDevice(&s->device);
+  int rc = plan_grid(s, voxels, extents);
+  if (rc) {
+    delete s;
+    return rc;
   }
-  int rc = 0;
+  const GridDesc& g = s->g;
   auto alloc = [&](void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) rc = fail(-3, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
@@ -256,48 +269,10 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
     delete s;
     return fail(-3, "cudaMallocHost failed");
   }
-  // twiddles exp(-2 pi i k / n) and the sin/cos tables of the modified wave vectors,
-  // both evaluated in FP64 (fourier.py:29-31: xi_d / 2 = pi k_d / N_d)
-  std::vector<float2> tw32;
-  std::vector<double2> tw64;
-  for (int n : {g.nx, g.ny, g.nz})
-    for (int k = 0; k < n; ++k) {
-      double a = -2.0 * M_PI * (double)k / (double)n;
-      double c = std::cos(a), sn = std::sin(a);
-      tw32.push_back(make_float2((float)c, (float)sn));
-      tw64.push_back(make_double2(c, sn));
-    }
-  std::vector<double> tab;
-  auto add_tab = [&](int n, int count) {
-    for (int k = 0; k < count; ++k) tab.push_back(std::sin((2.0 * M_PI * k / n) / 2.0));
-    for (int k = 0; k < count; ++k) tab.push_back(std::cos((2.0 * M_PI * k / n) / 2.0));
-  };
-  add_tab(g.nx, g.nx);
-  add_tab(g.ny, g.ny);
-  add_tab(g.nz, g.nzh);
-  if (cudaMemcpy(s->d_tw32, tw32.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(s->d_tw64, tw64.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(s->d_tables, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+  rc = upload_tables(s);
+  if (rc) {
     delete s;
-    return fail(-2, "upload of twiddle tables failed");
-  }
-  g.px.tw = s->d_tw32;
-  g.py.tw = s->d_tw32 + g.nx;
-  g.pz.tw = s->d_tw32 + g.nx + g.ny;
-  g.px.tw64 = s->d_tw64;
-  g.py.tw64 = s->d_tw64 + g.nx;
-  g.pz.tw64 = s->d_tw64 + g.nx + g.ny;
-  g.sx = s->d_tables;
-  g.cx = g.sx + g.nx;
-  g.sy = g.cx + g.nx;
-  g.cy = g.sy + g.ny;
-  g.sz = g.cy + g.ny;
-  g.cz = g.sz + g.nzh;
-  cudaError_t e = configure_kernels();
-  if (e == cudaSuccess) e = fast::configure();
-  if (e != cudaSuccess) {
-    delete s;
-    return fail(-2, "kernel configuration: %s", cudaGetErrorString(e));
+    return rc;
   }
   *out = s;
   return 0;
@@ -413,6 +388,11 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   }
 }
 
+}  // namespace
+
+namespace lsb {
+namespace detail {
+
 // Full solve with FP32 inputs/outputs. d_eps (FP32) is the FP32 work buffer and output.
 int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
               const double* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,
@@ -433,7 +413,8 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   if (s->precision != kPrecFP32) LSB_TRY(ensure_fp64(s));
 
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
-  LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
+  if (s->d_history)
+    LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
   launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st);
   launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
@@ -481,6 +462,11 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   s->last_batch = batch;
   return 0;
 }
+
+}  // namespace detail
+}  // namespace lsb
+
+namespace {
 
 // Full solve with FP64 inputs/outputs (FP64 fields throughout).
 int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_mu,

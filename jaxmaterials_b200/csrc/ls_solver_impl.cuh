@@ -1,0 +1,90 @@
+// Internal declarations shared by the host-side translation units of the library
+// (the solver handle and the driver entry points).
+#pragma once
+
+#include <cstdarg>
+#include <vector>
+
+#include "fast_passes.cuh"
+#include "ls_kernels.cuh"
+
+using namespace lsb;  // internal header: only the library's own translation units include it
+
+struct lsb_solver {
+  // Device buffers, launch shapes and plans of one grid; see ls_solver.cu.
+  int device = 0;
+  int batch_cap = 0;
+  int depth = 0;
+  int precision = kPrecMixed;
+  int stall_window = 8;
+  bool fast32 = false;   // FP32 passes with compile-time power-of-two lengths
+  GridDesc g{};
+  LaunchShape sh32{}, sh64{};
+  cudaStream_t stream = nullptr;
+  // FP32 work buffers
+  float* d_eps32 = nullptr;      // [batch][6][nv] (used when the caller passes no strain buffer)
+  float2* d_spec32 = nullptr;    // [batch][6][nm]
+  // FP64 work buffers, allocated on first use
+  double* d_eps64 = nullptr;
+  double2* d_spec64 = nullptr;
+  double* d_lame64 = nullptr;    // [2][nv]
+  // Anderson acceleration (depth > 0): rings of g = eps + r and r, Gram matrices, coefficients
+  float* d_aa_g32 = nullptr;     // [batch][m+1][6][nv]
+  float* d_aa_r32 = nullptr;
+  double* d_aa_g64 = nullptr;    // FP64 rings, allocated for FP64 runs
+  double* d_aa_r64 = nullptr;
+  double* d_aa_partials = nullptr;  // [batch][z blocks][m+1]
+  double* d_aa_mat = nullptr;    // [batch][m+1][m+1]
+  double* d_aa_alpha = nullptr;  // [batch][m+1]
+  int aa_zblocks = 0;
+  // shared
+  double* d_partials = nullptr;  // [batch][x blocks]
+  InstanceState* d_state = nullptr;
+  Medium* d_medium = nullptr;
+  double* d_epsbar = nullptr;    // [batch][6]
+  double* d_scratch = nullptr;   // 6 * 1024
+  double* d_mean_scratch = nullptr;
+  double* d_mean = nullptr;      // [batch][6]
+  double* d_history = nullptr;   // [batch][history_len]
+  int history_len = 0;
+  int last_batch = 0;
+  float2* d_tw32 = nullptr;
+  double2* d_tw64 = nullptr;
+  double* d_tables = nullptr;
+  InstanceState* h_state = nullptr;  // pinned
+  long long launches = 0;            // kernels enqueued by this solver
+  // false for a solver whose buffers point into memory it does not own (they are never
+  // freed, and the criterion history is not kept)
+  bool owns_memory = true;
+
+  ~lsb_solver() {
+    if (!owns_memory) return;
+    void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
+                    d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
+                    d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
+                    d_aa_alpha};
+    for (void* p : bufs) cudaFree(p);
+    if (h_state) cudaFreeHost(h_state);
+  }
+};
+
+namespace lsb {
+namespace detail {
+
+// Records a formatted message for lsb_last_error() and returns `code`.
+int fail(int code, const char* fmt, ...);
+// Radices of a length-n Stockham plan; false when n has too many prime factors.
+bool factorize(int n, Plan1D& p);
+// Fills s->g from voxels/extents, plans the launches and checks block sizes.
+int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]);
+// Uploads the twiddle and sin/cos tables into s->d_tw32/d_tw64/d_tables and points the
+// plans of s->g at them (the buffers must be sized for the grid).
+int upload_tables(lsb_solver* s);
+// Full FP32-input solve (see lsb_solve); d_eps is the FP32 work buffer and output.
+int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
+              const double* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,
+              double* mean_sigma, double rtol, double atol, int maxiter, int rule, int* iters,
+              int* status, double* residual);
+
+}  // namespace detail
+}  // namespace lsb
