@@ -128,6 +128,25 @@ int lsb_c_eff(const float *lambda, const float *mu, const int voxels[3],
               const double extents[3], float rtol, float atol, int maxiter, int depth,
               double *c_eff, int *iters);
 
+/* No reference counterpart. lsb_solve without any allocation, for callers that cannot
+ * call cudaMalloc: code running inside a framework that owns all device memory (a
+ * caching allocator, or a custom-operator interface that forbids allocation while it
+ * runs) and latency-critical callers that must not pay cudaMalloc's implicit device
+ * synchronisation. Inputs and outputs are the caller's (device pointers as in lsb_solve,
+ * eps_bar host float[batch*6]); all other scratch comes from one static device array of
+ * LSB_NOALLOC_SCRATCH_BYTES bytes per GPU, kept until the process exits (a 32^3 grid
+ * with 6 load cases needs about 5.5 MB of it). Larger grids or batches are rejected with
+ * an error. The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that call before any stream capture on the device. Every
+ * call reuses the array: calls whose GPU work overlaps in time race and must not be
+ * issued. FP32 fields, plain iteration, stop rule LSB_RULE_CUDA, FP32 stall detection
+ * (status LSB_STALLED), no criterion history; runs on the legacy default stream. */
+#define LSB_NOALLOC_SCRATCH_BYTES (8u << 20)
+int lsb_solve_noalloc(const int voxels[3], const double extents[3], int batch,
+                      const float *d_lambda, const float *d_mu, const float *eps_bar,
+                      float *d_eps, float *d_sigma, double *mean_sigma, float rtol,
+                      float atol, int maxiter, int *iters, int *status, double *residual);
+
 /* Message of the last error on this thread ("" if none). */
 const char *lsb_last_error(void);
 /* Library ABI version. */

@@ -47,6 +47,10 @@ SIGNATURES = {
     "lsb_c_eff": (ctypes.c_int, [c_float_p, c_float_p, c_int_p, c_double_p, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_int, ctypes.c_int, c_double_p,
                                  c_int_p]),
+    "lsb_solve_noalloc": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_int, c_void_p, c_void_p,
+                                         c_float_p, c_void_p, c_void_p, c_double_p,
+                                         ctypes.c_float, ctypes.c_float, ctypes.c_int, c_int_p,
+                                         c_int_p, c_double_p]),
     "lsb_last_error": (ctypes.c_char_p, []),
     "lsb_version": (ctypes.c_int, []),
 }
