@@ -88,18 +88,28 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (kYT * Split<NY>::P
 }
 
 // ----------------------------------------------------------------------------- x pass
-// Block = (TX kz columns, ky, instance); thread (c, p, t) with t fastest.
+// Block = (TX kz columns, ky, instance); thread (c, p, t) with t fastest. Component c owns
+// a shared-memory region holding either the natural layout [kx][t] or the transposed
+// layout [k1][p][t] with rows of P*T + T values (the padding makes the column reads of
+// the second step conflict-free).
 template <int NX>
 __host__ __device__ constexpr int x_cols() { return NX <= 32 ? 16 : (NX == 256 ? 4 : 8); }
+template <int NX>
+__host__ __device__ constexpr int x_row() { return Split<NX>::P * x_cols<NX>() + x_cols<NX>(); }
+template <int NX>
+__host__ __device__ constexpr int x_region() {
+  return Split<NX>::E * x_row<NX>() > NX * x_cols<NX>() ? Split<NX>::E * x_row<NX>() : NX * x_cols<NX>();
+}
 
 template <int NX>
 __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast(
     GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
     InstanceState* __restrict__ st, double* __restrict__ partials) {
-  constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols<NX>();
+  constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols<NX>(), RS = x_row<NX>(), REG = x_region<NX>();
   extern __shared__ __align__(16) unsigned char xfraw[];
-  float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 * NX * T values
+  float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
   __shared__ double red[32];
+  __shared__ double colf[3][T];  // per-column wave-vector factors
   const int b = blockIdx.z;
   if (!active32(st[b])) return;
   const int tid = threadIdx.x;
@@ -112,7 +122,16 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
   const size_t xstride = (size_t)g.ny * nzh;
   float2* gcol = spec + (size_t)b * 6 * g.nm + (size_t)c * g.nm + (size_t)ky * nzh + kz;
   const float2* tw = g.px.tw;
-  float2* tr = buf + (size_t)c * NX * T;   // this component's region
+  float2* tr = buf + (size_t)c * REG;   // this component's region
+
+  if (tid < T) {
+    // tilde(xi)_d = (2 n_d / L_d) * sin/cos products (fourier.py:9-58); the ky and kz
+    // factors of this block's columns, FP64
+    const int kzz = kz0 + tid < nzh ? kz0 + tid : 0;
+    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[ky] * g.cz[kzz];
+    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[ky] * g.cz[kzz];
+    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[ky] * g.sz[kzz];
+  }
 
   // forward: load, step A, transpose
   float2 v[E];
@@ -120,7 +139,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
   for (int e = 0; e < E; ++e) v[e] = valid ? gcol[(size_t)(p + P * e) * xstride] : make_float2(0.f, 0.f);
   step_a<NX>(v, p, tw);
 #pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) tr[(k1 * P + p) * T + t] = v[k1];
+  for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
   __syncthreads();
   float2 o[E];  // outputs X[k1 + E k2] for k1 = p + P j: o[j * P + k2]
 #pragma unroll
@@ -128,7 +147,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
     const int k1 = p + P * j;
     float2 w[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) w[q] = tr[(k1 * P + q) * T + t];
+    for (int q = 0; q < P; ++q) w[q] = tr[k1 * RS + q * T + t];
     Bfly<P>::run(w);
 #pragma unroll
     for (int k2 = 0; k2 < P; ++k2) o[j * P + k2] = w[k2];
@@ -142,7 +161,6 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
 
   // residual partials, zero mode, Gamma^0 (written conjugated for the inverse transform)
   const float c_a = med->c_a, c_b = med->c_b;
-  const double sxs = 2.0 * g.nx / g.Lx, sys = 2.0 * g.ny / g.Ly, szs = 2.0 * g.nz / g.Lz;
   double acc = 0.0;
   for (int idx = tid; idx < NX * T; idx += blockDim.x) {
     const int kx = idx / T, tt = idx % T;
@@ -150,10 +168,11 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
     if (kzz >= nzh) continue;
     float2 s[6];
 #pragma unroll
-    for (int cc = 0; cc < 6; ++cc) s[cc] = buf[((size_t)cc * NX + kx) * T + tt];
-    const double x0 = sxs * g.sx[kx] * g.cy[ky] * g.cz[kzz];
-    const double x1 = sys * g.cx[kx] * g.sy[ky] * g.cz[kzz];
-    const double x2 = szs * g.cx[kx] * g.cy[ky] * g.sz[kzz];
+    for (int cc = 0; cc < 6; ++cc) s[cc] = buf[(size_t)cc * REG + kx * T + tt];
+    const double sxk = g.sx[kx], cxk = g.cx[kx];
+    const double x0 = sxk * colf[0][tt];
+    const double x1 = cxk * colf[1][tt];
+    const double x2 = cxk * colf[2][tt];
     {
       const float f0 = (float)x0, f1 = (float)x1, f2 = (float)x2;
       float2 d0 = make_float2(f0 * s[0].x + f1 * s[3].x + f2 * s[4].x, f0 * s[0].y + f1 * s[3].y + f2 * s[4].y);
@@ -170,9 +189,10 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
         st[b].sig0[2 * cc + 1] = (double)s[cc].y;
       }
     }
-    double nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-    if (nrm < 1.0e-12) nrm = 1.0;
-    const float z0 = (float)(x0 / nrm), z1 = (float)(x1 / nrm), z2 = (float)(x2 / nrm);
+    // normalised wave vector: |xi| < 1e-12 (|xi|^2 < 1e-24) is replaced by 1 (fourier.py:84)
+    const double n2 = x0 * x0 + x1 * x1 + x2 * x2;
+    const double inv = n2 < 1.0e-24 ? 1.0 : rsqrt(n2);
+    const float z0 = (float)(x0 * inv), z1 = (float)(x1 * inv), z2 = (float)(x2 * inv);
     const float z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
     const float z01 = z0 * z1, z02 = z0 * z2, z12 = z1 * z2;
     float r[2][6];
@@ -195,7 +215,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
       r[part][5] = c_a * a5 + c_b * rho * z12;
     }
 #pragma unroll
-    for (int cc = 0; cc < 6; ++cc) buf[((size_t)cc * NX + kx) * T + tt] = make_float2(r[0][cc], -r[1][cc]);
+    for (int cc = 0; cc < 6; ++cc) buf[(size_t)cc * REG + kx * T + tt] = make_float2(r[0][cc], -r[1][cc]);
   }
   __syncthreads();
 
@@ -205,14 +225,14 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
   step_a<NX>(v, p, tw);
   __syncthreads();
 #pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) tr[(k1 * P + p) * T + t] = v[k1];
+  for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < E / P; ++j) {
     const int k1 = p + P * j;
     float2 w[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) w[q] = tr[(k1 * P + q) * T + t];
+    for (int q = 0; q < P; ++q) w[q] = tr[k1 * RS + q * T + t];
     Bfly<P>::run(w);
     if (valid) {
 #pragma unroll
@@ -238,10 +258,36 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
 
 // ----------------------------------------------------------------------------- z pass
 // Block = L (x, y) lines = 3L complex pair lines; thread (line q, p), p fastest.
+// The block's inputs (spectrum rows, strain rows, lambda/mu rows) are contiguous chunks;
+// one thread issues them as TMA bulk copies into shared memory (completion on an
+// mbarrier), so all of a block's loads are in flight at once and two resident blocks per
+// SM overlap one block's loads with the other's transforms.
 template <int NZ>
-__host__ __device__ constexpr int z_lines() { return 128 / Split<NZ>::P; }
+__host__ __device__ constexpr int z_lines() { return 192 / (3 * Split<NZ>::P); }
+// Line pitch of the transform buffer: room for the padded transposed layout
+// k1 * (P + 1) + p (conflict-free column reads), and = 8 (mod 16) so that the two lines
+// of a half-warp fall in disjoint banks.
 template <int NZ>
-__host__ __device__ constexpr int z_ld() { return NZ + (Split<NZ>::P == 4 ? 4 : 8); }
+__host__ __device__ constexpr int z_ld() {
+  return ((Split<NZ>::E * (Split<NZ>::P + 1) > NZ ? Split<NZ>::E * (Split<NZ>::P + 1) : NZ) + 7) / 16 * 16 + 8;
+}
+
+struct ZLayout {  // byte offsets inside the z pass's dynamic shared memory
+  size_t zbuf, rst, est, lst, total;
+};
+template <int NZ>
+__host__ __device__ constexpr ZLayout z_layout() {
+  constexpr int L = z_lines<NZ>(), NZH = NZ / 2 + 1;
+  constexpr size_t zb = (size_t)3 * L * z_ld<NZ>() * 8;
+  constexpr size_t rs = (size_t)6 * L * NZH * 8;
+  constexpr size_t es = (size_t)6 * L * NZ * 4;
+  constexpr size_t ls = (size_t)2 * L * NZ * 4;
+  return ZLayout{0, zb, zb + rs, zb + rs + es, zb + rs + es + ls};
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
 
 // In-place four-step FFT of the 3L lines of zbuf (natural order in and out).
 template <int NZ>
@@ -254,14 +300,14 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
   step_a<NZ>(v, p, tw);
   __syncthreads();
 #pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) line[k1 * P + p] = v[k1];
+  for (int k1 = 0; k1 < E; ++k1) line[k1 * (P + 1) + p] = v[k1];
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < E / P; ++j) {
     const int k1 = p + P * j;
     float2 w[P];
 #pragma unroll
-    for (int qq = 0; qq < P; ++qq) w[qq] = line[k1 * P + qq];
+    for (int qq = 0; qq < P; ++qq) w[qq] = line[k1 * (P + 1) + qq];
     Bfly<P>::run(w);
 #pragma unroll
     for (int k2 = 0; k2 < P; ++k2) v[j * P + k2] = w[k2];
@@ -274,18 +320,45 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
   __syncthreads();
 }
 
+// Bounded wait on a one-shot mbarrier (phase 0). Returns false if the copies did not
+// complete within the limit.
+__device__ __forceinline__ bool mbar_wait(unsigned mbar) {
+  for (long long spin = 0; spin < (1LL << 24); ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done) : "r"(mbar), "r"(0u) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
 // Modes as the generic z pass: 0 init from eps_bar/eps0, 1 plain update, 2 keep eps,
 // 3 Anderson residual (rings + Gram-row partials), 4 Anderson combine.
+// bulk: the block's global chunks are 16-byte aligned (TMA bulk copies); otherwise the
+// staging buffers are filled by ordinary loads.
 template <int NZ>
-__global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fast(
-    GridDesc g, int mode, const float* __restrict__ lambda, const float* __restrict__ mu,
+__global__ void __launch_bounds__(192, 2) zpass_fast(
+    GridDesc g, int mode, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
     const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med,
     AndersonArgs<float> aa) {
   constexpr int P = Split<NZ>::P, L = z_lines<NZ>(), LD = z_ld<NZ>(), NZH = NZ / 2 + 1;
-  extern __shared__ __align__(16) unsigned char zfraw[];
-  float2* zbuf = reinterpret_cast<float2*>(zfraw);   // 3L lines of LD values
+  constexpr ZLayout LY = z_layout<NZ>();
+  extern __shared__ __align__(128) unsigned char zfraw[];
+  float2* zbuf = reinterpret_cast<float2*>(zfraw + LY.zbuf);  // 3L lines of LD values
+  float2* rst = reinterpret_cast<float2*>(zfraw + LY.rst);    // [6][L][NZH] spectrum rows
+  float* est = reinterpret_cast<float*>(zfraw + LY.est);      // [6][L][NZ] strain rows
+  float* lst = reinterpret_cast<float*>(zfraw + LY.lst);      // [2][L][NZ] lambda, mu rows
   __shared__ double gred[kMaxDepth + 1][32];
+  __shared__ __align__(8) unsigned long long mbar_word;
   const int b = blockIdx.y;
   if (!active32(st[b])) return;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -295,16 +368,63 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
   float* eb = eps + (size_t)b * 6 * g.nv;
   float2* sb = spec + (size_t)b * 6 * g.nm;
   const float2* tw = g.pz.tw;
+  const bool need_r = (mode == 1 || mode == 3);
+  const bool need_e = (mode == 1 || mode == 2 || mode == 3);
+  const bool need_l = (mode != 3);
 
-  if (mode == 1 || mode == 3) {
+  // ---- stage this block's inputs in shared memory
+  if (bulk) {
+    const unsigned mbar = smem_u32(&mbar_word);
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mbar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const unsigned rbytes = L * NZH * 8, ebytes = L * NZ * 4;
+      const unsigned total = (need_r ? 6 * rbytes : 0) + (need_e ? 6 * ebytes : 0) + (need_l ? 2 * ebytes : 0);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(total) : "memory");
+      for (int c = 0; c < 6; ++c) {
+        if (need_r) bulk_g2s(rst + (size_t)c * L * NZH, sb + ((size_t)c * nlines + l0) * NZH, rbytes, mbar);
+        if (need_e) bulk_g2s(est + (size_t)c * L * NZ, eb + (size_t)c * g.nv + l0 * NZ, ebytes, mbar);
+      }
+      if (need_l) {
+        bulk_g2s(lst, lambda + l0 * NZ, ebytes, mbar);
+        bulk_g2s(lst + L * NZ, mu + l0 * NZ, ebytes, mbar);
+      }
+    }
+    if (!mbar_wait(mbar)) {
+      // the copies did not land in time: report and leave this instance stopped
+      if (tid == 0) {
+        st[b].status = kTimeout;
+        st[b].done = 1;
+      }
+      mbar_wait(mbar);
+      return;
+    }
+  } else {
+    for (int c = 0; c < 6; ++c) {
+      if (need_r)
+        for (int i = tid; i < L * NZH; i += nt) rst[c * L * NZH + i] = sb[((size_t)c * nlines + l0) * NZH + i];
+      if (need_e)
+        for (int i = tid; i < L * NZ; i += nt) est[c * L * NZ + i] = eb[(size_t)c * g.nv + l0 * NZ + i];
+    }
+    if (need_l)
+      for (int i = tid; i < L * NZ; i += nt) {
+        lst[i] = lambda[l0 * NZ + i];
+        lst[L * NZ + i] = mu[l0 * NZ + i];
+      }
+    __syncthreads();
+  }
+
+  if (need_r) {
+    // conj(Z) with Z[k] = A[k] + i B[k] (Hermitian extension; DC and Nyquist taken real)
     for (int idx = tid; idx < 3 * L * NZH; idx += nt) {
       const int pr = idx / (L * NZH);
       const int rem = idx - pr * (L * NZH);
       const int l = rem / NZH, k = rem - l * NZH;
-      const long long line = l0 + l;
-      if (line >= nlines) continue;
-      float2 A = sb[((size_t)(2 * pr) * nlines + line) * NZH + k];
-      float2 B = sb[((size_t)(2 * pr + 1) * nlines + line) * NZH + k];
+      float2 A = rst[(2 * pr) * L * NZH + rem];
+      float2 B = rst[(2 * pr + 1) * L * NZH + rem];
       const bool selfconj = (k == 0) || (2 * k == NZ);
       if (selfconj) { A.y = 0.f; B.y = 0.f; }
       float2* Z = zbuf + (size_t)(pr * L + l) * LD;
@@ -332,9 +452,7 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
     const float inv_nv = (float)(1.0 / (double)g.nv);
     for (int idx = tid; idx < L * NZ; idx += nt) {
       const int l = idx / NZ, n = idx % NZ;
-      const long long line = l0 + l;
-      if (line >= nlines) continue;
-      const size_t vx = (size_t)line * NZ + n;
+      const size_t vx = (size_t)(l0 + l) * NZ + n;
       float r[6];
 #pragma unroll
       for (int pr = 0; pr < 3; ++pr) {
@@ -346,7 +464,7 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
       for (int c = 0; c < 6; ++c) {
         const size_t o = (size_t)c * g.nv + vx;
         rb[slot * ring + o] = r[c];
-        gb[slot * ring + o] = eb[o] + r[c];
+        gb[slot * ring + o] = est[c * L * NZ + idx] + r[c];
       }
       for (int qq = 0; qq < filled; ++qq) {
         double d = 0.0;
@@ -393,20 +511,18 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
     const float inv_nv = (float)(1.0 / (double)g.nv);
     for (int idx = tid; idx < L * NZ; idx += nt) {
       const int l = idx / NZ, n = idx % NZ;
-      const long long line = l0 + l;
-      if (line >= nlines) continue;
-      const size_t vx = (size_t)line * NZ + n;
+      const size_t vx = (size_t)(l0 + l) * NZ + n;
       float e[6];
       if (mode == 1) {
 #pragma unroll
         for (int pr = 0; pr < 3; ++pr) {
           float2 w = zbuf[(size_t)(pr * L + l) * LD + n];
-          e[2 * pr] = eb[(size_t)(2 * pr) * g.nv + vx] + w.x * inv_nv;
-          e[2 * pr + 1] = eb[(size_t)(2 * pr + 1) * g.nv + vx] - w.y * inv_nv;
+          e[2 * pr] = est[(2 * pr) * L * NZ + idx] + w.x * inv_nv;
+          e[2 * pr + 1] = est[(2 * pr + 1) * L * NZ + idx] - w.y * inv_nv;
         }
       } else if (mode == 2) {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * g.nv + vx];
+        for (int c = 0; c < 6; ++c) e[c] = est[c * L * NZ + idx];
       } else if (mode == 4) {
         const float* gb = aa.g + (size_t)b * M1 * ring;
         const double* al = aa.alpha + (size_t)b * M1;
@@ -426,7 +542,7 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
       }
 #pragma unroll
       for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + vx] = e[c];
-      const float lam = lambda[vx], tmu = 2.f * mu[vx];
+      const float lam = lst[idx], tmu = 2.f * lst[L * NZ + idx];
       const float ltr = lam * (e[0] + e[1] + e[2]);
       float s[6];
 #pragma unroll
@@ -447,7 +563,6 @@ __global__ void __launch_bounds__(3 * z_lines<NZ>() * Split<NZ>::P, 2) zpass_fas
     const int rem = idx - pr * (L * NZH);
     const int l = rem / NZH, k = rem - l * NZH;
     const long long line = l0 + l;
-    if (line >= nlines) continue;
     const float2* Z = zbuf + (size_t)(pr * L + l) * LD;
     const float2 zk = Z[k];
     const float2 zm = Z[k == 0 ? 0 : NZ - k];
@@ -477,13 +592,13 @@ int x_tiles(const GridDesc& g) {
 }
 
 template <int N>
-static size_t zsmem() { return (size_t)3 * z_lines<N>() * z_ld<N>() * sizeof(float2); }
+static size_t zsmem() { return z_layout<N>().total; }
 template <int N>
 static int z_blocks_for(const GridDesc& g) {
   return (int)(((long long)g.nx * g.ny + z_lines<N>() - 1) / z_lines<N>());
 }
 template <int N>
-static size_t xsmem() { return (size_t)6 * N * x_cols<N>() * sizeof(float2); }
+static size_t xsmem() { return (size_t)6 * x_region<N>() * sizeof(float2); }
 
 template <int N>
 static cudaError_t configure_n() {
@@ -501,13 +616,17 @@ cudaError_t configure() {
   return configure_n<256>();
 }
 
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
 template <int N>
 static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
                     float* eps, float2* spec, const double* eps_bar, const float* eps0,
                     InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s) {
   dim3 grid((unsigned)z_blocks_for<N>(g), batch);
-  zpass_fast<N><<<grid, 3 * z_lines<N>() * Split<N>::P, zsmem<N>(), s>>>(g, mode, lambda, mu, eps, spec,
-                                                                          eps_bar, eps0, st, med, aa);
+  // every chunk offset is a multiple of 16 bytes when the base pointers are
+  const int bulk = aligned16(lambda) && aligned16(mu) && aligned16(eps) && aligned16(spec) ? 1 : 0;
+  zpass_fast<N><<<grid, 192, zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec, eps_bar, eps0,
+                                              st, med, aa);
 }
 
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,

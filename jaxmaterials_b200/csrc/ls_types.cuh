@@ -94,6 +94,7 @@ enum Status : int {
   kMaxIter = 2,
   kNonFinite = 3,
   kStalled = 4,   // FP32 round-off floor reached above the tolerance (FP32-only mode)
+  kTimeout = 5,   // a bounded wait for asynchronous copies ran out (the solve was abandoned)
 };
 
 // Per-instance iteration state, owned by the device.
