@@ -147,6 +147,20 @@ int lsb_solve_noalloc(const int voxels[3], const double extents[3], int batch,
                       float *d_eps, float *d_sigma, double *mean_sigma, float rtol,
                       float atol, int maxiter, int *iters, int *status, double *residual);
 
+/* No reference counterpart (the reference differentiates only forward-mode through
+ * JAX, src/driver.py:73-76). Gradient of a loss L of the effective stiffness M (row k =
+ * mean stress for the unit strain e_k, as lsb_c_eff) with respect to the Lame fields:
+ * d_eps holds the six converged strain fields of one microstructure, device
+ * [6 load cases][6][nv] (the output of a batch-6 lsb_solve with eps_bar = identity);
+ * dl_dc is host double[36] = dL/dM (row-major). Writes device d_dlambda[nv], d_dmu[nv].
+ * The six forward solutions are their own adjoints (the operator is self-adjoint in the
+ * energy inner product), so no further solve is needed. Runs on `stream`. */
+int lsb_ceff_gradient(const int voxels[3], const float *d_eps, const double *dl_dc,
+                      float *d_dlambda, float *d_dmu, void *stream);
+/* FP64 variant of lsb_ceff_gradient (fields of lsb_solve_f64). */
+int lsb_ceff_gradient_f64(const int voxels[3], const double *d_eps, const double *dl_dc,
+                          double *d_dlambda, double *d_dmu, void *stream);
+
 /* Message of the last error on this thread ("" if none). */
 const char *lsb_last_error(void);
 /* Library ABI version. */

@@ -51,6 +51,10 @@ SIGNATURES = {
                                          c_float_p, c_void_p, c_void_p, c_double_p,
                                          ctypes.c_float, ctypes.c_float, ctypes.c_int, c_int_p,
                                          c_int_p, c_double_p]),
+    "lsb_ceff_gradient": (ctypes.c_int, [c_int_p, c_void_p, c_double_p, c_void_p, c_void_p,
+                                         c_void_p]),
+    "lsb_ceff_gradient_f64": (ctypes.c_int, [c_int_p, c_void_p, c_double_p, c_void_p, c_void_p,
+                                             c_void_p]),
     "lsb_last_error": (ctypes.c_char_p, []),
     "lsb_version": (ctypes.c_int, []),
 }
