@@ -85,7 +85,16 @@ int lsb_set_stream(lsb_solver *solver, void *stream);
  * which FP32 round-off is taken to have stalled the iteration (default 8; 0 disables). */
 int lsb_set_precision(lsb_solver *solver, int precision, int stall_window);
 
-/* Solves `batch` instances that share d_lambda, d_mu (device float[nv]).
+/* No reference counterpart. Groups instances by microstructure: with
+ * instances_per_field = k > 0, instance b of a solve reads the Lame fields of structure
+ * b / k from d_lambda, d_mu laid out [batch / k][nv] (and gets that structure's own
+ * reference medium), so one launch sequence solves several structures, e.g. the six
+ * unit load cases of batch/6 structures with k = 6. batch must then be a multiple of k.
+ * k = 0 (default): every instance shares one field pair [nv]. */
+int lsb_set_lame_group(lsb_solver *solver, int instances_per_field);
+
+/* Solves `batch` instances that share d_lambda, d_mu (device float[nv]), or, after
+ * lsb_set_lame_group(solver, k), read structure b / k of [batch / k][nv] arrays.
  * eps_bar:   host float[batch*6]
  * d_eps0:    optional device float[batch*6*nv] warm start (NULL: eps = eps_bar)
  * d_eps:     device float[batch*6*nv] output strain
@@ -127,6 +136,21 @@ int lsb_profile_passes(lsb_solver *solver, int batch, const float *d_lambda,
 int lsb_c_eff(const float *lambda, const float *mu, const int voxels[3],
               const double extents[3], float rtol, float atol, int maxiter, int depth,
               double *c_eff, int *iters);
+
+/* Effective stiffness of a dataset: the loop over structures of
+ * src/jaxmaterials/data/data.py:148-186 (six unit-strain solves per structure, row k of
+ * C = mean stress for e_k) as batched solves on the current device. Structure i has
+ * voxels[3*i..3*i+2], extents[3*i..3*i+2] and host Lame fields lambda[i], mu[i]
+ * (float[nv_i]); grids may differ between structures. Structures of equal grid run
+ * together (instance b of a launch reads structure b / 6, each with its own reference
+ * medium and its own convergence), different grids concurrently on separate streams.
+ * depth: Anderson depth; precision: LSB_PREC_*; memory_gb: device memory the call may
+ * use (<= 0: 70% of the free memory). Outputs: c_eff host double[nstruct*36],
+ * iters and status host int[nstruct*6]. */
+int lsb_c_eff_batch(int nstruct, const int *voxels, const double *extents,
+                    const float *const *lambda, const float *const *mu, int depth,
+                    int precision, float rtol, float atol, int maxiter, double memory_gb,
+                    double *c_eff, int *iters, int *status);
 
 /* No reference counterpart. lsb_solve without any allocation, for callers that cannot
  * call cudaMalloc: code running inside a framework that owns all device memory (a

@@ -36,6 +36,12 @@ SIGNATURES = {
                                  ctypes.c_float, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
                                  c_double_p]),
     "lsb_set_precision": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
+    "lsb_set_lame_group": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "lsb_c_eff_batch": (ctypes.c_int, [ctypes.c_int, c_int_p, c_double_p,
+                                       ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                       ctypes.c_float, ctypes.c_int, ctypes.c_double,
+                                       c_double_p, c_int_p, c_int_p]),
     "lsb_solve_f64": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_double_p,
                                      c_void_p, c_void_p, c_void_p, c_double_p, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_int, ctypes.c_int, c_int_p,

@@ -1,0 +1,189 @@
+// lsb_c_eff_batch: effective stiffness of many microstructures of uneven grid sizes, six
+// unit load cases each -- the dataset loop of src/jaxmaterials/data/data.py:178-186 run
+// as batched solves on one GPU.
+//
+// Schedule. Structures are grouped into buckets of equal grid (voxels and extents). Each
+// bucket runs on its own host thread and CUDA stream, so the small-grid buckets fill the
+// GPU while a large-grid bucket's thread polls its convergence state. Inside a bucket
+// one solver holds `chunk` structures x 6 load cases; instance b reads the Lame fields
+// of structure b / 6 and its own reference medium, and retires at its own convergence
+// (kernels skip retired instances). The chunk is the largest that fits the bucket's share
+// of the memory budget (share proportional to the bucket's voxels); the chunks of a
+// bucket are evened out so that the last one is not a small remainder.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/lippmann_schwinger.h"
+#include "ls_solver_impl.cuh"
+
+using namespace lsb::detail;
+
+namespace {
+
+struct Bucket {
+  int voxels[3];
+  double extents[3];
+  std::vector<int> members;  // structure indices in input order
+  double voxels_total = 0.0;
+};
+
+// Device bytes one structure (6 instances) needs in a solver of the given configuration.
+size_t bytes_per_structure(long long nv, long long nm, int depth, int precision) {
+  const size_t inst32 = 24 * (size_t)nv + 48 * (size_t)nm +
+                        (depth > 0 ? 2 * (size_t)(depth + 1) * 24 * nv : 0) + 6 * 1024 * 8;
+  size_t inst64 = 0;
+  if (precision != LSB_PREC_FP32) {
+    inst64 = 48 * (size_t)nv + 96 * (size_t)nm;
+    if (precision == LSB_PREC_FP64 && depth > 0) inst64 += 2 * (size_t)(depth + 1) * 48 * nv;
+  }
+  const size_t lame = 8 * (size_t)nv + (precision != LSB_PREC_FP32 ? 16 * (size_t)nv : 0);
+  return 6 * (inst32 + inst64) + lame;
+}
+
+struct BucketResult {
+  int rc = 0;
+  std::string error;
+};
+
+void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int precision,
+                double rtol, double atol, int maxiter, const float* const* lambda,
+                const float* const* mu, double* c_eff, int* iters, int* status,
+                BucketResult* out) {
+  auto fail_here = [&](int rc) {
+    out->rc = rc;
+    out->error = lsb_last_error();
+  };
+  cudaSetDevice(device);
+  const long long nv = (long long)bk.voxels[0] * bk.voxels[1] * bk.voxels[2];
+  const long long nm = (long long)bk.voxels[0] * bk.voxels[1] * (bk.voxels[2] / 2 + 1);
+  const int n = (int)bk.members.size();
+  const size_t per = bytes_per_structure(nv, nm, depth, precision);
+  int chunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)n));
+  const int nchunks = (n + chunk - 1) / chunk;
+  chunk = (n + nchunks - 1) / nchunks;
+
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    out->rc = -2;
+    out->error = "cudaStreamCreate failed";
+    return;
+  }
+  lsb_solver* s = nullptr;
+  float* d_lame = nullptr;
+  int rc = lsb_create(&s, bk.voxels, bk.extents, 6 * chunk, depth);
+  if (rc) {
+    fail_here(rc);
+    cudaStreamDestroy(st);
+    return;
+  }
+  s->stream = st;
+  s->precision = precision;
+  s->lame_group = 6;
+  if (cudaMalloc(&d_lame, sizeof(float) * 2 * (size_t)chunk * nv) != cudaSuccess) {
+    out->rc = -3;
+    out->error = "cudaMalloc of the Lame fields of one chunk failed";
+  }
+  std::vector<double> eb(36 * (size_t)chunk, 0.0), mean(36 * (size_t)chunk);
+  for (int j = 0; j < chunk; ++j)
+    for (int k = 0; k < 6; ++k) eb[36 * j + 7 * k] = 1.0;
+  std::vector<int> it(6 * chunk), stt(6 * chunk);
+  for (int c0 = 0; c0 < n && out->rc == 0; c0 += chunk) {
+    const int c = std::min(chunk, n - c0);
+    for (int j = 0; j < c; ++j) {
+      const int m = bk.members[c0 + j];
+      cudaMemcpyAsync(d_lame + (size_t)j * nv, lambda[m], sizeof(float) * nv,
+                      cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(d_lame + (size_t)(c + j) * nv, mu[m], sizeof(float) * nv,
+                      cudaMemcpyHostToDevice, st);
+    }
+    rc = solve_f32(s, 6 * c, d_lame, d_lame + (size_t)c * nv, eb.data(), nullptr, s->d_eps32,
+                   nullptr, mean.data(), rtol, atol, maxiter, LSB_RULE_CUDA, it.data(),
+                   stt.data(), nullptr);
+    if (rc) {
+      fail_here(rc);
+      break;
+    }
+    for (int j = 0; j < c; ++j) {
+      const int m = bk.members[c0 + j];
+      std::memcpy(c_eff + 36 * (size_t)m, mean.data() + 36 * (size_t)j, sizeof(double) * 36);
+      std::memcpy(iters + 6 * (size_t)m, it.data() + 6 * (size_t)j, sizeof(int) * 6);
+      std::memcpy(status + 6 * (size_t)m, stt.data() + 6 * (size_t)j, sizeof(int) * 6);
+    }
+  }
+  cudaFree(d_lame);
+  lsb_destroy(s);
+  cudaStreamDestroy(st);
+}
+
+}  // namespace
+
+extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* extents,
+                               const float* const* lambda, const float* const* mu, int depth,
+                               int precision, float rtol, float atol, int maxiter,
+                               double memory_gb, double* c_eff, int* iters, int* status) {
+  if (nstruct < 0) return fail(-1, "nstruct must be >= 0");
+  if (nstruct == 0) return 0;
+  if (!voxels || !extents || !lambda || !mu || !c_eff || !iters || !status)
+    return fail(-1, "null argument");
+  if (depth < 0 || depth > kMaxDepth) return fail(-1, "Anderson depth %d outside [0, %d]", depth, kMaxDepth);
+  if (precision < LSB_PREC_FP32 || precision > LSB_PREC_FP64) return fail(-1, "unknown precision %d", precision);
+  if (maxiter < 0) return fail(-1, "maxiter must be >= 0");
+  for (int i = 0; i < nstruct; ++i)
+    if (!lambda[i] || !mu[i]) return fail(-1, "null Lame field of structure %d", i);
+
+  // buckets of equal grid, in order of first appearance
+  std::vector<Bucket> buckets;
+  std::map<std::vector<double>, int> index;
+  for (int i = 0; i < nstruct; ++i) {
+    const int* v = voxels + 3 * i;
+    const double* e = extents + 3 * i;
+    std::vector<double> key = {(double)v[0], (double)v[1], (double)v[2], e[0], e[1], e[2]};
+    auto f = index.find(key);
+    int b;
+    if (f == index.end()) {
+      b = (int)buckets.size();
+      index[key] = b;
+      Bucket nb;
+      std::memcpy(nb.voxels, v, sizeof(nb.voxels));
+      std::memcpy(nb.extents, e, sizeof(nb.extents));
+      buckets.push_back(nb);
+    } else {
+      b = f->second;
+    }
+    buckets[b].members.push_back(i);
+    buckets[b].voxels_total += (double)v[0] * v[1] * v[2];
+  }
+
+  int device = 0;
+  cudaGetDevice(&device);
+  size_t budget;
+  if (memory_gb > 0.0) {
+    budget = (size_t)(memory_gb * 1e9);
+  } else {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return fail(-2, "cudaMemGetInfo failed");
+    budget = (size_t)(0.7 * (double)free_b);
+  }
+  double total = 0.0;
+  for (const Bucket& b : buckets) total += b.voxels_total;
+
+  std::vector<BucketResult> res(buckets.size());
+  std::vector<std::thread> threads;
+  for (size_t b = 0; b < buckets.size(); ++b) {
+    const size_t share = (size_t)((double)budget * buckets[b].voxels_total / total);
+    threads.emplace_back(run_bucket, std::cref(buckets[b]), device, share, depth, precision,
+                         (double)rtol, (double)atol, maxiter, lambda, mu, c_eff, iters, status,
+                         &res[b]);
+  }
+  for (auto& t : threads) t.join();
+  for (size_t b = 0; b < buckets.size(); ++b)
+    if (res[b].rc)
+      return fail(res[b].rc, "bucket %dx%dx%d: %s", buckets[b].voxels[0], buckets[b].voxels[1],
+                  buckets[b].voxels[2], res[b].error.c_str());
+  return 0;
+}

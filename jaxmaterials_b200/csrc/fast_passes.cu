@@ -29,6 +29,15 @@ template <>
 struct Split<128> { static constexpr int E = 16, P = 8; };
 template <>
 struct Split<256> { static constexpr int E = 16, P = 16; };
+template <>
+struct Split<48> { static constexpr int E = 16, P = 3; };
+template <>
+struct Split<96> { static constexpr int E = 16, P = 6; };
+
+// Step B work per thread: the E DFTs of length P are dealt round-robin (k1 = p + P j);
+// when P does not divide E the last round is partial.
+template <int N>
+__host__ __device__ constexpr int rounds() { return (Split<N>::E + Split<N>::P - 1) / Split<N>::P; }
 
 __device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y); }
 
@@ -50,10 +59,10 @@ __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restric
 constexpr int kYT = 16;
 
 template <int NY>
-__global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (kYT * Split<NY>::P)) ypass_fast(GridDesc g, int inverse,
+__global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split<NY>::P + 31) / 32))) ypass_fast(GridDesc g, int inverse,
                                                                float2* __restrict__ spec,
                                                                const InstanceState* __restrict__ st) {
-  constexpr int E = Split<NY>::E, P = Split<NY>::P;
+  constexpr int E = Split<NY>::E, P = Split<NY>::P, NJ = rounds<NY>();
   __shared__ float2 buf[NY * kYT];
   const int bc = blockIdx.z;
   if (!active32(st[bc / 6])) return;
@@ -74,8 +83,9 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (kYT * Split<NY>::P
   for (int k1 = 0; k1 < E; ++k1) buf[(k1 * P + p) * kYT + t] = v[k1];
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < E / P; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const int k1 = p + P * j;
+    if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
     for (int q = 0; q < P; ++q) w[q] = buf[(k1 * P + q) * kYT + t];
@@ -93,7 +103,7 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (kYT * Split<NY>::P
 // layout [k1][p][t] with rows of P*T + T values (the padding makes the column reads of
 // the second step conflict-free).
 template <int NX>
-__host__ __device__ constexpr int x_cols() { return NX <= 32 ? 16 : (NX == 256 ? 4 : 8); }
+__host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ? 4 : 8); }
 template <int NX>
 __host__ __device__ constexpr int x_row() { return Split<NX>::P * x_cols<NX>() + x_cols<NX>(); }
 template <int NX>
@@ -106,6 +116,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
     GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
     InstanceState* __restrict__ st, double* __restrict__ partials) {
   constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols<NX>(), RS = x_row<NX>(), REG = x_region<NX>();
+  constexpr int NJ = rounds<NX>();
   extern __shared__ __align__(16) unsigned char xfraw[];
   float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
   __shared__ double red[32];
@@ -141,10 +152,11 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
 #pragma unroll
   for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
   __syncthreads();
-  float2 o[E];  // outputs X[k1 + E k2] for k1 = p + P j: o[j * P + k2]
+  float2 o[NJ * P];  // outputs X[k1 + E k2] for k1 = p + P j: o[j * P + k2]
 #pragma unroll
-  for (int j = 0; j < E / P; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const int k1 = p + P * j;
+    if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
     for (int q = 0; q < P; ++q) w[q] = tr[k1 * RS + q * T + t];
@@ -154,13 +166,15 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < E / P; ++j)
+  for (int j = 0; j < NJ; ++j)
+    if (p + P * j < E) {
 #pragma unroll
-    for (int k2 = 0; k2 < P; ++k2) tr[((p + P * j) + E * k2) * T + t] = o[j * P + k2];
+      for (int k2 = 0; k2 < P; ++k2) tr[((p + P * j) + E * k2) * T + t] = o[j * P + k2];
+    }
   __syncthreads();
 
   // residual partials, zero mode, Gamma^0 (written conjugated for the inverse transform)
-  const float c_a = med->c_a, c_b = med->c_b;
+  const float c_a = med[b / g.lame_group].c_a, c_b = med[b / g.lame_group].c_b;
   double acc = 0.0;
   for (int idx = tid; idx < NX * T; idx += blockDim.x) {
     const int kx = idx / T, tt = idx % T;
@@ -228,8 +242,9 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
   for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < E / P; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const int k1 = p + P * j;
+    if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
     for (int q = 0; q < P; ++q) w[q] = tr[k1 * RS + q * T + t];
@@ -263,7 +278,9 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast
 // mbarrier), so all of a block's loads are in flight at once and two resident blocks per
 // SM overlap one block's loads with the other's transforms.
 template <int NZ>
-__host__ __device__ constexpr int z_lines() { return 192 / (3 * Split<NZ>::P); }
+__host__ __device__ constexpr int z_lines() {
+  return Split<NZ>::P == 3 ? 16 : (Split<NZ>::P == 6 ? 8 : 192 / (3 * Split<NZ>::P));
+}
 // Line pitch of the transform buffer: room for the padded transposed layout
 // k1 * (P + 1) + p (conflict-free column reads), and = 8 (mod 16) so that the two lines
 // of a half-warp fall in disjoint banks.
@@ -292,9 +309,10 @@ __device__ __forceinline__ unsigned smem_u32(const void* p) {
 // In-place four-step FFT of the 3L lines of zbuf (natural order in and out).
 template <int NZ>
 __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const float2* __restrict__ tw) {
-  constexpr int E = Split<NZ>::E, P = Split<NZ>::P, LD = z_ld<NZ>();
+  constexpr int E = Split<NZ>::E, P = Split<NZ>::P, LD = z_ld<NZ>(), NJ = rounds<NZ>();
   float2* line = zbuf + (size_t)q * LD;
   float2 v[E];
+  float2 o[NJ * P];
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = line[p + P * e];
   step_a<NZ>(v, p, tw);
@@ -303,20 +321,23 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
   for (int k1 = 0; k1 < E; ++k1) line[k1 * (P + 1) + p] = v[k1];
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < E / P; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const int k1 = p + P * j;
+    if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
     for (int qq = 0; qq < P; ++qq) w[qq] = line[k1 * (P + 1) + qq];
     Bfly<P>::run(w);
 #pragma unroll
-    for (int k2 = 0; k2 < P; ++k2) v[j * P + k2] = w[k2];
+    for (int k2 = 0; k2 < P; ++k2) o[j * P + k2] = w[k2];
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < E / P; ++j)
+  for (int j = 0; j < NJ; ++j)
+    if (p + P * j < E) {
 #pragma unroll
-    for (int k2 = 0; k2 < P; ++k2) line[(p + P * j) + E * k2] = v[j * P + k2];
+      for (int k2 = 0; k2 < P; ++k2) line[(p + P * j) + E * k2] = o[j * P + k2];
+    }
   __syncthreads();
 }
 
@@ -368,6 +389,9 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
   float* eb = eps + (size_t)b * 6 * g.nv;
   float2* sb = spec + (size_t)b * 6 * g.nm;
   const float2* tw = g.pz.tw;
+  lambda += (size_t)(b / g.lame_group) * g.nv;
+  mu += (size_t)(b / g.lame_group) * g.nv;
+  med += b / g.lame_group;
   const bool need_r = (mode == 1 || mode == 3);
   const bool need_e = (mode == 1 || mode == 2 || mode == 3);
   const bool need_l = (mode != 3);
@@ -476,16 +500,24 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
         dots[qq] += d;
       }
     }
+    // Warp sums. The block may end in a partial warp (3 L P threads, e.g. 144); its lane
+    // count is a power of two, so the xor tree over the lanes that exist is complete.
+    static_assert(3 * L * P <= 192, "z pass block larger than its launch bound");
+    static_assert((3 * L * P) % 32 == 0 || (((3 * L * P) % 32) & ((3 * L * P) % 32 - 1)) == 0,
+                  "the last warp of the z pass must have a power-of-two lane count");
+    const int wlanes = min(32, nt - (tid & ~31));
+    const unsigned wmask = wlanes == 32 ? 0xffffffffu : ((1u << wlanes) - 1u);
     for (int qq = 0; qq < filled; ++qq) {
       double a = dots[qq];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      for (int off = 16; off > 0; off >>= 1)
+        if (off < wlanes) a += __shfl_xor_sync(wmask, a, off);
       if ((tid & 31) == 0) gred[qq][tid >> 5] = a;
     }
     __syncthreads();
     if (tid < filled) {
       double a = 0.0;
-      for (int w = 0; w < nt / 32; ++w) a += gred[tid][w];
+      for (int w = 0; w < (nt + 31) / 32; ++w) a += gred[tid][w];
       aa.partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + tid] = a;
     }
     return;
@@ -572,7 +604,9 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
 }
 
 // ----------------------------------------------------------------------------- host side
-static bool pow2_supported(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256; }
+static bool pow2_supported(int n) {
+  return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
+}
 
 bool supported(const GridDesc& g) {
   return pow2_supported(g.nx) && pow2_supported(g.ny) && pow2_supported(g.nz);
@@ -585,6 +619,8 @@ int x_tiles(const GridDesc& g) {
   switch (g.nx) {
     case 16: return x_blocks<16>(g);
     case 32: return x_blocks<32>(g);
+    case 48: return x_blocks<48>(g);
+    case 96: return x_blocks<96>(g);
     case 64: return x_blocks<64>(g);
     case 128: return x_blocks<128>(g);
     default: return x_blocks<256>(g);
@@ -611,7 +647,9 @@ cudaError_t configure() {
   cudaError_t e;
   if ((e = configure_n<16>()) != cudaSuccess) return e;
   if ((e = configure_n<32>()) != cudaSuccess) return e;
+  if ((e = configure_n<48>()) != cudaSuccess) return e;
   if ((e = configure_n<64>()) != cudaSuccess) return e;
+  if ((e = configure_n<96>()) != cudaSuccess) return e;
   if ((e = configure_n<128>()) != cudaSuccess) return e;
   return configure_n<256>();
 }
@@ -625,7 +663,7 @@ static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda,
   dim3 grid((unsigned)z_blocks_for<N>(g), batch);
   // every chunk offset is a multiple of 16 bytes when the base pointers are
   const int bulk = aligned16(lambda) && aligned16(mu) && aligned16(eps) && aligned16(spec) ? 1 : 0;
-  zpass_fast<N><<<grid, 192, zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec, eps_bar, eps0,
+  zpass_fast<N><<<grid, 3 * z_lines<N>() * Split<N>::P, zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec, eps_bar, eps0,
                                               st, med, aa);
 }
 
@@ -635,6 +673,8 @@ void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, c
   switch (g.nz) {
     case 16: zlaunch<16>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
     case 32: zlaunch<32>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+    case 48: zlaunch<48>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
+    case 96: zlaunch<96>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
     case 64: zlaunch<64>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
     case 128: zlaunch<128>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
     default: zlaunch<256>(g, mode, batch, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa, s); break;
@@ -648,6 +688,8 @@ int z_blocks(const GridDesc& g) {
   switch (g.nz) {
     case 16: return z_blocks_n<16>(g);
     case 32: return z_blocks_n<32>(g);
+    case 48: return z_blocks_n<48>(g);
+    case 96: return z_blocks_n<96>(g);
     case 64: return z_blocks_n<64>(g);
     case 128: return z_blocks_n<128>(g);
     default: return z_blocks_n<256>(g);
@@ -666,6 +708,8 @@ void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, cons
   switch (g.ny) {
     case 16: ylaunch<16>(g, inverse, batch, spec, st, s); break;
     case 32: ylaunch<32>(g, inverse, batch, spec, st, s); break;
+    case 48: ylaunch<48>(g, inverse, batch, spec, st, s); break;
+    case 96: ylaunch<96>(g, inverse, batch, spec, st, s); break;
     case 64: ylaunch<64>(g, inverse, batch, spec, st, s); break;
     case 128: ylaunch<128>(g, inverse, batch, spec, st, s); break;
     default: ylaunch<256>(g, inverse, batch, spec, st, s); break;
@@ -684,6 +728,8 @@ void launch_xpass(const GridDesc& g, int batch, float2* spec, const Medium* med,
   switch (g.nx) {
     case 16: xlaunch<16>(g, batch, spec, med, st, partials, s); break;
     case 32: xlaunch<32>(g, batch, spec, med, st, partials, s); break;
+    case 48: xlaunch<48>(g, batch, spec, med, st, partials, s); break;
+    case 96: xlaunch<96>(g, batch, spec, med, st, partials, s); break;
     case 64: xlaunch<64>(g, batch, spec, med, st, partials, s); break;
     case 128: xlaunch<128>(g, batch, spec, med, st, partials, s); break;
     default: xlaunch<256>(g, batch, spec, med, st, partials, s); break;

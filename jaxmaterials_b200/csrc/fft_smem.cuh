@@ -141,6 +141,28 @@ struct Bfly<3> {
   }
 };
 
+// 6-point DFT as 2 x 3: DFT over e of v[p + 2e] (p = 0, 1), twiddle exp(-2 pi i p k / 6),
+// then DFT over p, giving X[k1 + 3 k2].
+template <>
+struct Bfly<6> {
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    using R = decltype(C::x);
+    const R h = (R)0.5, s = (R)0.86602540378443864676;  // cos, sin(pi/3)
+    C a[3] = {v[0], v[2], v[4]};
+    C b[3] = {v[1], v[3], v[5]};
+    Bfly<3>::run(a);
+    Bfly<3>::run(b);
+    b[1] = mk<C>(h * b[1].x + s * b[1].y, h * b[1].y - s * b[1].x);    // exp(-i pi/3)
+    b[2] = mk<C>(-h * b[2].x + s * b[2].y, -h * b[2].y - s * b[2].x);  // exp(-2 i pi/3)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      v[k] = cadd(a[k], b[k]);
+      v[k + 3] = csub(a[k], b[k]);
+    }
+  }
+};
+
 template <>
 struct Bfly<5> {
   template <typename C>

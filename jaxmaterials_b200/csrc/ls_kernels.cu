@@ -85,6 +85,9 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
   C* sb = spec + (size_t)b * 6 * g.nm;
   const Plan1D& pz = g.pz;
   const C* tw = twiddles<T>(pz);
+  lambda += (size_t)(b / g.lame_group) * g.nv;
+  mu += (size_t)(b / g.lame_group) * g.nv;
+  med += b / g.lame_group;
 
   if (mode == 1 || mode == 3) {
     // Build conj(Z) with Z[k] = A[k] + i B[k] on the full line (Hermitian extension);
@@ -328,7 +331,8 @@ __global__ void __launch_bounds__(kMaxThreads) xpass_kernel(GridDesc g, int TT,
   fft_lines<VPT, true>(xbuf, W, W, 1, g.px, tw);
 
   // Residual partials, zero mode and Gamma^0 (written conjugated for the inverse DFT).
-  const T c_a = medium_ca<T>(*med), c_b = medium_cb<T>(*med);
+  const Medium& mb = med[b / g.lame_group];
+  const T c_a = medium_ca<T>(mb), c_b = medium_cb<T>(mb);
   const double sxs = 2.0 * g.nx / g.Lx, sys = 2.0 * g.ny / g.Ly, szs = 2.0 * g.nz / g.Lz;
   double acc = 0.0;
   const int modes = nx * TT;
@@ -573,10 +577,14 @@ __global__ void reset_state_kernel(int batch, int phase, InstanceState* st) {
 }
 
 // ----------------------------------------------------------------------------- medium
+// Structure blockIdx.y of [structure][nv] fields; partials to scratch[structure][block][6].
 template <typename TL>
 __global__ void minmax_partial_kernel(long long nv, const TL* __restrict__ lambda,
                                       const TL* __restrict__ mu, double* __restrict__ scratch) {
   __shared__ double sh[6][32];
+  lambda += (size_t)blockIdx.y * nv;
+  mu += (size_t)blockIdx.y * nv;
+  scratch += (size_t)blockIdx.y * gridDim.x * 6;
   double lmin = DBL_MAX, lmax = -DBL_MAX, mmin = DBL_MAX, mmax = -DBL_MAX;
   double lsum = 0.0, msum = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
@@ -614,9 +622,12 @@ __global__ void minmax_partial_kernel(long long nv, const TL* __restrict__ lambd
   }
 }
 
+// One block per structure: Medium med[structure] from its nblk partials.
 __global__ void minmax_final_kernel(int nblk, long long nv, int fp64_fields,
                                     const double* __restrict__ scratch, Medium* med) {
   if (threadIdx.x != 0) return;
+  scratch += (size_t)blockIdx.x * nblk * 6;
+  med += blockIdx.x;
   double lmin = DBL_MAX, lmax = -DBL_MAX, mmin = DBL_MAX, mmax = -DBL_MAX;
   double lsum = 0.0, msum = 0.0;
   for (int i = 0; i < nblk; ++i) {
@@ -672,13 +683,15 @@ __global__ void convert_plain_kernel(long long n, const Tin* __restrict__ in, To
 // ----------------------------------------------------------------------------- stress
 // sigma = C : eps for every instance of the given phase; sigma is written in TS.
 template <typename T, typename TS>
-__global__ void stress_kernel(long long nv, int phase, const InstanceState* __restrict__ st,
+__global__ void stress_kernel(long long nv, int phase, int lame_group, const InstanceState* __restrict__ st,
                               const T* __restrict__ lambda, const T* __restrict__ mu,
                               const T* __restrict__ eps, TS* __restrict__ sigma,
                               double* __restrict__ scratch) {
   __shared__ double sh[6][32];
   const int b = blockIdx.y;
   if (st[b].phase != phase) return;
+  lambda += (size_t)(b / lame_group) * nv;
+  mu += (size_t)(b / lame_group) * nv;
   const T* eb = eps + (size_t)b * 6 * nv;
   TS* sg = sigma ? sigma + (size_t)b * 6 * nv : nullptr;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -835,12 +848,12 @@ void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t st
 }
 
 template <typename TL>
-void launch_medium(long long nv, const TL* lambda, const TL* mu, double* scratch, Medium* med,
-                   cudaStream_t stream) {
-  int nblk = (int)std::min<long long>(1024, (nv + 255) / 256);
+void launch_medium(long long nv, int nstruct, const TL* lambda, const TL* mu, double* scratch,
+                   Medium* med, cudaStream_t stream) {
+  int nblk = (int)std::min<long long>(std::max(1, 1024 / nstruct), (nv + 255) / 256);
   if (nblk < 1) nblk = 1;
-  minmax_partial_kernel<TL><<<nblk, 256, 0, stream>>>(nv, lambda, mu, scratch);
-  minmax_final_kernel<<<1, 32, 0, stream>>>(nblk, nv, sizeof(TL) == 8 ? 1 : 0, scratch, med);
+  minmax_partial_kernel<TL><<<dim3(nblk, nstruct), 256, 0, stream>>>(nv, lambda, mu, scratch);
+  minmax_final_kernel<<<nstruct, 32, 0, stream>>>(nblk, nv, sizeof(TL) == 8 ? 1 : 0, scratch, med);
 }
 
 template <typename Tin, typename Tout>
@@ -864,7 +877,7 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
   int nblk = (int)std::min<long long>(1024, (g.nv + 255) / 256);
   if (nblk < 1) nblk = 1;
   dim3 grid(nblk, batch);
-  stress_kernel<T, TS><<<grid, 256, 0, stream>>>(g.nv, phase, st, lambda, mu, eps, sigma,
+  stress_kernel<T, TS><<<grid, 256, 0, stream>>>(g.nv, phase, g.lame_group, st, lambda, mu, eps, sigma,
                                                   mean ? scratch : nullptr);
   if (mean) mean_final_kernel<<<6 * batch, 32, 0, stream>>>(nblk, g.nv, phase, st, scratch, mean);
 }
@@ -878,7 +891,7 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
                                 const InstanceState*, cudaStream_t);                            \
   template void launch_xpass<T>(const GridDesc&, const LaunchShape&, int, cplx<T>*,             \
                                 const Medium*, InstanceState*, double*, cudaStream_t);          \
-  template void launch_medium<T>(long long, const T*, const T*, double*, Medium*, cudaStream_t);
+  template void launch_medium<T>(long long, int, const T*, const T*, double*, Medium*, cudaStream_t);
 LSB_INST(float)
 LSB_INST(double)
 #undef LSB_INST

@@ -25,7 +25,8 @@ LaunchShape plan_launch(const GridDesc& g, int elem_bytes);
 cudaError_t configure_kernels();
 
 // Pointers are batch base pointers; the kernels process instance b when it is not done
-// and its phase matches the precision T (float: phase 0, double: phase 1).
+// and its phase matches the precision T (float: phase 0, double: phase 1). Instance b
+// reads the Lame fields of structure b / g.lame_group and the medium med[b / g.lame_group].
 // mode 0: eps = eps_bar (or eps0 if given); mode 1: eps += r / N from spec; mode 2: keep
 // eps and the stored shift (continuation in another precision).
 // modes 3/4: Anderson residual / combine (see ls_kernels.cu).
@@ -46,10 +47,11 @@ void launch_finalize(const LaunchShape& ls, int phase, int batch, InstanceState*
                      const double* partials, double* history, int history_len,
                      const SolveParams& sp, cudaStream_t s);
 void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t s);
-// min/max and FP64 means of the Lame fields -> reference medium; scratch: 6*1024 doubles.
+// min/max and FP64 means of each of nstruct Lame field pairs ([structure][nv]) ->
+// reference media med[structure]; scratch: 6 * max(1024, nstruct) doubles.
 template <typename TL>
-void launch_medium(long long nv, const TL* lambda, const TL* mu, double* scratch, Medium* med,
-                   cudaStream_t s);
+void launch_medium(long long nv, int nstruct, const TL* lambda, const TL* mu, double* scratch,
+                   Medium* med, cudaStream_t s);
 // out = in for instances in phase 1 (if only_running: and not done).
 template <typename Tin, typename Tout>
 void launch_convert_fields(long long n_per_instance, int batch, int only_running,

@@ -74,6 +74,14 @@ bool factorize(int n, Plan1D& p) {
   return true;
 }
 
+int structures_of(lsb_solver* s, int batch) {
+  const int group = s->lame_group > 0 ? s->lame_group : batch;
+  if (batch % group != 0)
+    return fail(-1, "batch %d is not a multiple of %d instances per Lame field pair", batch, group);
+  s->g.lame_group = group;
+  return batch / group;
+}
+
 bool shape_fits(const LaunchShape& sh) {
   return sh.z_threads <= kMaxThreads && sh.y_threads <= kMaxThreads && sh.x_threads <= kMaxThreads;
 }
@@ -96,12 +104,19 @@ int ensure_history(lsb_solver* s, int len) {
   return 0;
 }
 
-int ensure_fp64(lsb_solver* s) {
+// FP64 work buffers, and FP64 copies of `nstruct` Lame field pairs when nstruct > 0.
+int ensure_fp64(lsb_solver* s, int nstruct) {
   const size_t B = (size_t)s->batch_cap;
   if (!s->d_spec64) {
     LSB_CUDA(cudaMalloc(&s->d_eps64, sizeof(double) * B * 6 * s->g.nv));
     LSB_CUDA(cudaMalloc(&s->d_spec64, sizeof(double2) * B * 6 * s->g.nm));
-    LSB_CUDA(cudaMalloc(&s->d_lame64, sizeof(double) * 2 * s->g.nv));
+  }
+  if (nstruct > s->lame64_structs) {
+    cudaFree(s->d_lame64);
+    s->d_lame64 = nullptr;
+    s->lame64_structs = 0;
+    LSB_CUDA(cudaMalloc(&s->d_lame64, sizeof(double) * 2 * (size_t)nstruct * s->g.nv));
+    s->lame64_structs = nstruct;
   }
   return 0;
 }
@@ -239,9 +254,9 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
             alloc((void**)&s->d_spec32, sizeof(float2) * B * 6 * g.nm) &&
             alloc((void**)&s->d_partials, sizeof(double) * B * xblk) &&
             alloc((void**)&s->d_state, sizeof(InstanceState) * B) &&
-            alloc((void**)&s->d_medium, sizeof(Medium)) &&
+            alloc((void**)&s->d_medium, sizeof(Medium) * B) &&
             alloc((void**)&s->d_epsbar, sizeof(double) * B * 6) &&
-            alloc((void**)&s->d_scratch, sizeof(double) * 6 * 1024) &&
+            alloc((void**)&s->d_scratch, sizeof(double) * 6 * std::max<size_t>(1024, B)) &&
             alloc((void**)&s->d_mean_scratch, sizeof(double) * B * 6 * 1024) &&
             alloc((void**)&s->d_mean, sizeof(double) * B * 6) &&
             alloc((void**)&s->d_tw32, sizeof(float2) * ntw) &&
@@ -407,16 +422,18 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   if (cur != s->device) return fail(-1, "solver was created on device %d, current is %d", s->device, cur);
   const GridDesc& g = s->g;
   cudaStream_t st = s->stream;
+  const int nstruct = structures_of(s, batch);
+  if (nstruct < 0) return nstruct;
   LSB_TRY(ensure_history(s, maxiter + 8));
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
   const bool fp64_start = s->precision == kPrecFP64;
-  if (s->precision != kPrecFP32) LSB_TRY(ensure_fp64(s));
+  if (s->precision != kPrecFP32) LSB_TRY(ensure_fp64(s, nstruct));
 
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
   if (s->d_history)
     LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
   launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st);
-  launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
   bool any64 = fp64_start;
   if (!fp64_start) {
@@ -425,8 +442,9 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   }
   if (any64) {
     const long long n6 = 6 * g.nv;
-    launch_convert<float, double>(g.nv, d_lambda, s->d_lame64, st);
-    launch_convert<float, double>(g.nv, d_mu, s->d_lame64 + g.nv, st);
+    const long long nl = (long long)nstruct * g.nv;
+    launch_convert<float, double>(nl, d_lambda, s->d_lame64, st);
+    launch_convert<float, double>(nl, d_mu, s->d_lame64 + nl, st);
     s->launches += 2;
     if (fp64_start && d_eps0) {
       launch_convert_fields<float, double>(n6, batch, 1, s->d_state, d_eps0, s->d_eps64, st);
@@ -439,10 +457,10 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
     // FP64 from the start runs Anderson in FP64; the continuation after an FP32 stall is
     // a few plain updates from the FP32 iterate.
     if (fp64_start) LSB_TRY(ensure_fp64_rings(s));
-    LSB_TRY(run_phase<double>(s, batch, s->d_lame64, s->d_lame64 + g.nv, s->d_eps64, s->d_spec64,
+    LSB_TRY(run_phase<double>(s, batch, s->d_lame64, s->d_lame64 + nl, s->d_eps64, s->d_spec64,
                               nullptr, init_mode, sp, fp64_start));
     launch_convert_fields<double, float>(n6, batch, 0, s->d_state, s->d_eps64, d_eps, st);
-    launch_stress<double, float>(g, 1, batch, s->d_state, s->d_lame64, s->d_lame64 + g.nv, s->d_eps64,
+    launch_stress<double, float>(g, 1, batch, s->d_state, s->d_lame64, s->d_lame64 + nl, s->d_eps64,
                                  d_sigma, s->d_mean_scratch, s->d_mean, st);
     s->launches += 3;
   }
@@ -479,13 +497,15 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   if (maxiter < 0) return fail(-1, "maxiter must be >= 0");
   const GridDesc& g = s->g;
   cudaStream_t st = s->stream;
+  const int nstruct = structures_of(s, batch);
+  if (nstruct < 0) return nstruct;
   LSB_TRY(ensure_history(s, maxiter + 8));
-  LSB_TRY(ensure_fp64(s));
+  LSB_TRY(ensure_fp64(s, 0));
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
   LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
   launch_reset_state(batch, 1, s->d_state, st);
-  launch_medium<double>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  launch_medium<double>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
   LSB_TRY(ensure_fp64_rings(s));
   LSB_TRY(run_phase<double>(s, batch, d_lambda, d_mu, d_eps, s->d_spec64, d_eps0, 0, sp, true));
@@ -551,6 +571,13 @@ int lsb_set_stream(lsb_solver* solver, void* stream) {
   return 0;
 }
 
+int lsb_set_lame_group(lsb_solver* solver, int instances_per_field) {
+  if (!solver) return fail(-1, "null solver");
+  if (instances_per_field < 0) return fail(-1, "instances_per_field must be >= 0");
+  solver->lame_group = instances_per_field;
+  return 0;
+}
+
 int lsb_set_precision(lsb_solver* solver, int precision, int stall_window) {
   if (!solver) return fail(-1, "null solver");
   if (precision < LSB_PREC_FP32 || precision > LSB_PREC_FP64) return fail(-1, "unknown precision %d", precision);
@@ -599,8 +626,10 @@ int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const fl
   std::vector<double> eb(6 * batch, 0.0);
   for (int b = 0; b < batch; ++b) eb[6 * b + (b % 6)] = 1.0;
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eb.data(), sizeof(double) * eb.size(), cudaMemcpyHostToDevice, st));
+  const int nstruct = structures_of(s, batch);
+  if (nstruct < 0) return nstruct;
   launch_reset_state(batch, 0, s->d_state, st);
-  launch_medium<float>(g.nv, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   const AndersonArgs<float> aa0 = anderson_args<float>(s, false);
   pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa0);
   pass_y<float>(s, false, batch, s->d_spec32);

@@ -17,6 +17,9 @@ struct lsb_solver {
   int depth = 0;
   int precision = kPrecMixed;
   int stall_window = 8;
+  // instances per (lambda, mu) field pair: 0 = every instance of a solve shares one pair;
+  // k > 0 = instance b uses structure b / k of [structure][nv] Lame arrays
+  int lame_group = 0;
   bool fast32 = false;   // FP32 passes with compile-time power-of-two lengths
   GridDesc g{};
   LaunchShape sh32{}, sh64{};
@@ -27,7 +30,8 @@ struct lsb_solver {
   // FP64 work buffers, allocated on first use
   double* d_eps64 = nullptr;
   double2* d_spec64 = nullptr;
-  double* d_lame64 = nullptr;    // [2][nv]
+  double* d_lame64 = nullptr;    // [2][structures][nv]
+  int lame64_structs = 0;        // structures d_lame64 holds
   // Anderson acceleration (depth > 0): rings of g = eps + r and r, Gram matrices, coefficients
   float* d_aa_g32 = nullptr;     // [batch][m+1][6][nv]
   float* d_aa_r32 = nullptr;
@@ -40,9 +44,9 @@ struct lsb_solver {
   // shared
   double* d_partials = nullptr;  // [batch][x blocks]
   InstanceState* d_state = nullptr;
-  Medium* d_medium = nullptr;
+  Medium* d_medium = nullptr;    // [structures]
   double* d_epsbar = nullptr;    // [batch][6]
-  double* d_scratch = nullptr;   // 6 * 1024
+  double* d_scratch = nullptr;   // 6 * max(1024, batch_cap)
   double* d_mean_scratch = nullptr;
   double* d_mean = nullptr;      // [batch][6]
   double* d_history = nullptr;   // [batch][history_len]
@@ -80,6 +84,9 @@ int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]);
 // Uploads the twiddle and sin/cos tables into s->d_tw32/d_tw64/d_tables and points the
 // plans of s->g at them (the buffers must be sized for the grid).
 int upload_tables(lsb_solver* s);
+// Sets s->g.lame_group for a solve of `batch` instances and returns the number of Lame
+// field pairs the solve reads (negative with an error message when batch does not split).
+int structures_of(lsb_solver* s, int batch);
 // Full FP32-input solve (see lsb_solve); d_eps is the FP32 work buffer and output.
 int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
               const double* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,

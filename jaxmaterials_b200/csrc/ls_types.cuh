@@ -56,6 +56,9 @@ struct GridDesc {
   long long nm;   // half-spectrum modes
   double Lx, Ly, Lz;
   Plan1D px, py, pz;
+  // Consecutive instances that share one (lambda, mu) field and one reference medium:
+  // instance b uses field b / lame_group ([structure][nv] arrays) and medium[b / lame_group].
+  int lame_group;
   // per-axis FP64 tables: s_d[k] = sin(pi k / n_d), c_d[k] = cos(pi k / n_d)
   const double* sx;
   const double* cx;

@@ -103,7 +103,7 @@ extern "C" int lsb_solve_noalloc(const int voxels[3], const double extents[3], i
   c.take(s.d_spec32, sizeof(float2) * B * 6 * g.nm);
   c.take(s.d_partials, sizeof(double) * B * s.sh32.x_blocks_per_instance);
   c.take(s.d_state, sizeof(InstanceState) * B);
-  c.take(s.d_medium, sizeof(Medium));
+  c.take(s.d_medium, sizeof(Medium) * B);
   c.take(s.d_epsbar, sizeof(double) * B * 6);
   c.take(s.d_scratch, sizeof(double) * 6 * 1024);
   c.take(s.d_mean_scratch, sizeof(double) * B * 6 * 1024);

@@ -101,8 +101,11 @@ class SolveResult:
 class Solver:
     """Reusable solver for one grid: owns the device buffers of ``batch`` instances.
 
-    Instances of one ``solve`` call share lambda and mu and differ in epsilon_bar (and
-    optionally the warm start). Uses the current CUDA device and torch's current stream.
+    Instances of one ``solve`` call share lambda and mu (shape (nx, ny, nz)) and differ
+    in epsilon_bar (and optionally the warm start), or, with lambda and mu of shape
+    (S, nx, ny, nz), instance b reads structure b // (B // S) (B a multiple of S; e.g.
+    the six load cases of S structures). Uses the current CUDA device and torch's
+    current stream.
     """
 
     def __init__(self, grid_spec, batch=1, depth=0, precision="mixed", stall_window=8):
@@ -170,8 +173,16 @@ class Solver:
         b = eb.shape[0]
         if eb.shape[1] != 6 or b < 1 or b > self.batch:
             raise ValueError(f"epsilon_bar must have shape (B, 6) with 1 <= B <= {self.batch}")
-        lm = self._as_device(lmbda, nshape, tdt)
-        m = self._as_device(mu, nshape, tdt)
+        lshape = tuple(np.shape(lmbda))
+        nstruct = 1 if lshape == nshape else (lshape[0] if len(lshape) == 4 else 0)
+        if nstruct < 1 or b % nstruct != 0:
+            raise ValueError(f"lambda must have shape {nshape} or (S,) + {nshape} with B = "
+                             f"{b} a multiple of S, got {lshape}")
+        fshape = nshape if lshape == nshape else (nstruct,) + nshape
+        lm = self._as_device(lmbda, fshape, tdt)
+        m = self._as_device(mu, fshape, tdt)
+        _lib.check(self._lib.lsb_set_lame_group(self._h, 0 if lshape == nshape else b // nstruct),
+                   "lsb_set_lame_group")
         e0 = None
         if epsilon0 is not None:
             e0 = self._as_device(epsilon0, (b, 6) + nshape, tdt)
@@ -212,6 +223,7 @@ class Solver:
         b = self.batch if batch is None else int(batch)
         lm = self._as_device(lmbda, g.shape)
         m = self._as_device(mu, g.shape)
+        _lib.check(self._lib.lsb_set_lame_group(self._h, 0), "lsb_set_lame_group")
         work = torch.empty((b, 6) + g.shape, dtype=torch.float32, device=self.device)
         ms = np.zeros(5, dtype=np.float32)
         stream = torch.cuda.current_stream(self.device).cuda_stream

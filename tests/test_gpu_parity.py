@@ -52,7 +52,9 @@ def oracle_fixed_iters(lm, mu, eb, g, iters):
                                    ("prime", (37, 47, 61)), ("mixed", (48, 20, 30)),
                                    ("line", (1, 1, 16)), ("flat", (16, 8, 1)),
                                    ("pow2a", (64, 32, 16)), ("pow2b", (16, 128, 256)),
-                                   ("pow2c", (256, 16, 32))])
+                                   ("pow2c", (256, 16, 32)), ("fast48", (48, 96, 32)),
+                                   ("fast96", (96, 48, 64)), ("fastz", (32, 16, 96)),
+                                   ("fastz48", (16, 32, 48))])
 def test_fields_match_oracle(ls, tag, n):
     from jaxmaterials_b200 import GridSpec
 
