@@ -42,7 +42,65 @@ def parse():
     p.add_argument("--depth", type=int, default=5)
     p.add_argument("--no-plain", action="store_true", help="skip the plain-iteration comparison")
     p.add_argument("--cpu-sample-s", type=float, default=12.0)
+    p.add_argument("--batched", type=int, default=512,
+                   help="structures of the batched uneven-size workload (0: skip)")
+    p.add_argument("--batched-plain", action="store_true",
+                   help="also time the batched workload with the plain iteration")
     return p.parse_args()
+
+
+def batched_workload(count, seed):
+    """Seeded structures with N in {32,48,64,96,128}, 2-6 layers, radius 2-5 voxels,
+    volume fraction 0.30-0.55; cubic voxels of unit size."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+
+    lms, mus, gs = [], [], []
+    for p in fibres.batch_structure_params(count, seed):
+        st = fibres.generate_layered_fibres(p["n"], p["nlayers"], p["radius"],
+                                            p["volume_fraction"], p["seed"])
+        lm, mu = fibres.lame_fields(st)
+        lms.append(lm)
+        mus.append(mu)
+        gs.append(GridSpec(*st.n, *st.extents))
+    return lms, mus, gs
+
+
+def batched_run(count, seed, depth):
+    """One pass of lsb_c_eff_batch over `count` structures x 6 load cases, host inputs
+    (lambda, mu) in and C_eff out; wall-clock around the blocking call. A warm-up pass
+    over one structure per grid size runs first."""
+    import torch
+    from jaxmaterials_b200.solver import c_eff_batch
+
+    lms, mus, gs = batched_workload(count, seed)
+    seen = {}
+    for i, g in enumerate(gs):
+        seen.setdefault(g.shape, i)
+    w = list(seen.values())
+    c_eff_batch([lms[i] for i in w], [mus[i] for i in w], [gs[i] for i in w], depth=depth,
+                maxiter=5000)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    C, iters, status = c_eff_batch(lms, mus, gs, depth=depth, maxiter=5000)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    nv = np.array([g.number_of_voxels for g in gs], dtype=np.float64)
+    by_n = {}
+    for g, it in zip(gs, iters):
+        by_n.setdefault(g.nx, []).append(float(it.mean()))
+    return {
+        "seconds": sec,
+        "solves": 6 * count,
+        "value": 6 * count / sec,
+        "unit": "solves/s",
+        "voxel_iter_per_s": float((nv[:, None] * iters).sum()) / sec,
+        "iters_per_solve": float(iters.mean()),
+        "iters_per_solve_by_n": {str(k): float(np.mean(v)) for k, v in sorted(by_n.items())},
+        "voxels_total": float(nv.sum()),
+        "all_converged": bool((status == 1).all()),
+        "h2d_bytes": float(8 * nv.sum()),
+    }
 
 
 def workload(seed):
@@ -362,6 +420,23 @@ def own_arm(args):
     loop_ms = sum(passes.values())
     loop_gbs = 152.0 * nv * b / (loop_ms / 1000.0) / 1e9
 
+    s.close()
+    batched = None
+    if args.batched > 0:
+        torch.cuda.empty_cache()
+        batched = {"structures": args.batched, "depth": args.depth, "precision": "mixed",
+                   "sizes": [32, 48, 64, 96, 128], "layers": [2, 6], "radius": [2.0, 5.0],
+                   "volume_fraction": [0.30, 0.55], "tol": 1e-6, "seed": 1000 + rank,
+                   "timing": "wall clock around the blocking call; host lambda, mu in, "
+                             "C_eff out; one warm-up pass over one structure per size"}
+        batched["anderson"] = batched_run(args.batched, 1000 + rank, args.depth)
+        if args.batched_plain:
+            batched["plain"] = batched_run(args.batched, 1000 + rank, 0)
+        if world > 1:
+            sec = torch.tensor([batched["anderson"]["seconds"]], device=dev, dtype=torch.float64)
+            dist.all_reduce(sec, op=dist.ReduceOp.MAX)
+            batched["anderson"]["value"] = 6 * args.batched * world / float(sec.item())
+
     if rank == 0:
         out = {
             "metric": METRIC,
@@ -381,6 +456,7 @@ def own_arm(args):
             "iters_per_solve": float(iters_total) / (6 * args.steps),
             "all_converged": converged,
             "plain": plain,
+            "batched": batched,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "gpu_launches": int(launches),
             "roofline": {
@@ -417,7 +493,6 @@ def own_arm(args):
                 "voxel_iter_per_s": 1.0 / s_per_vi,
             }
         print(json.dumps(out))
-    s.close()
     if world > 1:
         dist.destroy_process_group()
 
