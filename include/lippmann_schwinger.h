@@ -85,6 +85,13 @@ int lsb_set_stream(lsb_solver *solver, void *stream);
  * which FP32 round-off is taken to have stalled the iteration (default 8; 0 disables). */
 int lsb_set_precision(lsb_solver *solver, int precision, int stall_window);
 
+/* No reference counterpart. Reference criteria for the stop rule of later solves: with
+ * e0 (host double[batch], positive) instance b stops when e < max(rtol * e0[b], atol)
+ * instead of using its own first criterion. A warm-started solve given the criterion of
+ * the cold start (the residual of a maxiter = 0 solve from eps_bar) thereby stops at the
+ * same absolute residual as the cold solve. e0 = NULL clears it. */
+int lsb_set_reference_e0(lsb_solver *solver, int batch, const double *e0);
+
 /* No reference counterpart. Groups instances by microstructure: with
  * instances_per_field = k > 0, instance b of a solve reads the Lame fields of structure
  * b / k from d_lambda, d_mu laid out [batch / k][nv] (and gets that structure's own

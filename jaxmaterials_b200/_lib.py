@@ -1,5 +1,5 @@
 """ctypes binding of ``liblippmannschwinger.so`` (declarations in
-``include/lippmann_schwinger.h``).
+``include/lippmann_schwinger.h`` and ``include/spectral_net.h``).
 
 The library is looked up next to this file first, then through the dynamic loader
 (``LD_LIBRARY_PATH``), as the reference wrapper does
@@ -37,6 +37,7 @@ SIGNATURES = {
                                  c_double_p]),
     "lsb_set_precision": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
     "lsb_set_lame_group": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "lsb_set_reference_e0": (ctypes.c_int, [c_void_p, ctypes.c_int, c_double_p]),
     "lsb_c_eff_batch": (ctypes.c_int, [ctypes.c_int, c_int_p, c_double_p,
                                        ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                        ctypes.c_int, ctypes.c_int, ctypes.c_float,
@@ -62,6 +63,24 @@ SIGNATURES = {
     "lsb_ceff_gradient_f64": (ctypes.c_int, [c_int_p, c_void_p, c_double_p, c_void_p, c_void_p,
                                              c_void_p]),
     "lsb_last_error": (ctypes.c_char_p, []),
+    # include/spectral_net.h
+    "lsn_pointwise_forward": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_longlong, c_void_p, c_void_p, c_void_p,
+                                             c_void_p, c_void_p, c_void_p, ctypes.c_int,
+                                             c_void_p]),
+    "lsn_pointwise_backward": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_longlong, c_void_p, c_void_p, c_void_p,
+                                              c_void_p, ctypes.c_int, c_void_p, c_void_p,
+                                              c_void_p, c_void_p, c_void_p]),
+    "lsn_spectral_forward": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p,
+                                            c_int_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "lsn_spectral_backward": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p,
+                                             c_int_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                             c_void_p, c_void_p]),
+    "lsn_adam": (ctypes.c_int, [ctypes.c_longlong, c_void_p, c_void_p, c_void_p, c_void_p,
+                                ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                ctypes.c_int, c_void_p]),
+    "lsn_last_error": (ctypes.c_char_p, []),
     "lsb_version": (ctypes.c_int, []),
 }
 
@@ -93,6 +112,14 @@ def load():
             fn.argtypes = args
         _lib = lib
         return lib
+
+
+def check_net(rc, what="call"):
+    """As check(), for the network kernels of include/spectral_net.h."""
+    if rc < 0:
+        msg = load().lsn_last_error().decode(errors="replace")
+        raise LibraryError(f"{what} failed ({rc}): {msg}")
+    return rc
 
 
 def check(rc, what="call"):

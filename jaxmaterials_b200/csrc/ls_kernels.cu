@@ -459,7 +459,7 @@ __global__ void finalize_kernel(int nblk, int phase, InstanceState* __restrict__
   if (history != nullptr && s.evals < history_len) history[(size_t)b * history_len + s.evals] = e;
   s.evals += 1;
   s.e = e;
-  const double thr = fmax(sp.rtol * s.e0, sp.atol);
+  const double thr = fmax(sp.rtol * (s.e0_ref > 0.0 ? s.e0_ref : s.e0), sp.atol);
   const bool conv = sp.rule == 0 ? (e < thr) : (e <= thr);
   // the next forward transform is shifted by the current mean stress
   const double inv_nv = 1.0 / (double)sp.nv;
@@ -567,11 +567,12 @@ __global__ void anderson_solve_kernel(int nzblk, int depth, int phase, const Ins
   }
 }
 
-__global__ void reset_state_kernel(int batch, int phase, InstanceState* st) {
+__global__ void reset_state_kernel(int batch, int phase, const double* e0_ref, InstanceState* st) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < batch) {
     InstanceState z = {};
     z.phase = phase;
+    z.e0_ref = e0_ref ? e0_ref[b] : 0.0;
     st[b] = z;
   }
 }
@@ -843,8 +844,9 @@ void launch_finalize(const LaunchShape& s, int phase, int batch, InstanceState* 
                                               history_len, sp);
 }
 
-void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t stream) {
-  reset_state_kernel<<<(batch + 127) / 128, 128, 0, stream>>>(batch, phase, st);
+void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t stream,
+                        const double* e0_ref) {
+  reset_state_kernel<<<(batch + 127) / 128, 128, 0, stream>>>(batch, phase, e0_ref, st);
 }
 
 template <typename TL>

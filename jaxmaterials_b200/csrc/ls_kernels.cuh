@@ -46,7 +46,9 @@ void launch_xpass(const GridDesc& g, const LaunchShape& ls, int batch, cplx<T>* 
 void launch_finalize(const LaunchShape& ls, int phase, int batch, InstanceState* st,
                      const double* partials, double* history, int history_len,
                      const SolveParams& sp, cudaStream_t s);
-void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t s);
+// e0_ref (optional, device double[batch]): reference criteria for the stop threshold.
+void launch_reset_state(int batch, int phase, InstanceState* st, cudaStream_t s,
+                        const double* e0_ref = nullptr);
 // min/max and FP64 means of each of nstruct Lame field pairs ([structure][nv]) ->
 // reference media med[structure]; scratch: 6 * max(1024, nstruct) doubles.
 template <typename TL>

@@ -432,7 +432,7 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
   if (s->d_history)
     LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
-  launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st);
+  launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st, s->use_e0ref ? s->d_e0ref : nullptr);
   launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
   bool any64 = fp64_start;
@@ -504,7 +504,7 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
   LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
-  launch_reset_state(batch, 1, s->d_state, st);
+  launch_reset_state(batch, 1, s->d_state, st, s->use_e0ref ? s->d_e0ref : nullptr);
   launch_medium<double>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
   LSB_TRY(ensure_fp64_rings(s));
@@ -568,6 +568,21 @@ void lsb_destroy(lsb_solver* solver) { delete solver; }
 int lsb_set_stream(lsb_solver* solver, void* stream) {
   if (!solver) return fail(-1, "null solver");
   solver->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int lsb_set_reference_e0(lsb_solver* solver, int batch, const double* e0) {
+  if (!solver) return fail(-1, "null solver");
+  if (!e0) {
+    solver->use_e0ref = false;
+    return 0;
+  }
+  if (batch < 1 || batch > solver->batch_cap) return fail(-1, "batch %d outside [1, %d]", batch, solver->batch_cap);
+  for (int b = 0; b < batch; ++b)
+    if (!(e0[b] > 0.0) || !std::isfinite(e0[b])) return fail(-1, "e0[%d] must be positive and finite", b);
+  if (!solver->d_e0ref) LSB_CUDA(cudaMalloc(&solver->d_e0ref, sizeof(double) * solver->batch_cap));
+  LSB_CUDA(cudaMemcpy(solver->d_e0ref, e0, sizeof(double) * batch, cudaMemcpyHostToDevice));
+  solver->use_e0ref = true;
   return 0;
 }
 

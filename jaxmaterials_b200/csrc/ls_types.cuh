@@ -111,6 +111,7 @@ struct InstanceState {
   int switched;   // 1 once the instance moved from FP32 to FP64
   int aa_base;    // iteration count when the Anderson history (re)started
   double e0;      // criterion at the first iterate
+  double e0_ref;  // > 0: the stop threshold is rtol * e0_ref instead of rtol * e0
   double e;       // last criterion value
   double best_e;  // smallest criterion value seen in the current phase
   double sig0[12];  // zero mode of sigma_hat (6 complex) at the last evaluation

@@ -157,10 +157,13 @@ class Solver:
         return t
 
     def solve(self, lmbda, mu, epsilon_bar, rtol=1e-6, atol=1e-20, maxiter=32,
-              rule=RULE_CUDA, epsilon0=None, want_sigma=True, out=None, dtype=np.float32):
+              rule=RULE_CUDA, epsilon0=None, want_sigma=True, out=None, dtype=np.float32,
+              e0_ref=None):
         """Run the fixed point for every row of ``epsilon_bar`` (shape (B, 6) or (6,)).
 
-        ``dtype=np.float64`` runs FP64 fields end to end (inputs and outputs in FP64)."""
+        ``dtype=np.float64`` runs FP64 fields end to end (inputs and outputs in FP64).
+        ``e0_ref`` (B positive values): stop at rtol * e0_ref[b] instead of rtol times the
+        instance's first criterion (for warm starts, the cold-start criterion)."""
         import torch
 
         f64 = np.dtype(dtype) == np.float64
@@ -195,6 +198,12 @@ class Solver:
         mean = np.zeros((b, 6), dtype=np.float64)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._lib.lsb_set_stream(self._h, ctypes.c_void_p(stream)), "lsb_set_stream")
+        if e0_ref is None:
+            _lib.check(self._lib.lsb_set_reference_e0(self._h, b, None), "lsb_set_reference_e0")
+        else:
+            ref = np.ascontiguousarray(np.broadcast_to(np.asarray(e0_ref, np.float64), (b,)))
+            _lib.check(self._lib.lsb_set_reference_e0(self._h, b, ref.ctypes.data_as(_lib.c_double_p)),
+                       "lsb_set_reference_e0")
         fn = self._lib.lsb_solve_f64 if f64 else self._lib.lsb_solve
         ebp = eb.ctypes.data_as(_lib.c_double_p) if f64 else _fptr(eb)
         rc = fn(

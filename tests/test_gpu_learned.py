@@ -1,0 +1,188 @@
+"""Warm-start network kernels (include/spectral_net.h): forward against the FP64 CPU
+oracle, backward against central finite differences of the oracle and against torch
+autograd of a plain torch FP32 restatement, the Adam kernel against its formula; the
+reference-criterion stop rule; the data/training/evaluation pipeline on a small grid.
+
+Tolerances: forward 1e-5 relative to the output's max-abs (FP32 accumulation, BF16
+weights passed rounded to both sides); gradients 2e-3 relative to the gradient's
+max-abs against FD (h = 1e-3 in FP64) and 1e-4 against torch autograd.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import spectral_net_oracle as SO
+
+pytestmark = pytest.mark.gpu
+
+
+def is_weight(name):
+    return name.startswith("spec") or name.endswith("_w") or (name[0] == "w" and name[1:].isdigit())
+
+
+def rounded_params(net):
+    import torch
+
+    return {k: (v.detach().to(torch.bfloat16) if is_weight(k) else v.detach()).double().cpu().numpy()
+            for k, v in net.params.items()}
+
+
+def torch_reference(net, a):
+    """Plain torch FP32 forward with the BF16-rounded weights (differentiable)."""
+    import torch
+    import torch.nn.functional as F
+    from jaxmaterials_b200.learned.network import inverse_half_spectrum
+
+    p = net.params
+
+    def rw(w):
+        return w + (w.to(torch.bfloat16).float() - w).detach()
+
+    def pw(x, w, b):
+        return torch.einsum("oi,bi...->bo...", rw(w), x) + b.view(1, -1, 1, 1, 1)
+
+    n = tuple(a.shape[2:])
+    kx, ky, kz = (torch.as_tensor(v, device=a.device) for v in SO.retained_index(n, net.modes))
+    h = pw(a, p["lift_w"], p["lift_b"])
+    for l in range(net.layers):
+        xh = torch.fft.rfftn(h, dim=(-3, -2, -1))
+        w = rw(p[f"spec{l}"])
+        wc = torch.complex(w[..., 0], w[..., 1])
+        out = torch.einsum("bim,mio->bom", xh[:, :, kx, ky, kz], wc)
+        yh = torch.zeros((h.shape[0], wc.shape[2]) + tuple(xh.shape[2:]), dtype=xh.dtype,
+                         device=a.device)
+        yh[:, :, kx, ky, kz] = out
+        h = F.gelu(pw(h, p[f"w{l}"], p[f"b{l}"]) + inverse_half_spectrum(yh, n))
+    return pw(h, p["proj_w"], p["proj_b"])
+
+
+def tiny(n, seed=3):
+    import torch
+    from jaxmaterials_b200.learned.network import SpectralNet
+
+    net = SpectralNet(width=4, layers=2, modes=(4, 4, 3), out_channels=6, seed=seed)
+    g = torch.Generator().manual_seed(seed + 1)
+    for v in net.params.values():  # nonzero biases, so that they are tested too
+        if v.dim() == 1:
+            v.data.copy_((torch.rand(v.shape, generator=g) - 0.5).to(v.device))
+    a = torch.randn((2, 2) + n, generator=g).cuda()
+    return net, a
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (8, 6, 10), (10, 8, 7)])
+def test_forward_matches_oracle(n):
+    net, a = tiny(n)
+    y = net(a).detach().cpu().numpy()
+    ref = SO.forward(rounded_params(net), a.double().cpu().numpy(), net.layers, net.modes)
+    assert np.abs(y - ref).max() / np.abs(ref).max() < 1e-5
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (10, 8, 7)])
+def test_gradients_match_oracle_fd(n):
+    import torch
+
+    net, a = tiny(n)
+    rng = np.random.default_rng(7)
+    wts = rng.standard_normal((2, 6) + n)
+    out = net(a)
+    (out * torch.as_tensor(wts, device="cuda", dtype=torch.float32)).sum().backward()
+    params = rounded_params(net)
+    a64 = a.double().cpu().numpy()
+    for name, p in net.params.items():
+        g = p.grad.detach().double().cpu().numpy()
+        scale = np.abs(g).max()
+        for _ in range(3):
+            idx = tuple(int(rng.integers(s)) for s in g.shape)
+            fd = SO.fd_gradient(params, a64, net.layers, net.modes, wts, name, idx)
+            assert abs(g[idx] - fd) <= 2e-3 * scale, (name, idx, g[idx], fd)
+
+
+def test_gradients_match_torch_autograd():
+    import torch
+
+    net, a = tiny((8, 8, 8))
+    wts = torch.randn((2, 6, 8, 8, 8), device="cuda")
+    (net(a) * wts).sum().backward()
+    mine = {k: v.grad.clone() for k, v in net.params.items()}
+    for v in net.params.values():
+        v.grad = None
+    (torch_reference(net, a) * wts).sum().backward()
+    for k, v in net.params.items():
+        err = (mine[k] - v.grad).abs().max() / v.grad.abs().max()
+        assert err < 1e-4, (k, float(err))
+
+
+def test_full_width_forward_matches_torch():
+    """The 32-channel, 12-mode configuration (kernel pairs (2,32), (32,32), (32,36)) at
+    32^3 against the torch restatement."""
+    import torch
+    from jaxmaterials_b200.learned.network import SpectralNet
+
+    net = SpectralNet(seed=5)
+    a = torch.randn((2, 2, 32, 32, 32), device="cuda")
+    with torch.no_grad():
+        y = net(a)
+        ref = torch_reference(net, a)
+    assert ((y - ref).abs().max() / ref.abs().max()) < 1e-4
+
+
+def test_adam_kernel():
+    import torch
+    from jaxmaterials_b200.learned.network import Adam
+
+    p = torch.randn(1000, device="cuda", requires_grad=True)
+    opt = Adam([p], lr=1e-2)
+    ref = p.detach().clone()
+    m = torch.zeros_like(ref)
+    v = torch.zeros_like(ref)
+    for t in range(1, 4):
+        g = torch.randn(1000, device="cuda")
+        p.grad = g.clone()
+        opt.step()
+        m = 0.9 * m + 0.1 * g
+        v = 0.999 * v + 0.001 * g * g
+        ref = ref - 1e-2 * (m / (1 - 0.9 ** t)) / (torch.sqrt(v / (1 - 0.999 ** t)) + 1e-8)
+    assert torch.allclose(p.detach(), ref, rtol=1e-5, atol=1e-6)
+
+
+def test_warm_start_from_solution_needs_no_iterations():
+    """With the cold start's criterion as the reference, a solve started from the cold
+    solution stops at once; without it the stricter relative threshold makes it iterate."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.learned import warm_start as W
+    from jaxmaterials_b200.solver import Solver
+
+    ind = torch.as_tensor(W.indicators(W.structure_params(2, 32, 9), workers=1)).cuda()
+    lm, mu = W.lame_from_indicator(ind)
+    g = GridSpec(32, 32, 32, 32.0, 32.0, 32.0)
+    s = Solver(g, batch=12, depth=5)
+    eb = np.tile(np.eye(6, dtype=np.float32), (2, 1))
+    cold = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False)
+    e0 = s.solve(lm, mu, eb, maxiter=0, want_sigma=False).residual
+    cold_again = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False)
+    np.testing.assert_allclose(e0, s.history()[:, 0], rtol=1e-12)
+    np.testing.assert_array_equal(cold_again.iters, cold.iters)
+    warm = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False,
+                   epsilon0=cold.epsilon, e0_ref=e0)
+    assert (warm.iters == 0).all()
+    again = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False,
+                    epsilon0=cold.epsilon)
+    assert (again.iters > 0).all()
+
+
+def test_training_pipeline_small():
+    """Data from the solver, a few training epochs, cold vs warm evaluation (16^3)."""
+    import torch
+    from jaxmaterials_b200.learned import warm_start as W
+    from jaxmaterials_b200.learned.network import SpectralNet
+
+    ind = torch.as_tensor(W.indicators(W.structure_params(8, 16, 1), workers=1)).cuda()
+    targets, it = W.solve_dataset(ind, chunk=4)
+    assert targets.shape == (8, 36, 16, 16, 16) and (it > 0).all()
+    net = SpectralNet(modes=(8, 8, 8), seed=2)
+    losses = W.train(net, ind, targets, epochs=3, batch=4, lr=3e-3)
+    assert losses[-1] < losses[0]
+    summ = W.summarise(W.evaluate(net, ind[:4], chunk=4), 16)
+    assert summ["c_eff_warm_vs_cold_rel_max"] < 1e-5
+    assert summ["warm_iters_per_solve"] > 0
