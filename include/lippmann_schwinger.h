@@ -103,7 +103,14 @@ int lsb_set_lame_group(lsb_solver *solver, int instances_per_field);
 /* Solves `batch` instances that share d_lambda, d_mu (device float[nv]), or, after
  * lsb_set_lame_group(solver, k), read structure b / k of [batch / k][nv] arrays.
  * eps_bar:   host float[batch*6]
- * d_eps0:    optional device float[batch*6*nv] warm start (NULL: eps = eps_bar)
+ * d_eps0:    optional device float[batch*6*nv] warm start (NULL: eps = eps_bar). The
+ *            updates only add compatible fields, so a warm start must itself be
+ *            eps_bar + a compatible zero-mean field (the symmetric gradient of a periodic
+ *            displacement, in this discretisation); an arbitrary field converges to an
+ *            equilibrium that keeps its incompatible part. One update of the homogeneous
+ *            medium lambda = 0, mu = 1/2 from eps0 gives eps1 = eps_bar + (I - P)(eps0 -
+ *            eps_bar), P the projection onto compatible fields, so eps0 + eps_bar - eps1 is
+ *            the compatible part (Solver.project_compatible in the Python package).
  * d_eps:     device float[batch*6*nv] output strain
  * d_sigma:   optional device float[batch*6*nv] output stress sigma(eps)
  * mean_sigma: optional host double[batch*6], mean stress per instance (FP64 sums)

@@ -6,7 +6,8 @@ library for the six unit loads (Anderson, tol 1e-6). Inputs are kept on the devi
 phase indicators (uint8), targets as BF16 strain fluctuations eps - e_k [36][nv].
 
 Evaluation: for held-out structures, the cold solve starts from eps = e_k; the warm
-solve starts from the network's prediction and stops at the same absolute residual as
+solve starts from the compatible part of the network's prediction (the iteration keeps
+any incompatible part of its start, see Solver.project_compatible) and stops at the same absolute residual as
 the cold one (its threshold is rtol times the cold start's first criterion, obtained
 from a maxiter = 0 solve and passed as the reference criterion). Reported: iterations of
 both, wall time of both (the warm time includes inference and the extra criterion
@@ -147,9 +148,10 @@ def evaluate(net, ind, depth=5, rtol=1e-6, chunk=16, maxiter=5000):
         eps0 = net.warm_start(lm, mu)                      # [c, 6, 6, n, n, n]
         torch.cuda.synchronize()
         t2 = time.perf_counter()
+        eps0 = s.project_compatible(eps0.reshape(6 * c, 6, n, n, n), eb)
         e0 = s.solve(lm, mu, eb, maxiter=0, want_sigma=False).residual
         warm = s.solve(lm, mu, eb, rtol=rtol, maxiter=maxiter, want_sigma=False,
-                       epsilon0=eps0.reshape(6 * c, 6, n, n, n), e0_ref=e0)
+                       epsilon0=eps0, e0_ref=e0)
         torch.cuda.synchronize()
         t3 = time.perf_counter()
         out["cold_s"] += t1 - t0
@@ -161,8 +163,8 @@ def evaluate(net, ind, depth=5, rtol=1e-6, chunk=16, maxiter=5000):
         out["warm_iters"].append(warm.iters.reshape(c, 6))
         out["c_eff"].append(cold.mean_sigma.reshape(c, 6, 6))
         out["c_eff_warm"].append(warm.mean_sigma.reshape(c, 6, 6))
-        # network C_eff: mean stress of the predicted strain fields
-        e = eps0.double()
+        # network C_eff: mean stress of the (projected) predicted strain fields
+        e = eps0.view(c, 6, 6, n, n, n).double()
         tr = e[:, :, 0] + e[:, :, 1] + e[:, :, 2]
         lmd, mud = lm.double().unsqueeze(1), mu.double().unsqueeze(1)
         sig = 2.0 * mud.unsqueeze(2) * e

@@ -219,6 +219,31 @@ class Solver:
         self._last_maxiter = int(maxiter)
         return SolveResult(eps, sig, iters, status, resid, mean)
 
+    def project_compatible(self, epsilon, epsilon_bar):
+        """Compatible part of strain fields, for use as a warm start:
+        eps_bar + P(eps - eps_bar), P = Gamma^0 C^0 the projection onto zero-mean compatible
+        fields of this solver's discretisation (modified wave vectors). Computed as one
+        update of the homogeneous medium lambda = 0, mu = 1/2 started from eps, which gives
+        eps_bar + (I - P)(eps - eps_bar). epsilon: (B, 6, nx, ny, nz) float32 CUDA tensor,
+        epsilon_bar: (B, 6). Returns a new tensor."""
+        import torch
+
+        g = self.grid_spec
+        eb = np.ascontiguousarray(np.atleast_2d(np.asarray(
+            epsilon_bar.cpu() if isinstance(epsilon_bar, torch.Tensor) else epsilon_bar,
+            dtype=np.float32)))
+        lam0 = torch.zeros(g.shape, device=self.device, dtype=torch.float32)
+        mu0 = torch.full(g.shape, 0.5, device=self.device, dtype=torch.float32)
+        prec = self.precision
+        self.set_precision("fp32", 0)
+        try:
+            r = self.solve(lam0, mu0, eb, rtol=0.0, atol=0.0, maxiter=1, epsilon0=epsilon,
+                           want_sigma=False)
+        finally:
+            self.set_precision(prec)
+        ebt = torch.as_tensor(eb, device=self.device).view(eb.shape[0], 6, 1, 1, 1)
+        return epsilon + ebt - r.epsilon
+
     def kernel_launches(self):
         """Kernels enqueued by this solver so far."""
         return int(self._lib.lsb_kernel_launches(self._h))

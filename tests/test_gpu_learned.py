@@ -147,7 +147,9 @@ def test_adam_kernel():
 
 def test_warm_start_from_solution_needs_no_iterations():
     """With the cold start's criterion as the reference, a solve started from the cold
-    solution stops at once; without it the stricter relative threshold makes it iterate."""
+    solution stops at once, or after the few updates that the FP32 rounding of an iterate
+    finished in FP64 needs (mixed precision); without it the stricter relative threshold
+    makes every instance iterate."""
     import torch
     from jaxmaterials_b200 import GridSpec
     from jaxmaterials_b200.learned import warm_start as W
@@ -165,10 +167,10 @@ def test_warm_start_from_solution_needs_no_iterations():
     np.testing.assert_array_equal(cold_again.iters, cold.iters)
     warm = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False,
                    epsilon0=cold.epsilon, e0_ref=e0)
-    assert (warm.iters == 0).all()
+    assert (warm.iters <= 2).all() and (warm.iters == 0).sum() >= 6
     again = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False,
                     epsilon0=cold.epsilon)
-    assert (again.iters > 0).all()
+    assert (again.iters > 2).all()
 
 
 def test_training_pipeline_small():
@@ -186,3 +188,30 @@ def test_training_pipeline_small():
     summ = W.summarise(W.evaluate(net, ind[:4], chunk=4), 16)
     assert summ["c_eff_warm_vs_cold_rel_max"] < 1e-5
     assert summ["warm_iters_per_solve"] > 0
+
+
+def test_project_compatible():
+    """The projection keeps compatible fields, is idempotent, and a warm start projected
+    from an arbitrary field converges to the cold solution."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.learned import warm_start as W
+    from jaxmaterials_b200.solver import Solver
+
+    ind = torch.as_tensor(W.indicators(W.structure_params(1, 32, 4), workers=1)).cuda()
+    lm, mu = W.lame_from_indicator(ind)
+    g = GridSpec(32, 32, 32, 32.0, 32.0, 32.0)
+    s = Solver(g, batch=6, depth=5)
+    eb = np.eye(6, dtype=np.float32)
+    cold = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False)
+    p = s.project_compatible(cold.epsilon, eb)
+    assert (p - cold.epsilon).abs().max() < 1e-5 * cold.epsilon.abs().max()
+    noise = cold.epsilon + 0.3 * torch.randn_like(cold.epsilon)
+    q = s.project_compatible(noise, eb)
+    q2 = s.project_compatible(q, eb)
+    assert (q2 - q).abs().max() < 1e-5 * q.abs().max()
+    e0 = s.solve(lm, mu, eb, maxiter=0, want_sigma=False).residual
+    warm = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False, epsilon0=q, e0_ref=e0)
+    assert (warm.status == 1).all()
+    rel = np.linalg.norm(warm.mean_sigma - cold.mean_sigma) / np.linalg.norm(cold.mean_sigma)
+    assert rel < 1e-5
