@@ -222,13 +222,15 @@ class SpectralNet:
         return out + eye
 
     def state_dict(self):
+        import torch
+
         sd = {k: v.detach().cpu() for k, v in self.params.items()}
-        sd["_config"] = np.array([self.width, self.layers, *self.modes, self.out_channels])
+        sd["_config"] = torch.tensor([self.width, self.layers, *self.modes, self.out_channels])
         return sd
 
     @classmethod
     def from_state_dict(cls, sd, device="cuda"):
-        cfg = [int(v) for v in np.asarray(sd["_config"])]
+        cfg = [int(v) for v in sd["_config"]]
         net = cls(width=cfg[0], layers=cfg[1], modes=tuple(cfg[2:5]), out_channels=cfg[5],
                   device=device)
         for k in net.params:
