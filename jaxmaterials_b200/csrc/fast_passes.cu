@@ -361,8 +361,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// Modes as the generic z pass: 0 init from eps_bar/eps0, 1 plain update, 2 keep eps,
-// 3 Anderson residual (rings + Gram-row partials), 4 Anderson combine.
+// Modes as the generic z pass: 0 init from eps_bar/eps0, 1 plain update, 2 keep eps
+// (not rewritten), 3 Anderson residual into the rings.
 // bulk: the block's global chunks are 16-byte aligned (TMA bulk copies); otherwise the
 // staging buffers are filled by ordinary loads.
 template <int NZ>
@@ -378,7 +378,6 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
   float2* rst = reinterpret_cast<float2*>(zfraw + LY.rst);    // [6][L][NZH] spectrum rows
   float* est = reinterpret_cast<float*>(zfraw + LY.est);      // [6][L][NZ] strain rows
   float* lst = reinterpret_cast<float*>(zfraw + LY.lst);      // [2][L][NZ] lambda, mu rows
-  __shared__ double gred[kMaxDepth + 1][32];
   __shared__ __align__(8) unsigned long long mbar_word;
   const int b = blockIdx.y;
   if (!active32(st[b])) return;
@@ -459,20 +458,12 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
     zline_fft<NZ>(zbuf, q, p, tw);
   }
 
-  int slot = 0, filled = 0;
-  const int M1 = aa.depth + 1;
-  const size_t ring = (size_t)6 * g.nv;
-  if (mode >= 3) {
-    const int j = st[b].iter - 1 - st[b].aa_base;
-    slot = j % M1;
-    filled = j + 1 < M1 ? j + 1 : M1;
-  }
   if (mode == 3) {
+    const int M1 = aa.depth + 1;
+    const size_t ring = (size_t)6 * g.nv;
+    const int slot = (st[b].iter - 1 - st[b].aa_base) % M1;
     float* rb = aa.r + (size_t)b * M1 * ring;
     float* gb = aa.g + (size_t)b * M1 * ring;
-    double dots[kMaxDepth + 1];
-#pragma unroll
-    for (int qq = 0; qq <= kMaxDepth; ++qq) dots[qq] = 0.0;
     const float inv_nv = (float)(1.0 / (double)g.nv);
     for (int idx = tid; idx < L * NZ; idx += nt) {
       const int l = idx / NZ, n = idx % NZ;
@@ -490,35 +481,6 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
         rb[slot * ring + o] = r[c];
         gb[slot * ring + o] = est[c * L * NZ + idx] + r[c];
       }
-      for (int qq = 0; qq < filled; ++qq) {
-        double d = 0.0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          const float rs = qq == slot ? r[c] : rb[qq * ring + (size_t)c * g.nv + vx];
-          d += (c < 3 ? 1.0 : 2.0) * (double)r[c] * (double)rs;
-        }
-        dots[qq] += d;
-      }
-    }
-    // Warp sums. The block may end in a partial warp (3 L P threads, e.g. 144); its lane
-    // count is a power of two, so the xor tree over the lanes that exist is complete.
-    static_assert(3 * L * P <= 192, "z pass block larger than its launch bound");
-    static_assert((3 * L * P) % 32 == 0 || (((3 * L * P) % 32) & ((3 * L * P) % 32 - 1)) == 0,
-                  "the last warp of the z pass must have a power-of-two lane count");
-    const int wlanes = min(32, nt - (tid & ~31));
-    const unsigned wmask = wlanes == 32 ? 0xffffffffu : ((1u << wlanes) - 1u);
-    for (int qq = 0; qq < filled; ++qq) {
-      double a = dots[qq];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1)
-        if (off < wlanes) a += __shfl_xor_sync(wmask, a, off);
-      if ((tid & 31) == 0) gred[qq][tid >> 5] = a;
-    }
-    __syncthreads();
-    if (tid < filled) {
-      double a = 0.0;
-      for (int w = 0; w < (nt + 31) / 32; ++w) a += gred[tid][w];
-      aa.partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + tid] = a;
     }
     return;
   }
@@ -555,16 +517,6 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
       } else if (mode == 2) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = est[c * L * NZ + idx];
-      } else if (mode == 4) {
-        const float* gb = aa.g + (size_t)b * M1 * ring;
-        const double* al = aa.alpha + (size_t)b * M1;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) e[c] = 0.f;
-        for (int qq = 0; qq < filled; ++qq) {
-          const float a = (float)al[qq];
-#pragma unroll
-          for (int c = 0; c < 6; ++c) e[c] += a * gb[qq * ring + (size_t)c * g.nv + vx];
-        }
       } else if (eps0 != nullptr) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * g.nv + vx];
@@ -572,8 +524,10 @@ __global__ void __launch_bounds__(192, 2) zpass_fast(
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = (float)eps_bar[b * 6 + c];
       }
+      if (mode != 2) {
 #pragma unroll
-      for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + vx] = e[c];
+        for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + vx] = e[c];
+      }
       const float lam = lst[idx], tmu = 2.f * lst[L * NZ + idx];
       const float ltr = lam * (e[0] + e[1] + e[2]);
       float s[6];

@@ -31,10 +31,10 @@ __device__ __forceinline__ bool active(const InstanceState& s) {
 // Lines l = x * ny + y; pair p of components (2p, 2p+1) shares one complex line
 // z = a + i b (two real transforms for the price of one complex transform).
 // mode 0: eps = eps_bar (or eps0); mode 1: eps += r / N with r from the spectrum;
-// mode 2: keep eps (continuation of an instance in another precision);
-// mode 3: Anderson residual: r from the spectrum into the rings, g = eps + r, FP64
-//         Gram-row partials <r_j, r_s>_w (no stress, no forward transform);
-// mode 4: Anderson combine: eps = sum_s alpha_s g_s, then stress and forward transform.
+// mode 2: keep eps (continuation of an instance in another precision, or the iterate
+//         written by anderson_combine_kernel); eps is not rewritten;
+// mode 3: Anderson residual: r from the spectrum into the rings, g = eps + r (no stress,
+//         no forward transform; anderson_gram_kernel then forms the Gram row).
 template <typename T>
 __device__ __forceinline__ void anderson_slots(const InstanceState& s, int depth, int& slot, int& filled) {
   const int j = s.iter - 1 - s.aa_base;
@@ -73,7 +73,6 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char zraw[];
   C* zbuf = reinterpret_cast<C*>(zraw);
-  __shared__ double gred[kMaxDepth + 1][32];
   const int b = blockIdx.y;
   if (!active<T>(st[b])) return;
   const int nz = g.nz, nzh = g.nzh;
@@ -112,16 +111,13 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
   }
 
   if (mode == 3) {
-    // Anderson residual: rings and Gram-row partials, then done.
+    // Anderson residual: rings, then done.
     int slot, filled;
     anderson_slots<T>(st[b], aa.depth, slot, filled);
     const int M1 = aa.depth + 1;
     const size_t ring = (size_t)6 * g.nv;   // one slot
     T* rb = aa.r + (size_t)b * M1 * ring;
     T* gb = aa.g + (size_t)b * M1 * ring;
-    double dots[kMaxDepth + 1];
-#pragma unroll
-    for (int q = 0; q <= kMaxDepth; ++q) dots[q] = 0.0;
     const T inv_nv = (T)(1.0 / (double)g.nv);
     for (int idx = tid; idx < L * nz; idx += nt) {
       int l = idx / nz, n = idx - l * nz;
@@ -141,19 +137,7 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
         rb[slot * ring + o] = r[c];
         gb[slot * ring + o] = eb[o] + r[c];
       }
-      for (int q = 0; q < filled; ++q) {
-        double d = 0.0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          const T rs = q == slot ? r[c] : rb[q * ring + (size_t)c * g.nv + v];
-          d += (c < 3 ? 1.0 : 2.0) * (double)r[c] * (double)rs;
-        }
-        dots[q] += d;
-      }
     }
-    double out[kMaxDepth + 1];
-    block_sum_slots(dots, filled, gred, out);
-    if (tid < filled) aa.partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + tid] = out[tid];
     return;
   }
 
@@ -198,20 +182,6 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
       } else if (mode == 2) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * g.nv + v];
-      } else if (mode == 4) {
-        int slot, filled;
-        anderson_slots<T>(st[b], aa.depth, slot, filled);
-        const int M1 = aa.depth + 1;
-        const size_t ring = (size_t)6 * g.nv;
-        const T* gb = aa.g + (size_t)b * M1 * ring;
-        const double* al = aa.alpha + (size_t)b * M1;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) e[c] = 0;
-        for (int q = 0; q < filled; ++q) {
-          const T a = (T)al[q];
-#pragma unroll
-          for (int c = 0; c < 6; ++c) e[c] += a * gb[q * ring + (size_t)c * g.nv + v];
-        }
       } else if (eps0 != nullptr) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * g.nv + v];
@@ -219,8 +189,10 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
 #pragma unroll
         for (int c = 0; c < 6; ++c) e[c] = (T)eps_bar[b * 6 + c];
       }
+      if (mode != 2) {
 #pragma unroll
-      for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + v] = e[c];
+        for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + v] = e[c];
+      }
       const T lam = lambda[v], tmu = (T)2 * mu[v];
       const T ltr = lam * (e[0] + e[1] + e[2]);
       T s[6];
@@ -498,6 +470,94 @@ __global__ void finalize_kernel(int nblk, int phase, InstanceState* __restrict__
   }
   s.iter += 1;
 }
+
+// Gram-row partials of the newest residual r_j (slot j of the ring) for every instance in
+// `phase`: partials[b][blk][q] = sum over block blk's voxels of sum_c w_c r_j r_q, with
+// Voigt weights w = (1,1,1,2,2,2), in FP64 (lippmann_schwinger.py:217-231). A streaming
+// kernel of its own: every ring value of a voxel is requested before the first product,
+// so each thread keeps 6 M1 loads in flight (M1 = depth + 1 slots, a template constant).
+template <typename T, int M1>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) anderson_gram_kernel(long long nv, int phase,
+                                                               const InstanceState* __restrict__ st,
+                                                               const T* __restrict__ r,
+                                                               double* __restrict__ partials) {
+  __shared__ double red[kMaxDepth + 1][32];
+  const int b = blockIdx.y;
+  const InstanceState& s = st[b];
+  if (s.done || s.phase != phase) return;
+  int slot, filled;
+  anderson_slots<T>(s, M1 - 1, slot, filled);
+  const size_t ring = (size_t)6 * nv;
+  const T* rb = r + (size_t)b * M1 * ring;
+  double dots[M1];
+#pragma unroll
+  for (int q = 0; q < M1; ++q) dots[q] = 0.0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv;
+       v += (long long)gridDim.x * blockDim.x) {
+    T rq[M1][6];
+#pragma unroll
+    for (int q = 0; q < M1; ++q)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) rq[q][c] = q < filled ? rb[q * ring + (size_t)c * nv + v] : (T)0;
+    double rn[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      T x = rq[0][c];
+#pragma unroll
+      for (int q = 1; q < M1; ++q) x = q == slot ? rq[q][c] : x;
+      rn[c] = (c < 3 ? 1.0 : 2.0) * (double)x;
+    }
+#pragma unroll
+    for (int q = 0; q < M1; ++q) {
+      if (q < filled) {
+        double d = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) d += rn[c] * (double)rq[q][c];
+        dots[q] += d;
+      }
+    }
+  }
+  double pad[kMaxDepth + 1];
+#pragma unroll
+  for (int q = 0; q <= kMaxDepth; ++q) pad[q] = q < M1 ? dots[q < M1 ? q : 0] : 0.0;
+  double out[kMaxDepth + 1];
+  block_sum_slots(pad, filled, red, out);
+  if ((int)threadIdx.x < filled)
+    partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + threadIdx.x] = out[threadIdx.x];
+}
+
+// Anderson combine for every instance in `phase`: eps = sum_s alpha_s g_s over the filled
+// slots (lippmann_schwinger.py:228-231), accumulated in the field precision in slot order.
+template <typename T, int M1>
+__global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int phase,
+                                                               const InstanceState* __restrict__ st,
+                                                               const T* __restrict__ g,
+                                                               const double* __restrict__ alpha,
+                                                               T* __restrict__ eps) {
+  const int b = blockIdx.y;
+  const InstanceState& s = st[b];
+  if (s.done || s.phase != phase) return;
+  int slot, filled;
+  anderson_slots<T>(s, M1 - 1, slot, filled);
+  const T* gb = g + (size_t)b * M1 * n6;
+  const double* al = alpha + (size_t)b * M1;
+  T a[M1];
+#pragma unroll
+  for (int q = 0; q < M1; ++q) a[q] = q < filled ? (T)al[q] : (T)0;
+  T* eb = eps + (size_t)b * n6;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n6;
+       i += (long long)gridDim.x * blockDim.x) {
+    T gv[M1];
+#pragma unroll
+    for (int q = 0; q < M1; ++q) gv[q] = q < filled ? gb[q * n6 + i] : (T)0;
+    T e = 0;
+#pragma unroll
+    for (int q = 0; q < M1; ++q)
+      if (q < filled) e += a[q] * gv[q];
+    eb[i] = e;
+  }
+}
+
 
 // Anderson mixing coefficients (lippmann_schwinger.py:219-228): the new Gram row
 // <r_j, r_s>_w replaces row and column `slot` of A (the reference's roll of A is a
@@ -824,6 +884,33 @@ void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const Ins
 }
 
 template <typename T>
+void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batch,
+                          const InstanceState* st, const T* r, double* partials, cudaStream_t stream) {
+  const dim3 grid(nblk, batch);
+  switch (depth + 1) {
+#define LSB_GRAM(M) \
+    case M: anderson_gram_kernel<T, M><<<grid, 256, 0, stream>>>(nv, phase, st, r, partials); break;
+    LSB_GRAM(2) LSB_GRAM(3) LSB_GRAM(4) LSB_GRAM(5) LSB_GRAM(6) LSB_GRAM(7) LSB_GRAM(8) LSB_GRAM(9)
+#undef LSB_GRAM
+    default: break;
+  }
+}
+
+template <typename T>
+void launch_anderson_combine(long long nv, int depth, int phase, int batch, const InstanceState* st,
+                             const T* g, const double* alpha, T* eps, cudaStream_t stream) {
+  const long long n6 = 6 * nv;
+  const dim3 grid((unsigned)std::min<long long>(2048, (n6 + 255) / 256), batch);
+  switch (depth + 1) {
+#define LSB_COMB(M) \
+    case M: anderson_combine_kernel<T, M><<<grid, 256, 0, stream>>>(n6, phase, st, g, alpha, eps); break;
+    LSB_COMB(2) LSB_COMB(3) LSB_COMB(4) LSB_COMB(5) LSB_COMB(6) LSB_COMB(7) LSB_COMB(8) LSB_COMB(9)
+#undef LSB_COMB
+    default: break;
+  }
+}
+
+template <typename T>
 void launch_ypass(const GridDesc& g, const LaunchShape& s, bool inverse, int batch, cplx<T>* spec,
                   const InstanceState* st, cudaStream_t stream) {
   dim3 grid(s.y_tiles, g.nx, 6 * batch);
@@ -893,7 +980,11 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
                                 const InstanceState*, cudaStream_t);                            \
   template void launch_xpass<T>(const GridDesc&, const LaunchShape&, int, cplx<T>*,             \
                                 const Medium*, InstanceState*, double*, cudaStream_t);          \
-  template void launch_medium<T>(long long, int, const T*, const T*, double*, Medium*, cudaStream_t);
+  template void launch_medium<T>(long long, int, const T*, const T*, double*, Medium*, cudaStream_t); \
+  template void launch_anderson_gram<T>(long long, int, int, int, int, const InstanceState*,    \
+                                        const T*, double*, cudaStream_t);                       \
+  template void launch_anderson_combine<T>(long long, int, int, int, const InstanceState*,      \
+                                           const T*, const double*, T*, cudaStream_t);
 LSB_INST(float)
 LSB_INST(double)
 #undef LSB_INST

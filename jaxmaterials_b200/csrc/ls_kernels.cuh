@@ -28,12 +28,21 @@ cudaError_t configure_kernels();
 // and its phase matches the precision T (float: phase 0, double: phase 1). Instance b
 // reads the Lame fields of structure b / g.lame_group and the medium med[b / g.lame_group].
 // mode 0: eps = eps_bar (or eps0 if given); mode 1: eps += r / N from spec; mode 2: keep
-// eps and the stored shift (continuation in another precision).
-// modes 3/4: Anderson residual / combine (see ls_kernels.cu).
+// eps and the stored shift (continuation in another precision, or after the Anderson
+// combine); mode 3: Anderson residual into the rings (see ls_kernels.cu).
 template <typename T>
 void launch_zpass(const GridDesc& g, const LaunchShape& ls, int mode, int batch, const T* lambda,
                   const T* mu, T* eps, cplx<T>* spec, const double* eps_bar, const T* eps0,
                   InstanceState* st, const Medium* med, const AndersonArgs<T>& aa, cudaStream_t s);
+// Gram-row partials [batch][nblk][depth+1] of the newest residual of every instance in
+// `phase` (r: the residual ring [batch][depth+1][6][nv]).
+template <typename T>
+void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batch,
+                          const InstanceState* st, const T* r, double* partials, cudaStream_t s);
+// eps = sum_s alpha_s g_s for every instance in `phase` (g: [batch][depth+1][6][nv]).
+template <typename T>
+void launch_anderson_combine(long long nv, int depth, int phase, int batch, const InstanceState* st,
+                             const T* g, const double* alpha, T* eps, cudaStream_t s);
 // Anderson coefficients of every instance in `phase` from the Gram-row partials.
 void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
                            const double* partials, double* amat, double* alpha, cudaStream_t s);

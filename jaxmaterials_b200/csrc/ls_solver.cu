@@ -324,15 +324,6 @@ void pass_z(lsb_solver* s, int mode, int batch, const T* lam, const T* mu, T* ep
 }
 
 template <typename T>
-int z_blocks_of(const lsb_solver* s) {
-  if constexpr (sizeof(T) == 4) {
-    if (s->fast32) return fast::z_blocks(s->g);
-    return s->sh32.z_blocks;
-  }
-  return s->sh64.z_blocks;
-}
-
-template <typename T>
 void pass_y(lsb_solver* s, bool inverse, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
     if (s->fast32) {
@@ -366,6 +357,9 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   cudaStream_t st = s->stream;
   const AndersonArgs<T> aa = anderson_args<T>(s, anderson && s->depth > 0);
   const bool mix = aa.depth > 0;
+  // blocks per instance of the Gram-row kernel (its partials fit the z-block-sized buffer)
+  const int gblk = (int)std::max<long long>(
+      1, std::min<long long>({(long long)s->aa_zblocks, 592LL, (s->g.nv + 255) / 256}));
   pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0, aa);
   pass_y<T>(s, false, batch, spec);
   s->launches += 2;
@@ -380,17 +374,22 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
       launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
       pass_y<T>(s, true, batch, spec);
       if (mix) {
+        // residual into the rings, Gram row, coefficients, combine, stress + forward z
         pass_z<T>(s, 3, batch, lam, mu, eps, spec, nullptr, aa);
-        launch_anderson_solve(z_blocks_of<T>(s), s->depth, phase, batch, s->d_state,
-                              s->d_aa_partials, s->d_aa_mat, s->d_aa_alpha, st);
-        pass_z<T>(s, 4, batch, lam, mu, eps, spec, nullptr, aa);
+        launch_anderson_gram<T>(s->g.nv, gblk, s->depth, phase, batch, s->d_state, aa.r,
+                                s->d_aa_partials, st);
+        launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
+                              s->d_aa_mat, s->d_aa_alpha, st);
+        launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g,
+                                   s->d_aa_alpha, eps, st);
+        pass_z<T>(s, 2, batch, lam, mu, eps, spec, nullptr, aa);
       } else {
         pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
       }
       pass_y<T>(s, false, batch, spec);
     }
     launched += n;
-    s->launches += (mix ? 7LL : 5LL) * n;
+    s->launches += (mix ? 9LL : 5LL) * n;
     LSB_CUDA(cudaGetLastError());
     LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch,
                              cudaMemcpyDeviceToHost, st));
