@@ -92,6 +92,12 @@ int lsb_set_precision(lsb_solver *solver, int precision, int stall_window);
  * same absolute residual as the cold solve. e0 = NULL clears it. */
 int lsb_set_reference_e0(lsb_solver *solver, int batch, const double *e0);
 
+/* No reference counterpart. on != 0 (default): each phase of a solve captures one
+ * iteration's launches into a CUDA graph on a stream of the solver's own (ordered after
+ * the work already on the solver's stream, and that stream waits for it) and replays it;
+ * on = 0 launches the kernels one by one on the solver's stream. */
+int lsb_set_graphs(lsb_solver *solver, int on);
+
 /* No reference counterpart. Groups instances by microstructure: with
  * instances_per_field = k > 0, instance b of a solve reads the Lame fields of structure
  * b / k from d_lambda, d_mu laid out [batch / k][nv] (and gets that structure's own

@@ -56,7 +56,18 @@ __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restric
 
 // ----------------------------------------------------------------------------- y pass
 // Block = (16 kz columns, x, instance * 6 + component); thread (p, t), t fastest.
-constexpr int kYT = 16;
+// Tile shapes (kz columns per block of the y and x passes; resident x-pass blocks per SM).
+// Compile-time constants; the defaults are the measured best on the B200.
+#ifndef LSB_Y_COLS
+#define LSB_Y_COLS 16
+#endif
+#ifndef LSB_X_COLS_MID
+#define LSB_X_COLS_MID 8
+#endif
+#ifndef LSB_X_MIN_BLOCKS
+#define LSB_X_MIN_BLOCKS 2
+#endif
+constexpr int kYT = LSB_Y_COLS;
 
 template <int NY>
 __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split<NY>::P + 31) / 32))) ypass_fast(GridDesc g, int inverse,
@@ -103,7 +114,7 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split
 // layout [k1][p][t] with rows of P*T + T values (the padding makes the column reads of
 // the second step conflict-free).
 template <int NX>
-__host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ? 4 : 8); }
+__host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ? 4 : LSB_X_COLS_MID); }
 template <int NX>
 __host__ __device__ constexpr int x_row() { return Split<NX>::P * x_cols<NX>() + x_cols<NX>(); }
 template <int NX>
@@ -112,7 +123,7 @@ __host__ __device__ constexpr int x_region() {
 }
 
 template <int NX>
-__global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), 2) xpass_fast(
+__global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), LSB_X_MIN_BLOCKS) xpass_fast(
     GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
     InstanceState* __restrict__ st, double* __restrict__ partials) {
   constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols<NX>(), RS = x_row<NX>(), REG = x_region<NX>();

@@ -349,11 +349,74 @@ void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
 // Runs the loop of precision T for every instance in its phase until none is left there.
 // init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
 // With `anderson` the update is Anderson mixing of depth s->depth (rings of precision T).
+// Moves a phase's work to the solver's graph stream (ordered after everything already on
+// the caller's stream) and back (the caller's stream waits for the phase); owns the graph.
+struct GraphPhase {
+  lsb_solver* s;
+  cudaStream_t user;
+  bool on = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  explicit GraphPhase(lsb_solver* solver) : s(solver), user(solver->stream) {
+    if (!s->use_graphs) return;
+    if (!s->graph_stream && cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      s->graph_stream = nullptr;
+      cudaGetLastError();
+      return;
+    }
+    if ((!s->ev_in && cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming) != cudaSuccess) ||
+        (!s->ev_out && cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming) != cudaSuccess)) {
+      cudaGetLastError();
+      return;
+    }
+    if (cudaEventRecord(s->ev_in, user) != cudaSuccess ||
+        cudaStreamWaitEvent(s->graph_stream, s->ev_in, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    s->stream = s->graph_stream;
+    on = true;
+  }
+  // Captures one enqueue() into a graph; on any failure the phase runs without it.
+  template <typename F>
+  void capture(F&& enqueue) {
+    if (!on) return;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    enqueue();
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      exec = nullptr;
+      graph = nullptr;
+      cudaGetLastError();
+    }
+  }
+  ~GraphPhase() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (on) {
+      cudaEventRecord(s->ev_out, s->stream);
+      cudaStreamWaitEvent(user, s->ev_out, 0);
+      s->stream = user;
+    }
+  }
+};
+
+// Runs the loop of precision T for every instance in its phase until none is left there.
+// init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
+// With `anderson` the update is Anderson mixing of depth s->depth (rings of precision T).
+// One iteration is captured into a CUDA graph and replayed (s->use_graphs).
 template <typename T>
 int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
               const T* eps0, int init_mode, const SolveParams& sp, bool anderson) {
   const LaunchShape& sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
   const int phase = sizeof(T) == 8 ? 1 : 0;
+  GraphPhase gp(s);
   cudaStream_t st = s->stream;
   const AndersonArgs<T> aa = anderson_args<T>(s, anderson && s->depth > 0);
   const bool mix = aa.depth > 0;
@@ -364,29 +427,37 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   pass_y<T>(s, false, batch, spec);
   s->launches += 2;
   LSB_CUDA(cudaGetLastError());
+  auto iteration = [&]() {
+    pass_x<T>(s, batch, spec);
+    launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
+    pass_y<T>(s, true, batch, spec);
+    if (mix) {
+      // residual into the rings, Gram row, coefficients, combine, stress + forward z
+      pass_z<T>(s, 3, batch, lam, mu, eps, spec, nullptr, aa);
+      launch_anderson_gram<T>(s->g.nv, gblk, s->depth, phase, batch, s->d_state, aa.r,
+                              s->d_aa_partials, st);
+      launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
+                            s->d_aa_mat, s->d_aa_alpha, st);
+      launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g,
+                                 s->d_aa_alpha, eps, st);
+      pass_z<T>(s, 2, batch, lam, mu, eps, spec, nullptr, aa);
+    } else {
+      pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
+    }
+    pass_y<T>(s, false, batch, spec);
+  };
+  gp.capture(iteration);
   long long launched = 0;
   const long long max_evals = (long long)sp.maxiter + 2;
   int chunk = 1;
   for (;;) {
     int n = (int)std::min<long long>(chunk, max_evals - launched);
     for (int i = 0; i < n; ++i) {
-      pass_x<T>(s, batch, spec);
-      launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
-      pass_y<T>(s, true, batch, spec);
-      if (mix) {
-        // residual into the rings, Gram row, coefficients, combine, stress + forward z
-        pass_z<T>(s, 3, batch, lam, mu, eps, spec, nullptr, aa);
-        launch_anderson_gram<T>(s->g.nv, gblk, s->depth, phase, batch, s->d_state, aa.r,
-                                s->d_aa_partials, st);
-        launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
-                              s->d_aa_mat, s->d_aa_alpha, st);
-        launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g,
-                                   s->d_aa_alpha, eps, st);
-        pass_z<T>(s, 2, batch, lam, mu, eps, spec, nullptr, aa);
+      if (gp.exec) {
+        LSB_CUDA(cudaGraphLaunch(gp.exec, st));
       } else {
-        pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
+        iteration();
       }
-      pass_y<T>(s, false, batch, spec);
     }
     launched += n;
     s->launches += (mix ? 9LL : 5LL) * n;
@@ -582,6 +653,12 @@ int lsb_set_reference_e0(lsb_solver* solver, int batch, const double* e0) {
   if (!solver->d_e0ref) LSB_CUDA(cudaMalloc(&solver->d_e0ref, sizeof(double) * solver->batch_cap));
   LSB_CUDA(cudaMemcpy(solver->d_e0ref, e0, sizeof(double) * batch, cudaMemcpyHostToDevice));
   solver->use_e0ref = true;
+  return 0;
+}
+
+int lsb_set_graphs(lsb_solver* solver, int on) {
+  if (!solver) return fail(-1, "null solver");
+  solver->use_graphs = on != 0;
   return 0;
 }
 

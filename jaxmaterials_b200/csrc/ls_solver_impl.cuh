@@ -24,6 +24,11 @@ struct lsb_solver {
   GridDesc g{};
   LaunchShape sh32{}, sh64{};
   cudaStream_t stream = nullptr;
+  // The iterations of a phase are captured once into a CUDA graph (one iteration) and
+  // replayed; capture needs a stream of our own, ordered after/before `stream` by events.
+  bool use_graphs = true;
+  cudaStream_t graph_stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   // FP32 work buffers
   float* d_eps32 = nullptr;      // [batch][6][nv] (used when the caller passes no strain buffer)
   float2* d_spec32 = nullptr;    // [batch][6][nm]
@@ -71,6 +76,9 @@ struct lsb_solver {
                     d_aa_alpha, d_e0ref};
     for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
+    if (graph_stream) cudaStreamDestroy(graph_stream);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
   }
 };
 

@@ -136,6 +136,10 @@ class Solver:
                    "lsb_set_precision")
         self.precision = precision
 
+    def set_graphs(self, on=True):
+        """Replay each iteration as a CUDA graph (default) or launch kernel by kernel."""
+        _lib.check(self._lib.lsb_set_graphs(self._h, 1 if on else 0), "lsb_set_graphs")
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             self._lib.lsb_destroy(self._h)
