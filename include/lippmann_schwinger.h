@@ -92,6 +92,12 @@ int lsb_set_precision(lsb_solver *solver, int precision, int stall_window);
  * same absolute residual as the cold solve. e0 = NULL clears it. */
 int lsb_set_reference_e0(lsb_solver *solver, int batch, const double *e0);
 
+/* No reference counterpart. Tile variant of the FP32 x pass (extents 32-128: 0 = the
+ * wide tile, 1 = half as many kz columns per block with twice the resident blocks). By
+ * default the solver times both on its first FP32 solve and keeps the faster. variant =
+ * 0 or 1 fixes it, -1 only queries. Returns the variant in use (0 before tuning). */
+int lsb_tile_variant(lsb_solver *solver, int variant);
+
 /* No reference counterpart. on != 0 (default): each phase of a solve captures one
  * iteration's launches into a CUDA graph on a stream of the solver's own (ordered after
  * the work already on the solver's stream, and that stream waits for it) and replays it;

@@ -56,16 +56,10 @@ __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restric
 
 // ----------------------------------------------------------------------------- y pass
 // Block = (16 kz columns, x, instance * 6 + component); thread (p, t), t fastest.
-// Tile shapes (kz columns per block of the y and x passes; resident x-pass blocks per SM).
-// Compile-time constants; the defaults are the measured best on the B200.
+// kz columns per y-pass block (the x pass's column count is chosen per grid at run time,
+// see x_cols).
 #ifndef LSB_Y_COLS
 #define LSB_Y_COLS 16
-#endif
-#ifndef LSB_X_COLS_MID
-#define LSB_X_COLS_MID 8
-#endif
-#ifndef LSB_X_MIN_BLOCKS
-#define LSB_X_MIN_BLOCKS 2
 #endif
 constexpr int kYT = LSB_Y_COLS;
 
@@ -114,19 +108,27 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split
 // layout [k1][p][t] with rows of P*T + T values (the padding makes the column reads of
 // the second step conflict-free).
 template <int NX>
-__host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ? 4 : LSB_X_COLS_MID); }
-template <int NX>
-__host__ __device__ constexpr int x_row() { return Split<NX>::P * x_cols<NX>() + x_cols<NX>(); }
-template <int NX>
+__host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ? 4 : 8); }
+// Tile variants of the x pass: 0 = x_cols columns per block (two resident blocks per SM),
+// 1 = half as many (four resident blocks); the solver times both on its first solve and
+// keeps the faster (lsb::fast::launch_xpass `variant`).
+template <int NX, int V>
+__host__ __device__ constexpr int x_cols_v() { return (V == 1 && NX != 256 && NX != 16) ? x_cols<NX>() / 2 : x_cols<NX>(); }
+template <int NX, int V>
+__host__ __device__ constexpr int x_min_blocks() { return x_cols_v<NX, V>() < x_cols<NX>() ? 4 : 2; }
+template <int NX, int T>
+__host__ __device__ constexpr int x_row() { return Split<NX>::P * T + T; }
+template <int NX, int T>
 __host__ __device__ constexpr int x_region() {
-  return Split<NX>::E * x_row<NX>() > NX * x_cols<NX>() ? Split<NX>::E * x_row<NX>() : NX * x_cols<NX>();
+  return Split<NX>::E * x_row<NX, T>() > NX * T ? Split<NX>::E * x_row<NX, T>() : NX * T;
 }
 
-template <int NX>
-__global__ void __launch_bounds__(6 * Split<NX>::P * x_cols<NX>(), LSB_X_MIN_BLOCKS) xpass_fast(
+template <int NX, int V>
+__global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_blocks<NX, V>()) xpass_fast(
     GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
     InstanceState* __restrict__ st, double* __restrict__ partials) {
-  constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols<NX>(), RS = x_row<NX>(), REG = x_region<NX>();
+  constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols_v<NX, V>(), RS = x_row<NX, T>(),
+                REG = x_region<NX, T>();
   constexpr int NJ = rounds<NX>();
   extern __shared__ __align__(16) unsigned char xfraw[];
   float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
@@ -578,17 +580,20 @@ bool supported(const GridDesc& g) {
 }
 
 template <int N>
-static int x_blocks(const GridDesc& g) { return (g.nzh + x_cols<N>() - 1) / x_cols<N>(); }
+static int x_blocks(const GridDesc& g, int v) {
+  const int t = v ? x_cols_v<N, 1>() : x_cols_v<N, 0>();
+  return (g.nzh + t - 1) / t;
+}
 
-int x_tiles(const GridDesc& g) {
+int x_tiles(const GridDesc& g, int variant) {
   switch (g.nx) {
-    case 16: return x_blocks<16>(g);
-    case 32: return x_blocks<32>(g);
-    case 48: return x_blocks<48>(g);
-    case 96: return x_blocks<96>(g);
-    case 64: return x_blocks<64>(g);
-    case 128: return x_blocks<128>(g);
-    default: return x_blocks<256>(g);
+    case 16: return x_blocks<16>(g, variant);
+    case 32: return x_blocks<32>(g, variant);
+    case 48: return x_blocks<48>(g, variant);
+    case 96: return x_blocks<96>(g, variant);
+    case 64: return x_blocks<64>(g, variant);
+    case 128: return x_blocks<128>(g, variant);
+    default: return x_blocks<256>(g, variant);
   }
 }
 
@@ -598,14 +603,18 @@ template <int N>
 static int z_blocks_for(const GridDesc& g) {
   return (int)(((long long)g.nx * g.ny + z_lines<N>() - 1) / z_lines<N>());
 }
-template <int N>
-static size_t xsmem() { return (size_t)6 * x_region<N>() * sizeof(float2); }
+template <int N, int V>
+static size_t xsmem() {
+  return (size_t)6 * x_region<N, x_cols_v<N, V>()>() * sizeof(float2);
+}
 
 template <int N>
 static cudaError_t configure_n() {
   cudaError_t e = cudaFuncSetAttribute(zpass_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(xpass_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N>());
+  e = cudaFuncSetAttribute(xpass_fast<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(xpass_fast<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
 }
 
 cudaError_t configure() {
@@ -681,23 +690,31 @@ void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, cons
   }
 }
 
-template <int N>
+template <int N, int V>
 static void xlaunch(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
                     double* partials, cudaStream_t s) {
-  dim3 grid(x_blocks<N>(g), g.ny, batch);
-  xpass_fast<N><<<grid, 6 * Split<N>::P * x_cols<N>(), xsmem<N>(), s>>>(g, spec, med, st, partials);
+  dim3 grid(x_blocks<N>(g, V), g.ny, batch);
+  xpass_fast<N, V><<<grid, 6 * Split<N>::P * x_cols_v<N, V>(), xsmem<N, V>(), s>>>(g, spec, med, st,
+                                                                                  partials);
 }
 
-void launch_xpass(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
-                  double* partials, cudaStream_t s) {
+template <int N>
+static void xlaunch_v(int variant, const GridDesc& g, int batch, float2* spec, const Medium* med,
+                      InstanceState* st, double* partials, cudaStream_t s) {
+  if (variant) xlaunch<N, 1>(g, batch, spec, med, st, partials, s);
+  else xlaunch<N, 0>(g, batch, spec, med, st, partials, s);
+}
+
+void launch_xpass(const GridDesc& g, int variant, int batch, float2* spec, const Medium* med,
+                  InstanceState* st, double* partials, cudaStream_t s) {
   switch (g.nx) {
-    case 16: xlaunch<16>(g, batch, spec, med, st, partials, s); break;
-    case 32: xlaunch<32>(g, batch, spec, med, st, partials, s); break;
-    case 48: xlaunch<48>(g, batch, spec, med, st, partials, s); break;
-    case 96: xlaunch<96>(g, batch, spec, med, st, partials, s); break;
-    case 64: xlaunch<64>(g, batch, spec, med, st, partials, s); break;
-    case 128: xlaunch<128>(g, batch, spec, med, st, partials, s); break;
-    default: xlaunch<256>(g, batch, spec, med, st, partials, s); break;
+    case 16: xlaunch_v<16>(variant, g, batch, spec, med, st, partials, s); break;
+    case 32: xlaunch_v<32>(variant, g, batch, spec, med, st, partials, s); break;
+    case 48: xlaunch_v<48>(variant, g, batch, spec, med, st, partials, s); break;
+    case 96: xlaunch_v<96>(variant, g, batch, spec, med, st, partials, s); break;
+    case 64: xlaunch_v<64>(variant, g, batch, spec, med, st, partials, s); break;
+    case 128: xlaunch_v<128>(variant, g, batch, spec, med, st, partials, s); break;
+    default: xlaunch_v<256>(variant, g, batch, spec, med, st, partials, s); break;
   }
 }
 

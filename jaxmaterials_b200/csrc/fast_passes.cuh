@@ -6,10 +6,10 @@
 namespace lsb {
 namespace fast {
 
-// True when every extent is one of 16, 32, 64, 128, 256.
+// True when every extent is one of 16, 32, 48, 64, 96, 128, 256.
 bool supported(const GridDesc& g);
-// x-pass blocks per (ky) row: the number of kz tiles.
-int x_tiles(const GridDesc& g);
+// x-pass blocks per (ky) row for tile variant 0 or 1: the number of kz tiles.
+int x_tiles(const GridDesc& g, int variant);
 cudaError_t configure();
 // z-pass blocks per instance (number of Gram-row partials in the Anderson residual mode).
 int z_blocks(const GridDesc& g);
@@ -18,8 +18,8 @@ void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, c
                   InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s);
 void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
                   cudaStream_t s);
-void launch_xpass(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
-                  double* partials, cudaStream_t s);
+void launch_xpass(const GridDesc& g, int variant, int batch, float2* spec, const Medium* med,
+                  InstanceState* st, double* partials, cudaStream_t s);
 
 }  // namespace fast
 }  // namespace lsb

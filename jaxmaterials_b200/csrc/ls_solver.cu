@@ -172,7 +172,7 @@ int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]) {
   s->sh32 = plan_launch(g, sizeof(float2));
   s->sh64 = plan_launch(g, sizeof(double2));
   s->fast32 = fast::supported(g);
-  if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g) * g.ny;
+  if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g, s->xvariant) * g.ny;
   if (!shape_fits(s->sh32) || !shape_fits(s->sh64))
     return fail(-1, "grid %dx%dx%d needs FFT blocks above %d threads", g.nx, g.ny, g.nz, kMaxThreads);
   cudaError_t e = configure_kernels();
@@ -248,7 +248,9 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
     return e == cudaSuccess;
   };
   const size_t B = (size_t)batch;
-  const size_t xblk = (size_t)std::max(s->sh32.x_blocks_per_instance, s->sh64.x_blocks_per_instance);
+  // room for the partials of either x-pass tile variant
+  const size_t xblk = (size_t)std::max({s->sh32.x_blocks_per_instance, s->sh64.x_blocks_per_instance,
+                                        s->fast32 ? fast::x_tiles(g, 1) * g.ny : 0});
   const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
   bool ok = alloc((void**)&s->d_eps32, sizeof(float) * B * 6 * g.nv) &&
             alloc((void**)&s->d_spec32, sizeof(float2) * B * 6 * g.nm) &&
@@ -338,7 +340,8 @@ template <typename T>
 void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
     if (s->fast32) {
-      fast::launch_xpass(s->g, batch, spec, s->d_medium, s->d_state, s->d_partials, s->stream);
+      fast::launch_xpass(s->g, s->xvariant, batch, spec, s->d_medium, s->d_state, s->d_partials,
+                         s->stream);
       return;
     }
   }
@@ -473,6 +476,46 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   }
 }
 
+// Chooses the faster x-pass tile variant of the fast FP32 passes by timing both (three
+// launches each after one warm-up, CUDA events on the solver's stream) on this solver's
+// buffers; the passes only write the spectrum, the partials and the zero mode, all of
+// which the solve recomputes before use. Runs once per solver.
+int tune_xpass(lsb_solver* s, int batch) {
+  s->xtuned = true;
+  if (!s->fast32 || fast::x_tiles(s->g, 0) == fast::x_tiles(s->g, 1)) return 0;
+  cudaStream_t st = s->stream;
+  cudaEvent_t ev[2];
+  LSB_CUDA(cudaEventCreate(&ev[0]));
+  LSB_CUDA(cudaEventCreate(&ev[1]));
+  float best = 0.f;
+  int bestv = 0;
+  for (int v = 0; v < 2; ++v) {
+    fast::launch_xpass(s->g, v, batch, s->d_spec32, s->d_medium, s->d_state, s->d_partials, st);
+    cudaEventRecord(ev[0], st);
+    for (int r = 0; r < 3; ++r)
+      fast::launch_xpass(s->g, v, batch, s->d_spec32, s->d_medium, s->d_state, s->d_partials, st);
+    cudaEventRecord(ev[1], st);
+    cudaError_t e = cudaEventSynchronize(ev[1]);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(ev[0]);
+      cudaEventDestroy(ev[1]);
+      return fail(-2, "x-pass tuning: %s", cudaGetErrorString(e));
+    }
+    if (v == 0 || ms < best) {
+      best = ms;
+      bestv = v;
+    }
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  s->launches += 8;
+  s->xvariant = bestv;
+  s->sh32.x_blocks_per_instance = fast::x_tiles(s->g, bestv) * s->g.ny;
+  return 0;
+}
+
 }  // namespace
 
 namespace lsb {
@@ -505,6 +548,7 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st, s->use_e0ref ? s->d_e0ref : nullptr);
   launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
+  if (!s->xtuned && !fp64_start) LSB_TRY(tune_xpass(s, batch));
   bool any64 = fp64_start;
   if (!fp64_start) {
     LSB_TRY(run_phase<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, d_eps0, 0, sp, true));
@@ -654,6 +698,18 @@ int lsb_set_reference_e0(lsb_solver* solver, int batch, const double* e0) {
   LSB_CUDA(cudaMemcpy(solver->d_e0ref, e0, sizeof(double) * batch, cudaMemcpyHostToDevice));
   solver->use_e0ref = true;
   return 0;
+}
+
+int lsb_tile_variant(lsb_solver* solver, int variant) {
+  if (!solver) return fail(-1, "null solver");
+  if (variant < -1 || variant > 1) return fail(-1, "tile variant %d outside [-1, 1]", variant);
+  if (variant >= 0) {
+    if (!solver->fast32) return solver->xvariant;
+    solver->xvariant = variant;
+    solver->xtuned = true;
+    solver->sh32.x_blocks_per_instance = fast::x_tiles(solver->g, variant) * solver->g.ny;
+  }
+  return solver->xvariant;
 }
 
 int lsb_set_graphs(lsb_solver* solver, int on) {

@@ -20,7 +20,9 @@ struct lsb_solver {
   // instances per (lambda, mu) field pair: 0 = every instance of a solve shares one pair;
   // k > 0 = instance b uses structure b / k of [structure][nv] Lame arrays
   int lame_group = 0;
-  bool fast32 = false;   // FP32 passes with compile-time power-of-two lengths
+  bool fast32 = false;   // FP32 passes with compile-time lengths (fast_passes.cu)
+  int xvariant = 0;      // x-pass tile variant of the fast passes (chosen by timing)
+  bool xtuned = false;   // xvariant has been chosen
   GridDesc g{};
   LaunchShape sh32{}, sh64{};
   cudaStream_t stream = nullptr;

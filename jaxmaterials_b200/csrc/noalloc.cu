@@ -90,6 +90,7 @@ extern "C" int lsb_solve_noalloc(const int voxels[3], const double extents[3], i
   lsb_solver s;           // points into the scratch array; frees nothing when it goes away
   s.owns_memory = false;
   s.use_graphs = false;  // graph instantiation allocates
+  s.xtuned = true;       // default x-pass tiles (the partials below are sized for them)
   s.device = dev;
   s.batch_cap = batch;
   s.depth = 0;

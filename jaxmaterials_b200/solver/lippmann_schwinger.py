@@ -136,6 +136,12 @@ class Solver:
                    "lsb_set_precision")
         self.precision = precision
 
+    def tile_variant(self, variant=None):
+        """x-pass tile variant in use (chosen by timing on the first FP32 solve); an
+        argument 0 or 1 fixes it."""
+        return _lib.check(self._lib.lsb_tile_variant(self._h, -1 if variant is None else int(variant)),
+                          "lsb_tile_variant")
+
     def set_graphs(self, on=True):
         """Replay each iteration as a CUDA graph (default) or launch kernel by kernel."""
         _lib.check(self._lib.lsb_set_graphs(self._h, 1 if on else 0), "lsb_set_graphs")

@@ -447,3 +447,26 @@ def test_fp32_gradient_matches_fp64(ls):
     for a, b in ((lm32.grad, lm64.grad), (mu32.grad, mu64.grad)):
         a, b = a.double(), b
         assert float((a - b).norm() / b.norm()) < 1e-4
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 48), (96, 16, 32)])
+def test_x_tile_variants_agree(ls, n):
+    """Both x-pass tile variants give the same fields (bit for bit: the same arithmetic
+    per column), and the automatic choice is one of them."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import Solver
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    out = []
+    for v in (0, 1):
+        s = Solver(g, batch=1)
+        assert s.tile_variant(v) == v
+        r = s.solve(lm, mu, EPS_BAR, rtol=1e-20, atol=1e-5, maxiter=12, want_sigma=False)
+        out.append((r.epsilon.clone(), r.iters.copy()))
+        s.close()
+    assert torch.equal(out[0][0], out[1][0]) and (out[0][1] == out[1][1]).all()
+    s = Solver(g, batch=1)
+    s.solve(lm, mu, EPS_BAR, rtol=1e-20, atol=1e-5, maxiter=2, want_sigma=False)
+    assert s.tile_variant() in (0, 1)
