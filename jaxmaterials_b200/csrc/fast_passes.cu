@@ -55,7 +55,10 @@ __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restric
 }
 
 // ----------------------------------------------------------------------------- y pass
-// Block = (16 kz columns, x, instance * 6 + component); thread (p, t), t fastest.
+// Block = (16 kz columns, x, instance * 6 + component); thread (p, t), t fastest. When
+// nz/2+1 = 16 k + 1 (every even extent here but 16 and 48), the last column (the z
+// Nyquist plane) is not given a 16-column tile of its own per x: tile k instead takes that
+// column for 16 consecutive x.
 // kz columns per y-pass block (the x pass's column count is chosen per grid at run time,
 // see x_cols).
 #ifndef LSB_Y_COLS
@@ -73,9 +76,19 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split
   if (!active32(st[bc / 6])) return;
   const int t = threadIdx.x % kYT, p = threadIdx.x / kYT;
   const int nzh = g.nzh;
-  const int kz = blockIdx.x * kYT + t;
-  const bool valid = kz < nzh;
-  float2* base = spec + ((size_t)bc * g.nx + blockIdx.y) * (size_t)NY * nzh + kz;
+  int kz, x;
+  bool valid;
+  if (nzh % kYT == 1 && (int)blockIdx.x == nzh / kYT) {
+    if ((int)blockIdx.y * kYT >= g.nx) return;
+    kz = nzh - 1;
+    x = blockIdx.y * kYT + t;
+    valid = x < g.nx;
+  } else {
+    kz = blockIdx.x * kYT + t;
+    x = blockIdx.y;
+    valid = kz < nzh;
+  }
+  float2* base = spec + ((size_t)bc * g.nx + x) * (size_t)NY * nzh + kz;
   const float2* tw = g.py.tw;
   float2 v[E];
 #pragma unroll
@@ -138,10 +151,19 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
   if (!active32(st[b])) return;
   const int tid = threadIdx.x;
   const int t = tid % T, p = (tid / T) % P, c = tid / (T * P);
-  const int ky = blockIdx.y;
-  const int kz0 = blockIdx.x * T;
-  const int kz = kz0 + t;
   const int nzh = g.nzh;
+  // With nz/2+1 = T k + 1 the last tile takes the z Nyquist column for T consecutive ky
+  // instead of one column per ky (as the y pass); its surplus blocks only report a zero
+  // partial.
+  const bool tail = nzh % T == 1 && (int)blockIdx.x == nzh / T;
+  if (tail && (int)blockIdx.y * T >= g.ny) {
+    if (tid == 0) partials[(size_t)b * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = 0.0;
+    return;
+  }
+  auto col_ky = [&](int tt) { return tail ? (int)blockIdx.y * T + tt : (int)blockIdx.y; };
+  auto col_kz = [&](int tt) { return tail ? nzh - 1 : (int)blockIdx.x * T + tt; };
+  const int ky = col_ky(t);
+  const int kz = col_kz(t);
   const bool valid = kz < nzh;
   const size_t xstride = (size_t)g.ny * nzh;
   float2* gcol = spec + (size_t)b * 6 * g.nm + (size_t)c * g.nm + (size_t)ky * nzh + kz;
@@ -151,10 +173,11 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
   if (tid < T) {
     // tilde(xi)_d = (2 n_d / L_d) * sin/cos products (fourier.py:9-58); the ky and kz
     // factors of this block's columns, FP64
-    const int kzz = kz0 + tid < nzh ? kz0 + tid : 0;
-    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[ky] * g.cz[kzz];
-    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[ky] * g.cz[kzz];
-    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[ky] * g.sz[kzz];
+    const int kzz = col_kz(tid) < nzh ? col_kz(tid) : 0;
+    const int kyy = col_ky(tid);
+    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
+    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
+    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
   }
 
   // forward: load, step A, transpose
@@ -191,7 +214,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
   double acc = 0.0;
   for (int idx = tid; idx < NX * T; idx += blockDim.x) {
     const int kx = idx / T, tt = idx % T;
-    const int kzz = kz0 + tt;
+    const int kzz = col_kz(tt);
     if (kzz >= nzh) continue;
     float2 s[6];
 #pragma unroll
@@ -209,7 +232,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
                   (double)d1.y * d1.y + (double)d2.x * d2.x + (double)d2.y * d2.y;
       acc += ((kzz == 0 || 2 * kzz == g.nz) ? 1.0 : 2.0) * m2;
     }
-    if (kx == 0 && ky == 0 && kzz == 0) {
+    if (kx == 0 && col_ky(tt) == 0 && kzz == 0) {
 #pragma unroll
       for (int cc = 0; cc < 6; ++cc) {
         st[b].sig0[2 * cc] = (double)s[cc].x + (double)g.nv * st[b].shift[cc];
@@ -673,7 +696,8 @@ int z_blocks(const GridDesc& g) {
 template <int N>
 static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
                     cudaStream_t s) {
-  dim3 grid((g.nzh + kYT - 1) / kYT, g.nx, 6 * batch);
+  // with a one-column tail, full tiles + one tail tile (see ypass_fast)
+  dim3 grid(g.nzh % kYT == 1 ? g.nzh / kYT + 1 : (g.nzh + kYT - 1) / kYT, g.nx, 6 * batch);
   ypass_fast<N><<<grid, kYT * Split<N>::P, 0, s>>>(g, inverse ? 1 : 0, spec, st);
 }
 

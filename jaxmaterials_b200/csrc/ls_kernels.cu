@@ -683,21 +683,32 @@ __global__ void minmax_partial_kernel(long long nv, const TL* __restrict__ lambd
   }
 }
 
-// One block per structure: Medium med[structure] from its nblk partials.
+// One warp per structure: Medium med[structure] from its nblk partials (lane-strided
+// partial sums, then a fixed xor tree: deterministic).
 __global__ void minmax_final_kernel(int nblk, long long nv, int fp64_fields,
                                     const double* __restrict__ scratch, Medium* med) {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x;
   scratch += (size_t)blockIdx.x * nblk * 6;
   med += blockIdx.x;
   double lmin = DBL_MAX, lmax = -DBL_MAX, mmin = DBL_MAX, mmax = -DBL_MAX;
   double lsum = 0.0, msum = 0.0;
-  for (int i = 0; i < nblk; ++i) {
+  for (int i = lane; i < nblk; i += 32) {
     const double* o = scratch + 6 * i;
     lmin = fmin(lmin, o[0]); lmax = fmax(lmax, o[1]);
     mmin = fmin(mmin, o[2]); mmax = fmax(mmax, o[3]);
     lsum += o[4];
     msum += o[5];
   }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, off));
+    lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
+    mmin = fmin(mmin, __shfl_xor_sync(0xffffffffu, mmin, off));
+    mmax = fmax(mmax, __shfl_xor_sync(0xffffffffu, mmax, off));
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
+    msum += __shfl_xor_sync(0xffffffffu, msum, off);
+  }
+  if (lane != 0) return;
   Medium m;
   m.lmin = lmin; m.lmax = lmax; m.mmin = mmin; m.mmax = mmax;
   m.lmean = lsum / (double)nv;
