@@ -125,8 +125,13 @@ __host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ?
 // Tile variants of the x pass: 0 = x_cols columns per block (two resident blocks per SM),
 // 1 = half as many (four resident blocks); the solver times both on its first solve and
 // keeps the faster (lsb::fast::launch_xpass `variant`).
+// (variant 1 only where its block is still whole warps: the block reduction shuffles
+// over full warps)
 template <int NX, int V>
-__host__ __device__ constexpr int x_cols_v() { return (V == 1 && NX != 256 && NX != 16) ? x_cols<NX>() / 2 : x_cols<NX>(); }
+__host__ __device__ constexpr int x_cols_v() {
+  return (V == 1 && NX != 256 && NX != 16 && (6 * Split<NX>::P * (x_cols<NX>() / 2)) % 32 == 0)
+             ? x_cols<NX>() / 2 : x_cols<NX>();
+}
 template <int NX, int V>
 __host__ __device__ constexpr int x_min_blocks() { return x_cols_v<NX, V>() < x_cols<NX>() ? 4 : 2; }
 template <int NX, int T>
@@ -142,6 +147,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
     InstanceState* __restrict__ st, double* __restrict__ partials) {
   constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols_v<NX, V>(), RS = x_row<NX, T>(),
                 REG = x_region<NX, T>();
+  static_assert((6 * P * T) % 32 == 0, "the x pass reduces over whole warps");
   constexpr int NJ = rounds<NX>();
   extern __shared__ __align__(16) unsigned char xfraw[];
   float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
@@ -311,12 +317,19 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
 // Block = L (x, y) lines = 3L complex pair lines; thread (line q, p), p fastest.
 // The block's inputs (spectrum rows, strain rows, lambda/mu rows) are contiguous chunks;
 // one thread issues them as TMA bulk copies into shared memory (completion on an
-// mbarrier), so all of a block's loads are in flight at once and two resident blocks per
-// SM overlap one block's loads with the other's transforms.
+// mbarrier), so all of a block's loads are in flight at once, and the resident blocks of
+// an SM overlap one block's loads with the others' transforms.
 template <int NZ>
 __host__ __device__ constexpr int z_lines() {
-  return Split<NZ>::P == 3 ? 16 : (Split<NZ>::P == 6 ? 8 : 192 / (3 * Split<NZ>::P));
+  // 96 threads (72 for P = 3, 6): small blocks, four or more resident per SM, so that the
+  // TMA loads of some blocks overlap the transforms of others (measured: -14% at 128^3
+  // against 192-thread blocks)
+  return Split<NZ>::P == 3 ? 8 : (Split<NZ>::P == 6 ? 4 : 96 / (3 * Split<NZ>::P));
 }
+template <int NZ>
+__host__ __device__ constexpr int z_threads() { return 3 * z_lines<NZ>() * Split<NZ>::P; }
+template <int NZ>
+__host__ __device__ constexpr int z_min_blocks() { return z_threads<NZ>() > 192 ? 1 : 384 / z_threads<NZ>() > 2 ? 384 / z_threads<NZ>() : 2; }
 // Line pitch of the transform buffer: room for the padded transposed layout
 // k1 * (P + 1) + p (conflict-free column reads), and = 8 (mod 16) so that the two lines
 // of a half-warp fall in disjoint banks.
@@ -402,7 +415,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // bulk: the block's global chunks are 16-byte aligned (TMA bulk copies); otherwise the
 // staging buffers are filled by ordinary loads.
 template <int NZ>
-__global__ void __launch_bounds__(192, 2) zpass_fast(
+__global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fast(
     GridDesc g, int mode, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
     const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med,
@@ -660,7 +673,7 @@ static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda,
   dim3 grid((unsigned)z_blocks_for<N>(g), batch);
   // every chunk offset is a multiple of 16 bytes when the base pointers are
   const int bulk = aligned16(lambda) && aligned16(mu) && aligned16(eps) && aligned16(spec) ? 1 : 0;
-  zpass_fast<N><<<grid, 3 * z_lines<N>() * Split<N>::P, zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec, eps_bar, eps0,
+  zpass_fast<N><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec, eps_bar, eps0,
                                               st, med, aa);
 }
 
