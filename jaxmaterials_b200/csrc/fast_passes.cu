@@ -44,9 +44,8 @@ __device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y
 __device__ __forceinline__ bool active32(const InstanceState& s) { return !s.done && s.phase == 0; }
 
 // Step A of the four-step transform: DFT over e of v[e] = x[p + P e], then the twiddle.
-template <int N>
+template <int N, int E = Split<N>::E>
 __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restrict__ tw) {
-  constexpr int E = Split<N>::E;
   Bfly<E>::run(v);
   if (p > 0) {
 #pragma unroll
@@ -66,11 +65,26 @@ __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restric
 #endif
 constexpr int kYT = LSB_Y_COLS;
 
+// Split of the y transform (may differ from the x/z split): 128 = 8 x 16 puts 16 threads
+// on a column and halves the values each thread holds (measured -13% at 128^3 against
+// 16 x 8; the shorter extents are fastest with their x/z split).
+template <int N>
+struct YSplit { static constexpr int E = Split<N>::E, P = Split<N>::P; };
+template <>
+struct YSplit<128> { static constexpr int E = 8, P = 16; };
+template <int N>
+__host__ __device__ constexpr int y_threads() { return kYT * YSplit<N>::P; }
+template <int N>
+__host__ __device__ constexpr int y_min_blocks() {
+  // (256: three blocks, so that its 16 values per thread fit without spilling)
+  return N == 256 ? 3 : 1024 / (32 * ((y_threads<N>() + 31) / 32));
+}
+
 template <int NY>
-__global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split<NY>::P + 31) / 32))) ypass_fast(GridDesc g, int inverse,
+__global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fast(GridDesc g, int inverse,
                                                                float2* __restrict__ spec,
                                                                const InstanceState* __restrict__ st) {
-  constexpr int E = Split<NY>::E, P = Split<NY>::P, NJ = rounds<NY>();
+  constexpr int E = YSplit<NY>::E, P = YSplit<NY>::P, NJ = (E + P - 1) / P;
   __shared__ float2 buf[NY * kYT];
   const int bc = blockIdx.z;
   if (!active32(st[bc / 6])) return;
@@ -96,7 +110,7 @@ __global__ void __launch_bounds__(kYT * Split<NY>::P, 1024 / (32 * ((kYT * Split
     float2 a = valid ? base[(size_t)(p + P * e) * nzh] : make_float2(0.f, 0.f);
     v[e] = inverse ? conj2(a) : a;
   }
-  step_a<NY>(v, p, tw);
+  step_a<NY, E>(v, p, tw);
 #pragma unroll
   for (int k1 = 0; k1 < E; ++k1) buf[(k1 * P + p) * kYT + t] = v[k1];
   __syncthreads();
@@ -711,7 +725,7 @@ static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, co
                     cudaStream_t s) {
   // with a one-column tail, full tiles + one tail tile (see ypass_fast)
   dim3 grid(g.nzh % kYT == 1 ? g.nzh / kYT + 1 : (g.nzh + kYT - 1) / kYT, g.nx, 6 * batch);
-  ypass_fast<N><<<grid, kYT * Split<N>::P, 0, s>>>(g, inverse ? 1 : 0, spec, st);
+  ypass_fast<N><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, st);
 }
 
 void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
