@@ -136,6 +136,9 @@ __global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fas
 // the second step conflict-free).
 template <int NX>
 __host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ? 4 : 8); }
+// Split of the x transform (may differ from the z split).
+template <int N>
+struct XSplit { static constexpr int E = Split<N>::E, P = Split<N>::P; };
 // Tile variants of the x pass: 0 = x_cols columns per block (two resident blocks per SM),
 // 1 = half as many (four resident blocks); the solver times both on its first solve and
 // keeps the faster (lsb::fast::launch_xpass `variant`).
@@ -143,26 +146,26 @@ __host__ __device__ constexpr int x_cols() { return NX <= 48 ? 16 : (NX == 256 ?
 // over full warps)
 template <int NX, int V>
 __host__ __device__ constexpr int x_cols_v() {
-  return (V == 1 && NX != 256 && NX != 16 && (6 * Split<NX>::P * (x_cols<NX>() / 2)) % 32 == 0)
+  return (V == 1 && NX != 256 && NX != 16 && (6 * XSplit<NX>::P * (x_cols<NX>() / 2)) % 32 == 0)
              ? x_cols<NX>() / 2 : x_cols<NX>();
 }
 template <int NX, int V>
 __host__ __device__ constexpr int x_min_blocks() { return x_cols_v<NX, V>() < x_cols<NX>() ? 4 : 2; }
 template <int NX, int T>
-__host__ __device__ constexpr int x_row() { return Split<NX>::P * T + T; }
+__host__ __device__ constexpr int x_row() { return XSplit<NX>::P * T + T; }
 template <int NX, int T>
 __host__ __device__ constexpr int x_region() {
-  return Split<NX>::E * x_row<NX, T>() > NX * T ? Split<NX>::E * x_row<NX, T>() : NX * T;
+  return XSplit<NX>::E * x_row<NX, T>() > NX * T ? XSplit<NX>::E * x_row<NX, T>() : NX * T;
 }
 
 template <int NX, int V>
-__global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_blocks<NX, V>()) xpass_fast(
+__global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_blocks<NX, V>()) xpass_fast(
     GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
     InstanceState* __restrict__ st, double* __restrict__ partials) {
-  constexpr int E = Split<NX>::E, P = Split<NX>::P, T = x_cols_v<NX, V>(), RS = x_row<NX, T>(),
+  constexpr int E = XSplit<NX>::E, P = XSplit<NX>::P, T = x_cols_v<NX, V>(), RS = x_row<NX, T>(),
                 REG = x_region<NX, T>();
   static_assert((6 * P * T) % 32 == 0, "the x pass reduces over whole warps");
-  constexpr int NJ = rounds<NX>();
+  constexpr int NJ = (E + P - 1) / P;
   extern __shared__ __align__(16) unsigned char xfraw[];
   float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
   __shared__ double red[32];
@@ -204,7 +207,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
   float2 v[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = valid ? gcol[(size_t)(p + P * e) * xstride] : make_float2(0.f, 0.f);
-  step_a<NX>(v, p, tw);
+  step_a<NX, E>(v, p, tw);
 #pragma unroll
   for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
   __syncthreads();
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(6 * Split<NX>::P * x_cols_v<NX, V>(), x_min_bl
   // inverse (forward transform of the conjugate): step A from the natural layout
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = tr[(p + P * e) * T + t];
-  step_a<NX>(v, p, tw);
+  step_a<NX, E>(v, p, tw);
   __syncthreads();
 #pragma unroll
   for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
@@ -343,7 +346,9 @@ __host__ __device__ constexpr int z_lines() {
 template <int NZ>
 __host__ __device__ constexpr int z_threads() { return 3 * z_lines<NZ>() * Split<NZ>::P; }
 template <int NZ>
-__host__ __device__ constexpr int z_min_blocks() { return z_threads<NZ>() > 192 ? 1 : 384 / z_threads<NZ>() > 2 ? 384 / z_threads<NZ>() : 2; }
+__host__ __device__ constexpr int z_min_blocks() {
+  return z_threads<NZ>() > 192 ? 1 : (384 / z_threads<NZ>() > 2 ? 384 / z_threads<NZ>() : 2);
+}
 // Line pitch of the transform buffer: room for the padded transposed layout
 // k1 * (P + 1) + p (conflict-free column reads), and = 8 (mod 16) so that the two lines
 // of a half-warp fall in disjoint banks.
@@ -745,7 +750,7 @@ template <int N, int V>
 static void xlaunch(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
                     double* partials, cudaStream_t s) {
   dim3 grid(x_blocks<N>(g, V), g.ny, batch);
-  xpass_fast<N, V><<<grid, 6 * Split<N>::P * x_cols_v<N, V>(), xsmem<N, V>(), s>>>(g, spec, med, st,
+  xpass_fast<N, V><<<grid, 6 * XSplit<N>::P * x_cols_v<N, V>(), xsmem<N, V>(), s>>>(g, spec, med, st,
                                                                                   partials);
 }
 
