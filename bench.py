@@ -138,6 +138,18 @@ def fixture_iters(depth):
     return None
 
 
+def fixture_c_eff(depth):
+    """FP64 oracle C_eff of the seed-0 benchmark structure (tests/golden/bench_c2_128.npz,
+    made by tests/golden/make_bench_fixture.py), or None."""
+    path = os.path.join(ROOT, "tests", "golden", f"bench_{WORKLOAD}.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        key = f"ceff_d{depth}"
+        if key in d:
+            return np.asarray(d[key], dtype=np.float64)
+    return None
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -437,6 +449,10 @@ def own_arm(args):
             dist.all_reduce(sec, op=dist.ReduceOp.MAX)
             batched["anderson"]["value"] = 6 * args.batched * world / float(sec.item())
 
+    ref = fixture_c_eff(args.depth if args.depth in (0, 5) else 5)
+    c_eff_err = (float(np.linalg.norm(c_eff - ref) / np.linalg.norm(ref))
+                 if ref is not None and rank == 0 else None)
+
     if rank == 0:
         out = {
             "metric": METRIC,
@@ -458,6 +474,7 @@ def own_arm(args):
             "plain": plain,
             "batched": batched,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
+            "c_eff_rel_err_vs_fp64": c_eff_err,
             "gpu_launches": int(launches),
             "roofline": {
                 "bound": "hbm",
