@@ -470,3 +470,27 @@ def test_x_tile_variants_agree(ls, n):
     s = Solver(g, batch=1)
     s.solve(lm, mu, EPS_BAR, rtol=1e-20, atol=1e-5, maxiter=2, want_sigma=False)
     assert s.tile_variant() in (0, 1)
+
+
+@pytest.mark.parametrize("depth", [0, 3])
+def test_graph_replay_bit_identical(ls, depth):
+    """Iterations replayed from a CUDA graph and launched kernel by kernel give the same
+    bits (same kernels, same order)."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import Solver
+
+    n = (32, 32, 16)
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    eb = np.tile(EPS_BAR, (2, 1))
+    out = []
+    for graphs in (True, False):
+        s = Solver(g, batch=2, depth=depth)
+        s.tile_variant(0)
+        s.set_graphs(graphs)
+        r = s.solve(lm, mu, eb, rtol=1e-6, maxiter=200)
+        out.append((r.epsilon.clone(), r.sigma.clone(), r.iters.copy(), r.mean_sigma.copy()))
+        s.close()
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    assert (out[0][2] == out[1][2]).all() and (out[0][3] == out[1][3]).all()
