@@ -92,6 +92,14 @@ int lsb_set_precision(lsb_solver *solver, int precision, int stall_window);
  * same absolute residual as the cold solve. e0 = NULL clears it. */
 int lsb_set_reference_e0(lsb_solver *solver, int batch, const double *e0);
 
+/* No reference counterpart. on != 0 (Anderson depth >= 1 only): the warm start d_eps0 of
+ * later solves does not start the iteration; the iteration starts from eps_bar, and its
+ * first update sets eps = d_eps0, so that the cold start's and the warm start's residuals
+ * are both in the Anderson history and the mixing weighs them (a poor warm start then
+ * costs about one update instead of slowing the solve). The criterion e0 is the cold
+ * start's. d_eps0 must be eps_bar plus a compatible field (see lsb_solve). */
+int lsb_set_warm_history(lsb_solver *solver, int on);
+
 /* No reference counterpart. Tile variant of the FP32 x pass (extents 32-128: 0 = the
  * wide tile, 1 = half as many kz columns per block with twice the resident blocks). By
  * default the solver times both on its first FP32 solve and keeps the faster. variant =

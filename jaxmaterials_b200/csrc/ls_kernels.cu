@@ -533,6 +533,7 @@ __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int
                                                                const InstanceState* __restrict__ st,
                                                                const T* __restrict__ g,
                                                                const double* __restrict__ alpha,
+                                                               const T* __restrict__ inject,
                                                                T* __restrict__ eps) {
   const int b = blockIdx.y;
   const InstanceState& s = st[b];
@@ -545,6 +546,15 @@ __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int
 #pragma unroll
   for (int q = 0; q < M1; ++q) a[q] = q < filled ? (T)al[q] : (T)0;
   T* eb = eps + (size_t)b * n6;
+  if (inject && s.iter == 1 && s.aa_base == 0) {
+    // first update with a warm start in the history: the next iterate is the given field,
+    // whose residual then enters the ring beside the cold start's
+    const T* ib = inject + (size_t)b * n6;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n6;
+         i += (long long)gridDim.x * blockDim.x)
+      eb[i] = ib[i];
+    return;
+  }
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n6;
        i += (long long)gridDim.x * blockDim.x) {
     T gv[M1];
@@ -909,12 +919,13 @@ void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batc
 
 template <typename T>
 void launch_anderson_combine(long long nv, int depth, int phase, int batch, const InstanceState* st,
-                             const T* g, const double* alpha, T* eps, cudaStream_t stream) {
+                             const T* g, const double* alpha, T* eps, cudaStream_t stream,
+                             const T* inject) {
   const long long n6 = 6 * nv;
   const dim3 grid((unsigned)std::min<long long>(2048, (n6 + 255) / 256), batch);
   switch (depth + 1) {
 #define LSB_COMB(M) \
-    case M: anderson_combine_kernel<T, M><<<grid, 256, 0, stream>>>(n6, phase, st, g, alpha, eps); break;
+    case M: anderson_combine_kernel<T, M><<<grid, 256, 0, stream>>>(n6, phase, st, g, alpha, inject, eps); break;
     LSB_COMB(2) LSB_COMB(3) LSB_COMB(4) LSB_COMB(5) LSB_COMB(6) LSB_COMB(7) LSB_COMB(8) LSB_COMB(9)
 #undef LSB_COMB
     default: break;
@@ -995,7 +1006,7 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
   template void launch_anderson_gram<T>(long long, int, int, int, int, const InstanceState*,    \
                                         const T*, double*, cudaStream_t);                       \
   template void launch_anderson_combine<T>(long long, int, int, int, const InstanceState*,      \
-                                           const T*, const double*, T*, cudaStream_t);
+                                           const T*, const double*, T*, cudaStream_t, const T*);
 LSB_INST(float)
 LSB_INST(double)
 #undef LSB_INST

@@ -39,10 +39,12 @@ void launch_zpass(const GridDesc& g, const LaunchShape& ls, int mode, int batch,
 template <typename T>
 void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batch,
                           const InstanceState* st, const T* r, double* partials, cudaStream_t s);
-// eps = sum_s alpha_s g_s for every instance in `phase` (g: [batch][depth+1][6][nv]).
+// eps = sum_s alpha_s g_s for every instance in `phase` (g: [batch][depth+1][6][nv]);
+// with `inject` ([batch][6][nv]) the first update of a solve sets eps = inject instead.
 template <typename T>
 void launch_anderson_combine(long long nv, int depth, int phase, int batch, const InstanceState* st,
-                             const T* g, const double* alpha, T* eps, cudaStream_t s);
+                             const T* g, const double* alpha, T* eps, cudaStream_t s,
+                             const T* inject = nullptr);
 // Anderson coefficients of every instance in `phase` from the Gram-row partials.
 void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
                            const double* partials, double* amat, double* alpha, cudaStream_t s);

@@ -416,7 +416,8 @@ struct GraphPhase {
 // One iteration is captured into a CUDA graph and replayed (s->use_graphs).
 template <typename T>
 int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
-              const T* eps0, int init_mode, const SolveParams& sp, bool anderson) {
+              const T* eps0, int init_mode, const SolveParams& sp, bool anderson,
+              const T* inject = nullptr) {
   const LaunchShape& sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
   const int phase = sizeof(T) == 8 ? 1 : 0;
   GraphPhase gp(s);
@@ -442,7 +443,7 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
       launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
                             s->d_aa_mat, s->d_aa_alpha, st);
       launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g,
-                                 s->d_aa_alpha, eps, st);
+                                 s->d_aa_alpha, eps, st, inject);
       pass_z<T>(s, 2, batch, lam, mu, eps, spec, nullptr, aa);
     } else {
       pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
@@ -551,7 +552,11 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   if (!s->xtuned && !fp64_start) LSB_TRY(tune_xpass(s, batch));
   bool any64 = fp64_start;
   if (!fp64_start) {
-    LSB_TRY(run_phase<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, d_eps0, 0, sp, true));
+    // a warm start either starts the iteration or (warm_history) enters the Anderson
+    // history as the second iterate, after the cold start's
+    const bool hist = s->warm_history && d_eps0 && s->depth > 0;
+    LSB_TRY(run_phase<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, hist ? nullptr : d_eps0,
+                             0, sp, true, hist ? d_eps0 : nullptr));
     for (int b = 0; b < batch; ++b) any64 = any64 || (s->h_state[b].phase == 1 && !s->h_state[b].done);
   }
   if (any64) {
@@ -622,7 +627,9 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   launch_medium<double>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
   LSB_TRY(ensure_fp64_rings(s));
-  LSB_TRY(run_phase<double>(s, batch, d_lambda, d_mu, d_eps, s->d_spec64, d_eps0, 0, sp, true));
+  const bool hist = s->warm_history && d_eps0 && s->depth > 0;
+  LSB_TRY(run_phase<double>(s, batch, d_lambda, d_mu, d_eps, s->d_spec64, hist ? nullptr : d_eps0,
+                            0, sp, true, hist ? d_eps0 : nullptr));
   launch_stress<double, double>(g, 1, batch, s->d_state, d_lambda, d_mu, d_eps, d_sigma,
                                 s->d_mean_scratch, s->d_mean, st);
   s->launches += 2;
@@ -710,6 +717,13 @@ int lsb_tile_variant(lsb_solver* solver, int variant) {
     solver->sh32.x_blocks_per_instance = fast::x_tiles(solver->g, variant) * solver->g.ny;
   }
   return solver->xvariant;
+}
+
+int lsb_set_warm_history(lsb_solver* solver, int on) {
+  if (!solver) return fail(-1, "null solver");
+  if (on && solver->depth == 0) return fail(-1, "a warm start in the Anderson history needs depth >= 1");
+  solver->warm_history = on != 0;
+  return 0;
 }
 
 int lsb_set_graphs(lsb_solver* solver, int on) {

@@ -23,6 +23,7 @@ struct lsb_solver {
   bool fast32 = false;   // FP32 passes with compile-time lengths (fast_passes.cu)
   int xvariant = 0;      // x-pass tile variant of the fast passes (chosen by timing)
   bool xtuned = false;   // xvariant has been chosen
+  bool warm_history = false;  // d_eps0 enters the Anderson history instead of starting it
   GridDesc g{};
   LaunchShape sh32{}, sh64{};
   cudaStream_t stream = nullptr;

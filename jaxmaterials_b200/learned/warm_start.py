@@ -6,9 +6,11 @@ library for the six unit loads (Anderson, tol 1e-6). Inputs are kept on the devi
 phase indicators (uint8), targets as BF16 strain fluctuations eps - e_k [36][nv].
 
 Evaluation: for held-out structures, the cold solve starts from eps = e_k; the warm
-solve starts from the compatible part of the network's prediction (and the scaled warm
-solve from e_k + theta (prediction - e_k), theta minimising the start's residual) (the iteration keeps
-any incompatible part of its start, see Solver.project_compatible) and stops at the same absolute residual as
+solve starts from the compatible part of the network's prediction (the iteration keeps
+any incompatible part of its start, see Solver.project_compatible), the scaled warm solve
+from e_k + theta (prediction - e_k) with theta minimising the start's residual, and the
+history solve from e_k with the prediction as the second Anderson iterate
+(Solver.set_warm_history). The warm and scaled solves stop at the same absolute residual as
 the cold one (its threshold is rtol times the cold start's first criterion, obtained
 from a maxiter = 0 solve and passed as the reference criterion). Reported: iterations of
 both, wall time of both (the warm time includes inference and the extra criterion
@@ -163,9 +165,9 @@ def evaluate(net, ind, depth=5, rtol=1e-6, chunk=16, maxiter=5000):
     chunk = min(chunk, count)
     s = Solver(g, batch=6 * chunk, depth=depth)
     eye6 = np.eye(6, dtype=np.float32)
-    out = {"cold_iters": [], "warm_iters": [], "scaled_iters": [], "theta": [], "c_eff": [],
-           "c_eff_warm": [], "c_eff_scaled": [], "c_eff_net": [], "cold_s": 0.0, "warm_s": 0.0,
-           "scaled_s": 0.0, "inference_s": 0.0}
+    out = {"cold_iters": [], "warm_iters": [], "scaled_iters": [], "hist_iters": [], "theta": [],
+           "c_eff": [], "c_eff_warm": [], "c_eff_scaled": [], "c_eff_hist": [], "c_eff_net": [],
+           "cold_s": 0.0, "warm_s": 0.0, "scaled_s": 0.0, "hist_s": 0.0, "inference_s": 0.0}
     for c0 in range(0, count, chunk):
         c = min(chunk, count - c0)
         lm, mu = lame_from_indicator(ind[c0:c0 + c])
@@ -191,6 +193,15 @@ def evaluate(net, ind, depth=5, rtol=1e-6, chunk=16, maxiter=5000):
                          epsilon0=start, e0_ref=e0s)
         torch.cuda.synchronize()
         t4 = time.perf_counter()
+        # the prediction as the second entry of the Anderson history (after the cold start)
+        s.set_warm_history(True)
+        hist = s.solve(lm, mu, eb, rtol=rtol, maxiter=maxiter, want_sigma=False, epsilon0=eps0)
+        s.set_warm_history(False)
+        torch.cuda.synchronize()
+        t5 = time.perf_counter()
+        out["hist_s"] += (t2b - t1) + (t5 - t4)
+        out["hist_iters"].append(hist.iters.reshape(c, 6))
+        out["c_eff_hist"].append(hist.mean_sigma.reshape(c, 6, 6))
         out["cold_s"] += t1 - t0
         out["warm_s"] += t3 - t1
         out["scaled_s"] += (t2b - t1) + (t4 - t3)
@@ -213,8 +224,8 @@ def evaluate(net, ind, depth=5, rtol=1e-6, chunk=16, maxiter=5000):
         out["c_eff_net"].append(sig.mean(dim=(-3, -2, -1)).cpu().numpy())
         del eps0, e, sig
     s.close()
-    for k in ("cold_iters", "warm_iters", "scaled_iters", "theta", "c_eff", "c_eff_warm",
-              "c_eff_scaled", "c_eff_net"):
+    for k in ("cold_iters", "warm_iters", "scaled_iters", "hist_iters", "theta", "c_eff",
+              "c_eff_warm", "c_eff_scaled", "c_eff_hist", "c_eff_net"):
         out[k] = np.concatenate(out[k])
     return out
 
@@ -240,6 +251,10 @@ def summarise(ev, n):
         "scaled_iterations_saved": float(1.0 - ev["scaled_iters"].mean() / ev["cold_iters"].mean()),
         "scaled_solves_per_s": solves / ev["scaled_s"],
         "theta_mean": float(ev["theta"].mean()),
+        "history_iters_per_solve": float(ev["hist_iters"].mean()),
+        "history_iterations_saved": float(1.0 - ev["hist_iters"].mean() / ev["cold_iters"].mean()),
+        "history_solves_per_s": solves / ev["hist_s"],
+        "c_eff_history_vs_cold_rel_max": float(rel(ev["c_eff_hist"], c).max()),
         "c_eff_warm_vs_cold_rel_max": float(max(rel(cw, c).max(), rel(ev["c_eff_scaled"], c).max())),
         "c_eff_network_rel_mean": float(rel(cn, c).mean()),
         "c_eff_network_rel_max": float(rel(cn, c).max()),

@@ -142,6 +142,12 @@ class Solver:
         return _lib.check(self._lib.lsb_tile_variant(self._h, -1 if variant is None else int(variant)),
                           "lsb_tile_variant")
 
+    def set_warm_history(self, on=True):
+        """With on, a warm start (``epsilon0``) enters the Anderson history as the second
+        iterate instead of starting the iteration (needs depth >= 1)."""
+        _lib.check(self._lib.lsb_set_warm_history(self._h, 1 if on else 0), "lsb_set_warm_history")
+        self._warm_history = bool(on)
+
     def set_graphs(self, on=True):
         """Replay each iteration as a CUDA graph (default) or launch kernel by kernel."""
         _lib.check(self._lib.lsb_set_graphs(self._h, 1 if on else 0), "lsb_set_graphs")
@@ -245,12 +251,17 @@ class Solver:
         lam0 = torch.zeros(g.shape, device=self.device, dtype=torch.float32)
         mu0 = torch.full(g.shape, 0.5, device=self.device, dtype=torch.float32)
         prec = self.precision
+        hist = getattr(self, "_warm_history", False)
         self.set_precision("fp32", 0)
+        if hist:
+            self.set_warm_history(False)   # the update must start from epsilon
         try:
             r = self.solve(lam0, mu0, eb, rtol=0.0, atol=0.0, maxiter=1, epsilon0=epsilon,
                            want_sigma=False)
         finally:
             self.set_precision(prec)
+            if hist:
+                self.set_warm_history(True)
         ebt = torch.as_tensor(eb, device=self.device).view(eb.shape[0], 6, 1, 1, 1)
         return epsilon + ebt - r.epsilon
 

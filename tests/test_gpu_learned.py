@@ -215,3 +215,31 @@ def test_project_compatible():
     assert (warm.status == 1).all()
     rel = np.linalg.norm(warm.mean_sigma - cold.mean_sigma) / np.linalg.norm(cold.mean_sigma)
     assert rel < 1e-5
+
+
+def test_warm_start_in_anderson_history():
+    """A warm start placed in the Anderson history: the exact solution cuts the solve to a
+    few updates, a poor compatible field still converges to the cold C_eff."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.learned import warm_start as W
+    from jaxmaterials_b200.solver import Solver
+
+    ind = torch.as_tensor(W.indicators(W.structure_params(1, 32, 12), workers=1)).cuda()
+    lm, mu = W.lame_from_indicator(ind)
+    g = GridSpec(32, 32, 32, 32.0, 32.0, 32.0)
+    s = Solver(g, batch=6, depth=5)
+    eb = np.eye(6, dtype=np.float32)
+    cold = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False)
+    s.set_warm_history(True)
+    exact = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False, epsilon0=cold.epsilon)
+    assert (exact.status == 1).all() and (exact.iters <= 4).all()
+    # (the projection switches the history mode off for its own update)
+    poor = s.project_compatible(cold.epsilon + 0.5 * torch.randn_like(cold.epsilon), eb)
+    assert (poor - cold.epsilon).abs().max() > 0.1
+    r = s.solve(lm, mu, eb, rtol=1e-6, maxiter=3000, want_sigma=False, epsilon0=poor)
+    s.set_warm_history(False)
+    assert (r.status == 1).all()
+    for x in (exact, r):
+        rel = np.linalg.norm(x.mean_sigma - cold.mean_sigma) / np.linalg.norm(cold.mean_sigma)
+        assert rel < 1e-5
