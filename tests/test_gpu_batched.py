@@ -114,3 +114,22 @@ def test_c_eff_batch_rejects_bad_input():
         c_eff_batch([a], [a], [g], depth=9)
     with pytest.raises(ValueError):
         c_eff_batch([a], [a[:8]], [g])
+
+
+def test_dataset_generation(tmp_path):
+    """Generated dataset rows equal the single-structure C_eff of the stored fields
+    ([mu, lambda] channel order), and survive a save/load round trip."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import dataset as D
+    from jaxmaterials_b200.solver import c_eff
+
+    lame, sig, dom, iters = D.generate(3, n=16, seed=4)
+    assert lame.shape == (3, 2, 16, 16, 16) and sig.shape == (3, 6, 6) and (iters > 0).all()
+    g = GridSpec(16, 16, 16, 16.0, 16.0, 16.0)
+    for j in range(3):
+        c, _, _ = c_eff(lame[j, 1], lame[j, 0], g, rtol=1e-6, depth=5)
+        np.testing.assert_allclose(sig[j], c.astype(np.float32), rtol=1e-6, atol=1e-6)
+    path = tmp_path / "d.npz"
+    D.save(path, lame, sig, dom)
+    ds = D.LayeredFibresDataset(path)
+    np.testing.assert_array_equal(ds[2][1], sig[2])
