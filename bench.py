@@ -445,9 +445,17 @@ def own_arm(args):
         if args.batched_plain:
             batched["plain"] = batched_run(args.batched, 1000 + rank, 0)
         if world > 1:
-            sec = torch.tensor([batched["anderson"]["seconds"]], device=dev, dtype=torch.float64)
-            dist.all_reduce(sec, op=dist.ReduceOp.MAX)
-            batched["anderson"]["value"] = 6 * args.batched * world / float(sec.item())
+            # whole-job figures: all ranks' solves and voxel-iterations over the slowest rank
+            for key in [k for k in ("anderson", "plain") if k in batched]:
+                part = batched[key]
+                sec = torch.tensor([part["seconds"]], device=dev, dtype=torch.float64)
+                vit = torch.tensor([part["voxel_iter_per_s"] * part["seconds"]], device=dev,
+                                   dtype=torch.float64)
+                dist.all_reduce(sec, op=dist.ReduceOp.MAX)
+                dist.all_reduce(vit, op=dist.ReduceOp.SUM)
+                part["seconds"] = float(sec.item())
+                part["value"] = 6 * args.batched * world / part["seconds"]
+                part["voxel_iter_per_s"] = float(vit.item()) / part["seconds"]
 
     ref = fixture_c_eff(args.depth if args.depth in (0, 5) else 5)
     c_eff_err = (float(np.linalg.norm(c_eff - ref) / np.linalg.norm(ref))
