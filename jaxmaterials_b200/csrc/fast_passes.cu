@@ -74,6 +74,10 @@ __device__ __forceinline__ void step_a_smem(float2* v, int p, const float2* tw) 
 #define LSB_Y_COLS 16
 #endif
 constexpr int kYT = LSB_Y_COLS;
+// kz columns per y-pass block for extent N (128, with 16 threads per column: 8 columns,
+// eight resident blocks per SM; measured -3% against 16 columns, 32 columns +14%)
+template <int N>
+__host__ __device__ constexpr int y_cols() { return N == 128 ? 8 : kYT; }
 
 // Split of the y transform (may differ from the x/z split): 128 = 8 x 16 puts 16 threads
 // on a column and halves the values each thread holds (measured -13% at 128^3 against
@@ -83,7 +87,7 @@ struct YSplit { static constexpr int E = Split<N>::E, P = Split<N>::P; };
 template <>
 struct YSplit<128> { static constexpr int E = 8, P = 16; };
 template <int N>
-__host__ __device__ constexpr int y_threads() { return kYT * YSplit<N>::P; }
+__host__ __device__ constexpr int y_threads() { return y_cols<N>() * YSplit<N>::P; }
 template <int N>
 __host__ __device__ constexpr int y_min_blocks() {
   // (256: three blocks, so that its 16 values per thread fit without spilling)
@@ -95,20 +99,21 @@ __global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fas
                                                                float2* __restrict__ spec,
                                                                const InstanceState* __restrict__ st) {
   constexpr int E = YSplit<NY>::E, P = YSplit<NY>::P, NJ = (E + P - 1) / P;
-  __shared__ float2 buf[NY * kYT];
+  constexpr int YT = y_cols<NY>();
+  __shared__ float2 buf[NY * YT];
   const int bc = blockIdx.z;
   if (!active32(st[bc / 6])) return;
-  const int t = threadIdx.x % kYT, p = threadIdx.x / kYT;
+  const int t = threadIdx.x % YT, p = threadIdx.x / YT;
   const int nzh = g.nzh;
   int kz, x;
   bool valid;
-  if (nzh % kYT == 1 && (int)blockIdx.x == nzh / kYT) {
-    if ((int)blockIdx.y * kYT >= g.nx) return;
+  if (nzh % YT == 1 && (int)blockIdx.x == nzh / YT) {
+    if ((int)blockIdx.y * YT >= g.nx) return;
     kz = nzh - 1;
-    x = blockIdx.y * kYT + t;
+    x = blockIdx.y * YT + t;
     valid = x < g.nx;
   } else {
-    kz = blockIdx.x * kYT + t;
+    kz = blockIdx.x * YT + t;
     x = blockIdx.y;
     valid = kz < nzh;
   }
@@ -122,7 +127,7 @@ __global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fas
   }
   step_a<NY, E>(v, p, tw);
 #pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) buf[(k1 * P + p) * kYT + t] = v[k1];
+  for (int k1 = 0; k1 < E; ++k1) buf[(k1 * P + p) * YT + t] = v[k1];
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < NJ; ++j) {
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fas
     if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) w[q] = buf[(k1 * P + q) * kYT + t];
+    for (int q = 0; q < P; ++q) w[q] = buf[(k1 * P + q) * YT + t];
     Bfly<P>::run(w);
     if (valid) {
 #pragma unroll
@@ -749,7 +754,8 @@ template <int N>
 static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
                     cudaStream_t s) {
   // with a one-column tail, full tiles + one tail tile (see ypass_fast)
-  dim3 grid(g.nzh % kYT == 1 ? g.nzh / kYT + 1 : (g.nzh + kYT - 1) / kYT, g.nx, 6 * batch);
+  constexpr int YT = y_cols<N>();
+  dim3 grid(g.nzh % YT == 1 ? g.nzh / YT + 1 : (g.nzh + YT - 1) / YT, g.nx, 6 * batch);
   ypass_fast<N><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, st);
 }
 
