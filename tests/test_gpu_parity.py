@@ -320,7 +320,7 @@ def test_mixed_precision_reaches_tolerance_at_128(ls):
 
 
 # ------------------------------------------------------------------ Anderson acceleration
-@pytest.mark.parametrize("depth", [1, 2, 4, 5])
+@pytest.mark.parametrize("depth", [1, 2, 3, 4, 5, 8])
 @pytest.mark.parametrize("n", [(12, 10, 8), (32, 16, 64), (37, 47, 61)])
 def test_anderson_fields_match_oracle(ls, depth, n):
     """Same number of Anderson updates (lippmann_schwinger.py:217-231) as the FP64 oracle."""
