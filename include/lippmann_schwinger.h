@@ -224,6 +224,29 @@ const char *lsb_last_error(void);
 /* Library ABI version. */
 int lsb_version(void);
 
+/* No reference counterpart as a library call: voxelises layered fibre composites on the
+ * GPU, as the reference's LayeredFibresDatasetGenerator.material_properties
+ * (src/jaxmaterials/data/data.py:267-314) does on the host, for `nsamples` structures at once, with identical results (bit for bit, FP64 predicates).
+ *
+ * Voxel (i, j, k) has centre (h_x (i + 1/2), h_y (j + 1/2), h_z (k + 1/2)), h_d = L_d / n_d.
+ * Every field starts at the matrix value; voxels with z < d_void or z > z_top_void get
+ * (void - matrix) added once; then (fibre - matrix) is added once for every fibre that
+ * contains the voxel: a fibre record (u0, z0, r2, orientation) contains it when
+ * (u - u0)^2 + (z - z0)^2 < r2 with u = x (orientation 0) or y (orientation 1). Each
+ * addition is rounded to the output type, as numpy's in-place additions are.
+ *
+ * voxels[3], extents[3]: grid; d_void, z_top_void: void-layer bounds (z_top_void is L_z -
+ * d_void as the caller computes it); values[6] = (mu_void, lambda_void, mu_fibre,
+ * lambda_fibre, mu_material, lambda_material); fibre_offsets (host int[nsamples + 1]):
+ * sample s owns records fibre_offsets[s] .. fibre_offsets[s+1]-1 of fibres (host
+ * double[4 * total]); elem_size 4 (float) or 8 (double); d_out (device) receives
+ * [nsamples][2][nx][ny][nz], channel 0 = mu, 1 = lambda (the reference's order); stream: a
+ * cudaStream_t or NULL. Returns 0, or a negative code with lsb_last_error(). */
+int lsb_voxelise_fibres(int nsamples, const int voxels[3], const double extents[3],
+                        double d_void, double z_top_void, const double values[6],
+                        const int *fibre_offsets, const double *fibres, int elem_size,
+                        void *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

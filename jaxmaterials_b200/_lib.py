@@ -1,5 +1,6 @@
-"""ctypes binding of ``liblippmannschwinger.so`` (declarations in
-``include/lippmann_schwinger.h`` and ``include/spectral_net.h``).
+"""ctypes bindings of ``liblippmannschwinger.so`` (declarations in
+``include/lippmann_schwinger.h`` and ``include/spectral_net.h``) and of the host library
+``libfibres.so`` (``include/fibres.h``).
 
 The library is looked up next to this file first, then through the dynamic loader
 (``LD_LIBRARY_PATH``), as the reference wrapper does
@@ -85,7 +86,24 @@ SIGNATURES = {
                                 ctypes.c_int, c_void_p]),
     "lsn_last_error": (ctypes.c_char_p, []),
     "lsb_version": (ctypes.c_int, []),
+    "lsb_voxelise_fibres": (ctypes.c_int, [ctypes.c_int, c_int_p, c_double_p, ctypes.c_double,
+                                           ctypes.c_double, c_double_p, c_int_p, c_double_p,
+                                           ctypes.c_int, c_void_p, c_void_p]),
 }
+
+FIBRES_NAME = "libfibres.so"
+c_uint_p = ctypes.POINTER(ctypes.c_uint)
+FIBRES_SIGNATURES = {
+    "dist_periodic": (None, [ctypes.c_uint, c_double_p, c_double_p, c_double_p, c_double_p]),
+    "initialise_rng": (None, [ctypes.c_uint, c_uint_p, ctypes.c_char_p]),
+    "move_fibres": (None, [ctypes.c_uint, c_double_p, c_double_p, c_double_p, ctypes.c_uint,
+                           ctypes.c_double, ctypes.c_uint, c_uint_p, ctypes.c_char_p]),
+    "fibres_move_batch": (ctypes.c_int, [ctypes.c_int, c_uint_p, c_double_p, c_double_p,
+                                         c_double_p, ctypes.c_uint, ctypes.c_double,
+                                         ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                                         ctypes.c_int]),
+}
+_fibres = None
 
 
 class LibraryError(RuntimeError):
@@ -114,6 +132,28 @@ def load():
             fn.restype = res
             fn.argtypes = args
         _lib = lib
+        return lib
+
+
+def load_fibres():
+    """Load libfibres.so (next to this file, else through the dynamic loader); raise if it
+    is missing."""
+    global _fibres
+    with _lock:
+        if _fibres is not None:
+            return _fibres
+        path = os.path.join(_HERE, FIBRES_NAME)
+        try:
+            lib = ctypes.CDLL(path if os.path.exists(path) else FIBRES_NAME)
+        except OSError as exc:
+            raise LibraryError(
+                f"Unable to load {FIBRES_NAME}: build it with `make -C jaxmaterials_b200/csrc`."
+            ) from exc
+        for name, (res, args) in FIBRES_SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _fibres = lib
         return lib
 
 

@@ -23,11 +23,12 @@ def golden():
 
 @pytest.fixture(scope="session")
 def built_library():
-    """Path of liblippmannschwinger.so, building it with nvcc if it is missing."""
+    """Path of liblippmannschwinger.so, building it (and libfibres.so) if either is missing."""
     from jaxmaterials_b200 import _lib
 
     path = _lib.library_path()
-    if not os.path.exists(path):
+    fibres = os.path.join(os.path.dirname(path), _lib.FIBRES_NAME)
+    if not os.path.exists(path) or not os.path.exists(fibres):
         subprocess.run(["make", "-C", os.path.join(ROOT, "jaxmaterials_b200", "csrc")],
                        check=True, capture_output=True)
     return path

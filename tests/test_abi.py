@@ -9,9 +9,17 @@ import re
 from tests.conftest import ROOT
 
 
-def declared_functions():
+FIBRES_HEADER = "fibres.h"  # declarations of libfibres.so; every other header: the solver library
+
+
+def declared_functions(headers=None):
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        base = os.path.basename(h)
+        if headers is None and base == FIBRES_HEADER:
+            continue
+        if headers is not None and base not in headers:
+            continue
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(",
@@ -39,6 +47,17 @@ def test_binding_covers_every_symbol(built_library):
     lib = _lib.load()
     assert set(_lib.SIGNATURES) == declared_functions()
     assert lib.lsb_version() >= 1
+
+
+def test_fibres_library_exports_and_binding(built_library):
+    from jaxmaterials_b200 import _lib
+
+    names = declared_functions({FIBRES_HEADER})
+    assert {"dist_periodic", "initialise_rng", "move_fibres"} <= names
+    lib = _lib.load_fibres()
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.FIBRES_SIGNATURES) == names
 
 
 def test_product_does_not_import_oracle():
