@@ -46,7 +46,41 @@ def parse():
                    help="structures of the batched uneven-size workload (0: skip)")
     p.add_argument("--batched-plain", action="store_true",
                    help="also time the batched workload with the plain iteration")
+    p.add_argument("--generator", type=int, default=16,
+                   help="samples of the layered-fibre dataset generator leg (0: skip)")
     return p.parse_args()
+
+
+def generator_run(count, seed):
+    """The reference's dataset generator in its own script's configuration
+    (src/generate_data.py:14-56) for `count` samples, through
+    jaxmaterials_b200.data.layered.benchmark (placement on the host cores, GPU voxelisation,
+    whole pipeline with the six C_eff solves per sample), beside the oracle's NumPy
+    voxelisation of the first sample (the reference's CPU code path, restated) as the CPU
+    baseline and the check that both fields are equal."""
+    from jaxmaterials_b200.data.layered import benchmark, reference_config_generator
+    from oracle import fibres_oracle
+
+    res, (sample, field) = benchmark(count, seed, keep_first=True)
+    gen = reference_config_generator(1, seed)
+    g = gen.grid_spec
+    t = time.perf_counter()
+    ref = fibres_oracle.material_properties((g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz), gen.d_void,
+                                            gen._values, *sample, dtype=np.float32)
+    t_cpu = time.perf_counter() - t
+    peak, peak_kind = measured_peak()
+    gbs = res["voxelise_bytes_per_sample"] / (res["voxelise_ms_per_sample"] / 1000.0) / 1e9
+    res.update({
+        "placement_threads": os.cpu_count(),
+        "voxelise_write_GBs": gbs, "voxelise_frac_of_peak": gbs / peak, "peak_source": peak_kind,
+        "cpu_baseline": {"value": t_cpu, "unit": "s/sample", "cores": 1, "kind": "port",
+                         "sample": "voxelisation of the first sample by the oracle's NumPy "
+                                   "restatement of data.py:267-314"},
+        "voxelise_matches_oracle": bool(np.array_equal(field, ref)),
+        "pipeline": "placement + voxelisation + 6 plain solves per sample (rtol = atol = "
+                    "1e-4, maxiter 100) + host copies",
+    })
+    return res
 
 
 def batched_workload(count, seed):
@@ -457,6 +491,14 @@ def own_arm(args):
                 part["value"] = 6 * args.batched * world / part["seconds"]
                 part["voxel_iter_per_s"] = float(vit.item()) / part["seconds"]
 
+    generator = None
+    if args.generator > 0 and world == 1:
+        torch.cuda.empty_cache()
+        try:
+            generator = generator_run(args.generator, 5713853)
+        except Exception as exc:  # reported in the line; the solver figures stand
+            generator = {"error": f"{type(exc).__name__}: {exc}"}
+
     ref = fixture_c_eff(args.depth if args.depth in (0, 5) else 5)
     c_eff_err = (float(np.linalg.norm(c_eff - ref) / np.linalg.norm(ref))
                  if ref is not None and rank == 0 else None)
@@ -481,6 +523,7 @@ def own_arm(args):
             "all_converged": converged,
             "plain": plain,
             "batched": batched,
+            "generator": generator,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "c_eff_rel_err_vs_fp64": c_eff_err,
             "gpu_launches": int(launches),

@@ -22,7 +22,7 @@ import numpy as np
 from .. import _lib
 from .distributions_fibres import initial_lattice, place_batch
 
-__all__ = ["LayeredFibresDatasetGenerator", "voxelise"]
+__all__ = ["LayeredFibresDatasetGenerator", "voxelise", "voxelise_records", "fibre_records"]
 
 _ELEM = {np.dtype(np.float32): 4, np.dtype(np.float64): 8}
 
@@ -37,28 +37,32 @@ def _records(fibre_positions, fibre_radii, fibre_orientations):
     return np.asarray(rows, dtype=np.float64).reshape(-1, 4)
 
 
-def voxelise(samples, grid_spec, d_void, values, dtype=np.float32, device=None):
-    """(mu, lambda) fields of many samples on the GPU: a torch tensor of shape
-    (S, 2, nx, ny, nz) on ``device``.
+def fibre_records(samples):
+    """Offsets (S + 1,) and records (total, 4) of the fibres of many samples, the inputs of
+    ``lsb_voxelise_fibres``."""
+    recs = [_records(*s) for s in samples]
+    off = np.zeros(len(samples) + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(r) for r in recs])
+    fib = np.ascontiguousarray(np.concatenate(recs, axis=0) if recs else np.zeros((0, 4)))
+    return off, fib
 
-    samples: list of (fibre_positions, fibre_radii, fibre_orientations) as returned by
-    ``generate_fibre_positions`` (without the boundaries); values = (mu_void, lambda_void,
-    mu_fibre, lambda_fibre, mu_material, lambda_material)."""
+
+def voxelise_records(off, fib, grid_spec, d_void, values, dtype=np.float32, device=None):
+    """``voxelise`` from prepared records (``fibre_records``)."""
     import torch
 
     dt = np.dtype(dtype)
     if dt not in _ELEM:
         raise ValueError("dtype must be float32 or float64")
     g = grid_spec
+    n = len(off) - 1
     device = torch.device(device) if device is not None else torch.device("cuda")
-    recs = [_records(*s) for s in samples]
-    off = np.zeros(len(samples) + 1, dtype=np.int32)
-    off[1:] = np.cumsum([len(r) for r in recs])
-    fib = np.ascontiguousarray(np.concatenate(recs, axis=0) if recs else np.zeros((0, 4)))
-    out = torch.empty((len(samples), 2, g.nx, g.ny, g.nz),
+    out = torch.empty((n, 2, g.nx, g.ny, g.nz),
                       dtype=torch.float32 if dt == np.float32 else torch.float64, device=device)
-    if not samples:
+    if n == 0:
         return out
+    off = np.ascontiguousarray(off, dtype=np.int32)
+    fib = np.ascontiguousarray(fib, dtype=np.float64)
     voxels = np.array([g.nx, g.ny, g.nz], dtype=np.int32)
     extents = np.array([g.Lx, g.Ly, g.Lz], dtype=np.float64)
     vals = np.asarray(values, dtype=np.float64)
@@ -66,13 +70,23 @@ def voxelise(samples, grid_spec, d_void, values, dtype=np.float32, device=None):
     with torch.cuda.device(device):
         stream = torch.cuda.current_stream(device).cuda_stream
         rc = lib.lsb_voxelise_fibres(
-            len(samples), voxels.ctypes.data_as(_lib.c_int_p),
-            extents.ctypes.data_as(_lib.c_double_p), float(d_void), float(g.Lz - d_void),
-            vals.ctypes.data_as(_lib.c_double_p), off.ctypes.data_as(_lib.c_int_p),
-            fib.ctypes.data_as(_lib.c_double_p), _ELEM[dt], ctypes.c_void_p(out.data_ptr()),
-            ctypes.c_void_p(stream))
+            n, voxels.ctypes.data_as(_lib.c_int_p), extents.ctypes.data_as(_lib.c_double_p),
+            float(d_void), float(g.Lz - d_void), vals.ctypes.data_as(_lib.c_double_p),
+            off.ctypes.data_as(_lib.c_int_p), fib.ctypes.data_as(_lib.c_double_p), _ELEM[dt],
+            ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream))
     _lib.check(rc, "lsb_voxelise_fibres")
     return out
+
+
+def voxelise(samples, grid_spec, d_void, values, dtype=np.float32, device=None):
+    """(mu, lambda) fields of many samples on the GPU: a torch tensor of shape
+    (S, 2, nx, ny, nz) on ``device``.
+
+    samples: list of (fibre_positions, fibre_radii, fibre_orientations) as returned by
+    ``generate_fibre_positions`` (without the boundaries); values = (mu_void, lambda_void,
+    mu_fibre, lambda_fibre, mu_material, lambda_material)."""
+    off, fib = fibre_records(samples)
+    return voxelise_records(off, fib, grid_spec, d_void, values, dtype, device)
 
 
 class LayeredFibresDatasetGenerator:
@@ -222,3 +236,85 @@ class LayeredFibresDatasetGenerator:
             "Data not generated yet, call generate() first."
         g = self.grid_spec
         save(filename, self._lame_parameters, self._sigma_bar, [g.Lx, g.Ly, g.Lz])
+
+
+def reference_config_generator(n_samples, seed=5713853, dtype=np.float32):
+    """The reference's dataset script configuration (src/generate_data.py:14-56): 160 x 160 x
+    64 voxels on 0.5 x 0.5 x 0.2, 3 fibre layers, void layers 0.01, volume fraction 0.3,
+    radii normal 7.5e-3 +- 0.5e-3 in [5e-3, 1e-2]."""
+    from .. import GridSpec
+    from .distributions_fibres import FibreRadiusDistribution
+
+    rd = FibreRadiusDistribution(r_avg=7.5e-3, r_min=5.0e-3, r_max=10.0e-3, sigma=0.5e-3,
+                                 gaussian=True)
+    return LayeredFibresDatasetGenerator(
+        GridSpec(160, 160, 64, 0.5, 0.5, 0.2), 3, 0.01, n_samples, rd, volume_fraction=0.3,
+        mu_fibre=0.5, mu_material=1.0, mu_void=0.1, lambda_fibre=0.1, lambda_material=0.5,
+        lambda_void=1.0, dtype=dtype, rng=np.random.default_rng(seed))
+
+
+def benchmark(n_samples, seed=5713853, pipeline=True, keep_first=False):
+    """Timings of the reference configuration for ``n_samples`` samples: fibre placement on
+    all host cores and on one, GPU voxelisation (CUDA events around the library call:
+    record upload and kernels), and (``pipeline``) the whole ``generate`` (wall clock)."""
+    import time
+
+    import torch
+
+    from .distributions_fibres import place_batch
+
+    gen = reference_config_generator(n_samples, seed)
+    g = gen.grid_spec
+    t = time.perf_counter()
+    samples = [smp[1:] for smp in gen.generate_fibre_positions_batch(n_samples)]
+    t_place = time.perf_counter() - t
+    gen1 = reference_config_generator(n_samples, seed)
+    flat = [layer for _ in range(n_samples) for layer in gen1._draw_layers()[1]]
+    t = time.perf_counter()
+    place_batch([b for _, b, _, _ in flat], [r for _, _, _, r in flat],
+                [x for _, _, x, _ in flat], threads=1)
+    t_place1 = time.perf_counter() - t
+    off, fib = fibre_records(samples)
+    vals = gen._values
+    voxelise_records(off, fib, g, gen.d_void, vals)  # warm-up (sizes the device scratch)
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = voxelise_records(off, fib, g, gen.d_void, vals)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    res = {"samples": n_samples, "grid": [g.nx, g.ny, g.nz], "layers": gen.nlayers,
+           "volume_fraction": gen.volume_fraction, "fibres_per_sample": len(fib) / n_samples,
+           "placement_s_per_sample": t_place / n_samples,
+           "placement_s_per_sample_1_thread": t_place1 / n_samples,
+           "voxelise_ms_per_sample": ms / n_samples,
+           "voxelise_bytes_per_sample": 2 * g.number_of_voxels * 4}
+    first = (samples[0], out[0].cpu().numpy()) if keep_first else None
+    del out
+    if pipeline:
+        gen2 = reference_config_generator(n_samples, seed)
+        t = time.perf_counter()
+        gen2.generate()
+        res["pipeline_samples_per_s"] = n_samples / (time.perf_counter() - t)
+    return res, first
+
+
+def main(argv=None):
+    """``python -m jaxmaterials_b200.data.layered --samples N [--no-pipeline]``: timings of the
+    reference dataset configuration as one JSON line."""
+    import argparse
+    import json
+
+    p = argparse.ArgumentParser()
+    p.add_argument("--samples", type=int, default=16)
+    p.add_argument("--no-pipeline", action="store_true")
+    a = p.parse_args(argv)
+    res, _ = benchmark(a.samples, pipeline=not a.no_pipeline)
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
