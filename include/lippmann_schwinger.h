@@ -247,6 +247,43 @@ int lsb_voxelise_fibres(int nsamples, const int voxels[3], const double extents[
                         const int *fibre_offsets, const double *fibres, int elem_size,
                         void *d_out, void *stream);
 
+/* ---- Damage extension (src/jaxmaterials/solver/lippmann_schwinger.py:36-100, 330-547).
+ * Voigt components (v0..v5) of strain and stress sit in the 3 x 3 tensor as
+ * [[v0, v5, v4], [v5, v1, v3], [v4, v3, v2]] (src/jaxmaterials/utilities.py:65-85). */
+
+/* Replaces elasticity_solve's stress law (lippmann_schwinger.py:330-455): from the next
+ * solve on, every stress evaluation of `solver` uses compute_sigma_damaged
+ * (lippmann_schwinger.py:36-75), sigma = ((1 - d)^2 + k) sigma+ + sigma-, where sigma+-
+ * are the stresses of the strain's tension and compression parts (spectral split, trace
+ * split at 0). d_damage: device [structures][nv] in the layout of the Lame fields (elem_size
+ * 4 = float, 8 = double; the other precision is derived per solve); NULL restores the linear
+ * law. The field must stay valid while solves use it. Returns 0 or a negative code. */
+int lsb_set_damage(lsb_solver *solver, const void *d_damage, int elem_size, double k);
+
+/* Replaces compute_sigma_damaged (lippmann_schwinger.py:36-75) as a standalone call:
+ * sigma [batch][6][nv] from eps [batch][6][nv] and lambda, mu, d [nv] (device; d may be
+ * NULL: no degradation); elem_size 4 or 8; stream: cudaStream_t or NULL. */
+int lsb_damage_stress(long long nv, int batch, const void *d_eps, const void *d_lambda,
+                      const void *d_mu, const void *d_damage, double k, void *d_sigma,
+                      int elem_size, void *stream);
+
+/* Replaces compute_strain_energy (lippmann_schwinger.py:78-100) and the history update of
+ * the staggered scheme (tests/phasefield.py: HH = max(HH, psi)): psi+ = 1/2 lambda
+ * <tr eps>+^2 + mu sum <eig>+^2 from eps [6][nv]; writes psi (if d_psi) and/or
+ * history = max(history, psi) (if d_history). Device pointers; elem_size 4 or 8. */
+int lsb_strain_energy(long long nv, const void *d_eps, const void *d_lambda, const void *d_mu,
+                      void *d_psi, void *d_history, int elem_size, void *stream);
+
+/* Replaces phase_field_solve (lippmann_schwinger.py:457-547) on the grid of `solver` and on
+ * its stream: d = F^-1[F[chi] / (A0 + |xi~|^2)], chi = B - (A - A0) d with A = 1/lc^2 +
+ * 2H/(gc lc), B = 2H/(gc lc), A0 = (min A + max A)/2, until ||chi_new - chi|| <= tolerance
+ * ||chi_new|| or maxiter updates. d_history (H) [nv], d_damage [nv] in: previous damage,
+ * out: new damage (device, elem_size 4 or 8). Writes the updates done to *iters and the last
+ * residual to *residual (either may be NULL). */
+int lsb_phase_field_solve(lsb_solver *solver, const void *d_history, void *d_damage, double gc,
+                          double lc, double tolerance, int maxiter, int elem_size, int *iters,
+                          double *residual);
+
 #ifdef __cplusplus
 }
 #endif

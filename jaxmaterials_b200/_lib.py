@@ -86,6 +86,15 @@ SIGNATURES = {
                                 ctypes.c_int, c_void_p]),
     "lsn_last_error": (ctypes.c_char_p, []),
     "lsb_version": (ctypes.c_int, []),
+    "lsb_set_damage": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_double]),
+    "lsb_damage_stress": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, c_void_p, c_void_p,
+                                         c_void_p, c_void_p, ctypes.c_double, c_void_p,
+                                         ctypes.c_int, c_void_p]),
+    "lsb_strain_energy": (ctypes.c_int, [ctypes.c_longlong, c_void_p, c_void_p, c_void_p,
+                                         c_void_p, c_void_p, ctypes.c_int, c_void_p]),
+    "lsb_phase_field_solve": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_int, c_int_p, c_double_p]),
     "lsb_voxelise_fibres": (ctypes.c_int, [ctypes.c_int, c_int_p, c_double_p, ctypes.c_double,
                                            ctypes.c_double, c_double_p, c_int_p, c_double_p,
                                            ctypes.c_int, c_void_p, c_void_p]),

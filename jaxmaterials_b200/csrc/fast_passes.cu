@@ -11,6 +11,7 @@
 // size and for FP64 fields.
 #include <cmath>
 
+#include "damage.cuh"
 #include "fast_passes.cuh"
 #include "fft_smem.cuh"
 
@@ -458,7 +459,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // (not rewritten), 3 Anderson residual into the rings.
 // bulk: the block's global chunks are 16-byte aligned (TMA bulk copies); otherwise the
 // staging buffers are filled by ordinary loads.
-template <int NZ>
+template <int NZ, bool DMG>
 __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fast(
     GridDesc g, int mode, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
@@ -621,13 +622,19 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
 #pragma unroll
         for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + vx] = e[c];
       }
-      const float lam = lst[idx], tmu = 2.f * lst[L * NZ + idx];
-      const float ltr = lam * (e[0] + e[1] + e[2]);
       float s[6];
+      if constexpr (DMG) {
+        // the damage extension's law (damage field read per voxel, not staged)
+        const float om = 1.f - g.dmg32[(size_t)(b / g.lame_group) * g.nv + vx];
+        damaged_stress<float>(e, lst[idx], lst[L * NZ + idx], om * om + (float)g.dmg_k, s);
+      } else {
+        const float lam = lst[idx], tmu = 2.f * lst[L * NZ + idx];
+        const float ltr = lam * (e[0] + e[1] + e[2]);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
+        for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
 #pragma unroll
-      for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+        for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+      }
 #pragma unroll
       for (int pr = 0; pr < 3; ++pr)
         zbuf[(size_t)(pr * L + l) * LD + n] =
@@ -690,7 +697,9 @@ static size_t xsmem() {
 
 template <int N>
 static cudaError_t configure_n() {
-  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(zpass_fast<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(xpass_fast<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
   if (e != cudaSuccess) return e;
@@ -717,8 +726,12 @@ static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda,
   dim3 grid((unsigned)z_blocks_for<N>(g), batch);
   // every chunk offset is a multiple of 16 bytes when the base pointers are
   const int bulk = aligned16(lambda) && aligned16(mu) && aligned16(eps) && aligned16(spec) ? 1 : 0;
-  zpass_fast<N><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec, eps_bar, eps0,
-                                              st, med, aa);
+  if (g.dmg32)
+    zpass_fast<N, true><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                eps_bar, eps0, st, med, aa);
+  else
+    zpass_fast<N, false><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                 eps_bar, eps0, st, med, aa);
 }
 
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,

@@ -17,6 +17,7 @@
 #include <cfloat>
 #include <cmath>
 
+#include "damage.cuh"
 #include "fft_smem.cuh"
 #include "ls_kernels.cuh"
 
@@ -87,6 +88,8 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
   lambda += (size_t)(b / g.lame_group) * g.nv;
   mu += (size_t)(b / g.lame_group) * g.nv;
   med += b / g.lame_group;
+  const T* dmg = damage_field<T>(g);
+  if (dmg) dmg += (size_t)(b / g.lame_group) * g.nv;
 
   if (mode == 1 || mode == 3) {
     // Build conj(Z) with Z[k] = A[k] + i B[k] on the full line (Hermitian extension);
@@ -193,13 +196,18 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
 #pragma unroll
         for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + v] = e[c];
       }
-      const T lam = lambda[v], tmu = (T)2 * mu[v];
-      const T ltr = lam * (e[0] + e[1] + e[2]);
       T s[6];
+      if (dmg) {
+        const T om = (T)1 - dmg[v];
+        damaged_stress<T>(e, lambda[v], mu[v], om * om + (T)g.dmg_k, s);
+      } else {
+        const T lam = lambda[v], tmu = (T)2 * mu[v];
+        const T ltr = lam * (e[0] + e[1] + e[2]);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
+        for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
 #pragma unroll
-      for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+        for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+      }
 #pragma unroll
       for (int p = 0; p < 3; ++p)
         zbuf[(size_t)(p * L + l) * ldz + n] =
@@ -768,12 +776,13 @@ template <typename T, typename TS>
 __global__ void stress_kernel(long long nv, int phase, int lame_group, const InstanceState* __restrict__ st,
                               const T* __restrict__ lambda, const T* __restrict__ mu,
                               const T* __restrict__ eps, TS* __restrict__ sigma,
-                              double* __restrict__ scratch) {
+                              double* __restrict__ scratch, const T* __restrict__ dmg, T dmg_k) {
   __shared__ double sh[6][32];
   const int b = blockIdx.y;
   if (st[b].phase != phase) return;
   lambda += (size_t)(b / lame_group) * nv;
   mu += (size_t)(b / lame_group) * nv;
+  if (dmg) dmg += (size_t)(b / lame_group) * nv;
   const T* eb = eps + (size_t)b * 6 * nv;
   TS* sg = sigma ? sigma + (size_t)b * 6 * nv : nullptr;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -782,13 +791,18 @@ __global__ void stress_kernel(long long nv, int phase, int lame_group, const Ins
     T e[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * nv + i];
-    const T lam = lambda[i], tmu = (T)2 * mu[i];
-    const T ltr = lam * (e[0] + e[1] + e[2]);
     T s[6];
+    if (dmg) {
+      const T om = (T)1 - dmg[i];
+      damaged_stress<T>(e, lambda[i], mu[i], om * om + dmg_k, s);
+    } else {
+      const T lam = lambda[i], tmu = (T)2 * mu[i];
+      const T ltr = lam * (e[0] + e[1] + e[2]);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
+      for (int c = 0; c < 3; ++c) s[c] = tmu * e[c] + ltr;
 #pragma unroll
-    for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+      for (int c = 3; c < 6; ++c) s[c] = tmu * e[c];
+    }
     if (sg) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) sg[(size_t)c * nv + i] = (TS)s[c];
@@ -989,7 +1003,8 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
   if (nblk < 1) nblk = 1;
   dim3 grid(nblk, batch);
   stress_kernel<T, TS><<<grid, 256, 0, stream>>>(g.nv, phase, g.lame_group, st, lambda, mu, eps, sigma,
-                                                  mean ? scratch : nullptr);
+                                                  mean ? scratch : nullptr, damage_field<T>(g),
+                                                  (T)g.dmg_k);
   if (mean) mean_final_kernel<<<6 * batch, 32, 0, stream>>>(nblk, g.nv, phase, st, scratch, mean);
 }
 
@@ -1015,6 +1030,7 @@ template void launch_convert_fields<float, double>(long long, int, int, const In
 template void launch_convert_fields<double, float>(long long, int, int, const InstanceState*,
                                                    const double*, float*, cudaStream_t);
 template void launch_convert<float, double>(long long, const float*, double*, cudaStream_t);
+template void launch_convert<double, float>(long long, const double*, float*, cudaStream_t);
 template void launch_stress<float, float>(const GridDesc&, int, int, const InstanceState*, const float*,
                                           const float*, const float*, float*, double*, double*,
                                           cudaStream_t);

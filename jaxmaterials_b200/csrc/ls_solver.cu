@@ -105,6 +105,38 @@ int ensure_history(lsb_solver* s, int len) {
 }
 
 // FP64 work buffers, and FP64 copies of `nstruct` Lame field pairs when nstruct > 0.
+// Points s->g at the damage field of lsb_set_damage for a solve over nstruct structures,
+// converting the caller's field into the other precision (the mixed-precision continuation
+// and the FP64 solve read FP64, the FP32 passes FP32).
+int prepare_damage(lsb_solver* s, int nstruct) {
+  GridDesc& g = s->g;
+  g.dmg32 = nullptr;
+  g.dmg64 = nullptr;
+  g.dmg_k = s->dmg_k;
+  if (!s->dmg_user) return 0;
+  const long long n = (long long)nstruct * g.nv;
+  const size_t bytes = (size_t)n * (s->dmg_elem == 4 ? sizeof(double) : sizeof(float));
+  if (bytes > s->dmg_conv_bytes) {
+    if (s->d_dmg_conv) cudaFree(s->d_dmg_conv);
+    s->d_dmg_conv = nullptr;
+    s->dmg_conv_bytes = 0;
+    LSB_CUDA(cudaMalloc(&s->d_dmg_conv, bytes));
+    s->dmg_conv_bytes = bytes;
+  }
+  if (s->dmg_elem == 4) {
+    g.dmg32 = static_cast<const float*>(s->dmg_user);
+    g.dmg64 = static_cast<const double*>(s->d_dmg_conv);
+    launch_convert<float, double>(n, g.dmg32, static_cast<double*>(s->d_dmg_conv), s->stream);
+  } else {
+    g.dmg64 = static_cast<const double*>(s->dmg_user);
+    g.dmg32 = static_cast<const float*>(s->d_dmg_conv);
+    launch_convert<double, float>(n, g.dmg64, static_cast<float*>(s->d_dmg_conv), s->stream);
+  }
+  ++s->launches;
+  LSB_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int ensure_fp64(lsb_solver* s, int nstruct) {
   const size_t B = (size_t)s->batch_cap;
   if (!s->d_spec64) {
@@ -538,6 +570,7 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   cudaStream_t st = s->stream;
   const int nstruct = structures_of(s, batch);
   if (nstruct < 0) return nstruct;
+  LSB_TRY(prepare_damage(s, nstruct));
   LSB_TRY(ensure_history(s, maxiter + 8));
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
   const bool fp64_start = s->precision == kPrecFP64;
@@ -618,6 +651,7 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   cudaStream_t st = s->stream;
   const int nstruct = structures_of(s, batch);
   if (nstruct < 0) return nstruct;
+  LSB_TRY(prepare_damage(s, nstruct));
   LSB_TRY(ensure_history(s, maxiter + 8));
   LSB_TRY(ensure_fp64(s, 0));
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
@@ -767,6 +801,17 @@ int lsb_solve_f64(lsb_solver* solver, int batch, const double* d_lambda, const d
   g_last_error.clear();
   return solve_f64(solver, batch, d_lambda, d_mu, eps_bar, d_eps0, d_eps, d_sigma, mean_sigma,
                    rtol, atol, maxiter, rule, iters, status, residual);
+}
+
+int lsb_set_damage(lsb_solver* solver, const void* d_damage, int elem_size, double k) {
+  g_last_error.clear();
+  if (!solver) return fail(-1, "null solver");
+  if (d_damage && elem_size != 4 && elem_size != 8) return fail(-1, "elem_size must be 4 or 8");
+  if (!std::isfinite(k)) return fail(-1, "k must be finite");
+  solver->dmg_user = d_damage;
+  solver->dmg_elem = d_damage ? elem_size : 4;
+  solver->dmg_k = k;
+  return 0;
 }
 
 long long lsb_kernel_launches(lsb_solver* solver) { return solver ? solver->launches : -1; }

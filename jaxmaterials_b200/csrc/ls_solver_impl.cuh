@@ -55,6 +55,13 @@ struct lsb_solver {
   Medium* d_medium = nullptr;    // [structures]
   double* d_epsbar = nullptr;    // [batch][6]
   double* d_e0ref = nullptr;     // [batch_cap] reference criteria (lsb_set_reference_e0)
+  // damage extension (lsb_set_damage): the caller's field, its element size, k, and the
+  // copy in the other precision for the passes of that precision
+  const void* dmg_user = nullptr;
+  int dmg_elem = 4;
+  double dmg_k = 0.0;
+  void* d_dmg_conv = nullptr;
+  size_t dmg_conv_bytes = 0;
   bool use_e0ref = false;
   double* d_scratch = nullptr;   // 6 * max(1024, batch_cap)
   double* d_mean_scratch = nullptr;
@@ -76,7 +83,7 @@ struct lsb_solver {
     void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
                     d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
                     d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
-                    d_aa_alpha, d_e0ref};
+                    d_aa_alpha, d_e0ref, d_dmg_conv};
     for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
     if (graph_stream) cudaStreamDestroy(graph_stream);

@@ -66,7 +66,20 @@ struct GridDesc {
   const double* cy;
   const double* sz;
   const double* cz;
+  // Damage field of the damage extension (null: the linear law): instance b reads structure
+  // b / lame_group ([structure][nv]); dmg_k is the stiffness left at full damage. The FP32
+  // and FP64 passes read the copy of their precision.
+  const float* dmg32 = nullptr;
+  const double* dmg64 = nullptr;
+  double dmg_k = 0.0;
 };
+
+template <typename T>
+__host__ __device__ inline const T* damage_field(const GridDesc& g);
+template <>
+__host__ __device__ inline const float* damage_field<float>(const GridDesc& g) { return g.dmg32; }
+template <>
+__host__ __device__ inline const double* damage_field<double>(const GridDesc& g) { return g.dmg64; }
 
 // Reference medium, derived on the device from min/max of the Lame fields
 // (lambda0 = (min + max) / 2, evaluated in the precision of the iteration).

@@ -148,6 +148,26 @@ class Solver:
         _lib.check(self._lib.lsb_set_warm_history(self._h, 1 if on else 0), "lsb_set_warm_history")
         self._warm_history = bool(on)
 
+    def set_damage(self, damage, k=1e-12, dtype=np.float32):
+        """Stress law of the damage extension for the following solves (see
+        ``jaxmaterials_b200.solver.damage``): damage field of shape (nx, ny, nz) or (S, nx,
+        ny, nz) like lambda and mu (kept on the device by this solver), residual stiffness
+        k; ``None`` restores the linear law."""
+        import torch
+
+        if damage is None:
+            self._damage = None
+            _lib.check(self._lib.lsb_set_damage(self._h, None, 4, 0.0), "lsb_set_damage")
+            return
+        tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+        t = torch.as_tensor(damage, dtype=tdt, device=self.device).contiguous()
+        g = self.grid_spec
+        if tuple(t.shape[-3:]) != (g.nx, g.ny, g.nz) or t.dim() not in (3, 4):
+            raise ValueError(f"damage must have shape {(g.nx, g.ny, g.nz)} or (S,) + that")
+        self._damage = t
+        _lib.check(self._lib.lsb_set_damage(self._h, ctypes.c_void_p(t.data_ptr()),
+                                            t.element_size(), float(k)), "lsb_set_damage")
+
     def set_graphs(self, on=True):
         """Replay each iteration as a CUDA graph (default) or launch kernel by kernel."""
         _lib.check(self._lib.lsb_set_graphs(self._h, 1 if on else 0), "lsb_set_graphs")

@@ -253,7 +253,7 @@ def lame_reference(lmbda, mu):
 
 def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, depth=0,
                        maxiter=32, dtype=np.float32, spectrum="half", workers=None,
-                       epsilon0=None, history=None, xizero_fn=None):
+                       epsilon0=None, history=None, xizero_fn=None, stress=None):
     """Moulinec-Suquet fixed point with Anderson acceleration of depth ``depth``
     (``src/jaxmaterials/solver/lippmann_schwinger.py:146-265``).
 
@@ -262,7 +262,8 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
     ``epsilon0`` optionally replaces the cold start eps = epsilon_bar by a warm start.
     ``history``, if a list, receives the criterion value after every evaluation.
     ``xizero_fn(grid, dtype)`` replaces ``get_xizero`` (e.g. ``get_xizero_cuda32`` for
-    the reference CUDA library's construction).
+    the reference CUDA library's construction). ``stress(lmbda, mu, eps)`` replaces the
+    linear law (the damage extension's ``elasticity_solve``, lippmann_schwinger.py:330-455).
 
     Returns ``(epsilon, sigma, iterations)`` with sigma = sigma(epsilon); the loop stops
     when e <= atol or e <= rtol * e0 (e0 at the first iterate) or after maxiter updates.
@@ -306,7 +307,8 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
     res = np.zeros((depth + 1, 6) + shape, dtype=dtype)
     a_mat = np.eye(depth + 1, dtype=dtype)
     u_rhs = np.zeros(depth + 1, dtype=dtype)
-    sigma = compute_sigma(lmbda, mu, eps[0])
+    law = stress or compute_sigma
+    sigma = law(lmbda, mu, eps[0])
     sigma_hat = fwd(sigma)
     e = crit(sigma_hat)
     e0 = e
@@ -328,7 +330,7 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
         eps_new = np.einsum("s,saijk", alpha, eps + res).astype(dtype)
         eps = np.roll(eps, 1, axis=0)
         eps[0] = eps_new
-        sigma = compute_sigma(lmbda, mu, eps[0])
+        sigma = law(lmbda, mu, eps[0])
         sigma_hat = fwd(sigma)
         e = crit(sigma_hat)
         if history is not None:

@@ -75,6 +75,14 @@ def max(a, axis=None):
     return _wrap(_np.max(a, axis=_axis(axis)))
 
 
+def trace(a, axis1=0, axis2=1):
+    return _wrap(_np.trace(a, axis1=axis1, axis2=axis2))
+
+
+def where(cond, x, y):
+    return _wrap(_np.where(cond, x, y))
+
+
 def astype(a, dtype):
     return _wrap(_np.asarray(a).astype(dtype))
 
@@ -101,6 +109,10 @@ class _Linalg:
     @staticmethod
     def eigvalsh(a):
         return _wrap(_np.linalg.eigvalsh(a))
+
+    @staticmethod
+    def norm(a):
+        return _wrap(_np.linalg.norm(a))
 
 
 fft = _Fft()
