@@ -48,6 +48,8 @@ def parse():
                    help="also time the batched workload with the plain iteration")
     p.add_argument("--generator", type=int, default=16,
                    help="samples of the layered-fibre dataset generator leg (0: skip)")
+    p.add_argument("--damage", type=int, default=128,
+                   help="grid of the phase-field fracture step leg (0: skip)")
     return p.parse_args()
 
 
@@ -79,6 +81,37 @@ def generator_run(count, seed):
         "voxelise_matches_oracle": bool(np.array_equal(field, ref)),
         "pipeline": "placement + voxelisation + 6 plain solves per sample (rtol = atol = "
                     "1e-4, maxiter 100) + host copies",
+    })
+    return res
+
+
+def damage_run(n):
+    """One staggered step of the reference's phase-field fracture driver (tests/phasefield.py)
+    on the n^3 benchmark composite through jaxmaterials_b200.solver.damage.benchmark, beside
+    the oracle's NumPy damaged iteration (the reference's JAX code path, restated) timed on a
+    bounded sample as the CPU baseline."""
+    from jaxmaterials_b200.solver.damage import benchmark
+    from oracle import damage_oracle as D
+    from oracle import ls_oracle as O
+
+    res = benchmark(n)
+    m = 48
+    rng = np.random.default_rng(0)
+    lm = rng.uniform(1.0, 20.0, (m, m, m))
+    mu = rng.uniform(1.0, 20.0, (m, m, m))
+    dd = rng.uniform(0.0, 1.0, (m, m, m))
+    t = time.perf_counter()
+    D.elasticity_solve(lm, mu, np.array([0.0, 1e-3, 0, 0, 0, 0]), dd, 1e-6,
+                       O.Grid(m, m, m, float(m), float(m), float(m)), rtol=0.0, atol=0.0, depth=3,
+                       maxiter=3, dtype=np.float32, spectrum="half")
+    per_vi = (time.perf_counter() - t) / (4 * m ** 3)  # 4 stress evaluations / transforms
+    nv = n ** 3
+    gpu_vips = res["damaged_iters"] * nv / (res["damaged_solve_ms"] / 1000.0)
+    res.update({
+        "damaged_voxel_iter_per_s": gpu_vips,
+        "cpu_baseline": {"value": 1.0 / per_vi, "unit": "voxel-iterations/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": f"3 damaged Anderson updates at {m}^3 "
+                         "(oracle, FP32 fields, SciPy FFT on all cores)"},
     })
     return res
 
@@ -499,6 +532,14 @@ def own_arm(args):
         except Exception as exc:  # reported in the line; the solver figures stand
             generator = {"error": f"{type(exc).__name__}: {exc}"}
 
+    damage = None
+    if args.damage > 0 and world == 1:
+        torch.cuda.empty_cache()
+        try:
+            damage = damage_run(args.damage)
+        except Exception as exc:  # reported in the line; the solver figures stand
+            damage = {"error": f"{type(exc).__name__}: {exc}"}
+
     ref = fixture_c_eff(args.depth if args.depth in (0, 5) else 5)
     c_eff_err = (float(np.linalg.norm(c_eff - ref) / np.linalg.norm(ref))
                  if ref is not None and rank == 0 else None)
@@ -524,6 +565,7 @@ def own_arm(args):
             "plain": plain,
             "batched": batched,
             "generator": generator,
+            "damage": damage,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "c_eff_rel_err_vs_fp64": c_eff_err,
             "gpu_launches": int(launches),

@@ -123,15 +123,48 @@ __global__ void __launch_bounds__(256) pf_minmax_kernel(long long nv, const T* _
 
 // A0 = (A(min H) + A(max H)) / 2 in the field precision (A is monotone in H), and the
 // initial state (one update at least, as the reference's loop starts at residual 1).
-template <typename T>
-__global__ void pf_setup_kernel(int nblk, const double* __restrict__ part, PFCoef c,
-                                double tolerance, int maxiter, PFState* __restrict__ st) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double lo = INFINITY, hi = -INFINITY;
-  for (int b = 0; b < nblk; ++b) {
-    lo = fmin(lo, part[2 * b]);
-    hi = fmax(hi, part[2 * b + 1]);
+// One block of 256 threads: thread t folds partials t, t + 256, ... in order, then a fixed
+// tree combines the threads (deterministic for a given partial count).
+template <bool MINMAX>
+__device__ __forceinline__ void fold_pairs(int nblk, const double* __restrict__ part, double& a,
+                                           double& b) {
+  __shared__ double sa[256], sb[256];
+  double x = MINMAX ? INFINITY : 0.0, y = MINMAX ? -INFINITY : 0.0;
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    if (MINMAX) {
+      x = fmin(x, part[2 * k]);
+      y = fmax(y, part[2 * k + 1]);
+    } else {
+      x += part[2 * k];
+      y += part[2 * k + 1];
+    }
   }
+  sa[threadIdx.x] = x;
+  sb[threadIdx.x] = y;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      if (MINMAX) {
+        sa[threadIdx.x] = fmin(sa[threadIdx.x], sa[threadIdx.x + s]);
+        sb[threadIdx.x] = fmax(sb[threadIdx.x], sb[threadIdx.x + s]);
+      } else {
+        sa[threadIdx.x] += sa[threadIdx.x + s];
+        sb[threadIdx.x] += sb[threadIdx.x + s];
+      }
+    }
+    __syncthreads();
+  }
+  a = sa[0];
+  b = sb[0];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) pf_setup_kernel(int nblk, const double* __restrict__ part, PFCoef c,
+                                                       double tolerance, int maxiter,
+                                                       PFState* __restrict__ st) {
+  double lo, hi;
+  fold_pairs<true>(nblk, part, lo, hi);
+  if (threadIdx.x != 0) return;
   const T amin = coef_a<T>((T)lo, c), amax = coef_a<T>((T)hi, c);
   st->a0 = (double)((T)0.5 * (amin + amax));
   st->resid = 1.0;
@@ -308,14 +341,13 @@ __global__ void __launch_bounds__(kMaxThreads) pf_zinv_kernel(GridDesc g, int L,
 
 // residual = ||chi_new - chi|| / ||chi_new|| (0 when ||chi_new|| <= 1e-12), stop decision
 // (lippmann_schwinger.py:503-520).
-__global__ void pf_finalize_kernel(int nblk, const double* __restrict__ part, double tolerance,
-                                   int maxiter, PFState* __restrict__ st) {
-  if (threadIdx.x != 0 || blockIdx.x != 0 || st->done) return;
-  double a = 0.0, b = 0.0;
-  for (int k = 0; k < nblk; ++k) {
-    a += part[2 * k];
-    b += part[2 * k + 1];
-  }
+__global__ void __launch_bounds__(256) pf_finalize_kernel(int nblk, const double* __restrict__ part,
+                                                          double tolerance, int maxiter,
+                                                          PFState* __restrict__ st) {
+  if (st->done) return;
+  double a, b;
+  fold_pairs<false>(nblk, part, a, b);
+  if (threadIdx.x != 0) return;
   const double nb = sqrt(b);
   st->resid = nb > 1e-12 ? sqrt(a) / nb : 0.0;
   st->iter += 1;
@@ -343,31 +375,34 @@ int phase_field(lsb_solver* s, const T* d_h, T* d_d, double gc, double lc, doubl
   const int zblocks = (int)((nlines + Lz - 1) / Lz);
   const int mmblk = (int)std::min<long long>(1024, (nv + 255) / 256);
   const int pblk = std::max(zblocks, mmblk);
-  C* w = nullptr;
-  T* chi = nullptr;
-  double* part = nullptr;
-  PFState* dst = nullptr;
-  PFState* hst = nullptr;
-  auto cleanup = [&]() {
-    if (w) cudaFree(w);
-    if (chi) cudaFree(chi);
-    if (part) cudaFree(part);
-    if (dst) cudaFree(dst);
-    if (hst) cudaFreeHost(hst);
-  };
-  cudaError_t e = cudaMalloc(&w, sizeof(C) * nv);
-  if (e == cudaSuccess) e = cudaMalloc(&chi, sizeof(T) * nv);
-  if (e == cudaSuccess) e = cudaMalloc(&part, sizeof(double) * 2 * pblk);
-  if (e == cudaSuccess) e = cudaMalloc(&dst, sizeof(PFState));
-  if (e == cudaSuccess) e = cudaMallocHost(&hst, sizeof(PFState));
-  if (e != cudaSuccess) {
-    cleanup();
-    return fail(-3, "phase field: allocation: %s", cudaGetErrorString(e));
+  // work buffers kept by the solver across calls (sized for FP64, so either precision fits)
+  if (!s->d_pf_w) {
+    cudaError_t ae = cudaMalloc(&s->d_pf_w, sizeof(double2) * nv);
+    if (ae == cudaSuccess) ae = cudaMalloc(&s->d_pf_chi, sizeof(double) * nv);
+    if (ae == cudaSuccess) ae = cudaMalloc(&s->d_pf_part, sizeof(double) * 2 * pblk);
+    if (ae == cudaSuccess) ae = cudaMalloc(&s->d_pf_state, sizeof(PFState));
+    if (ae == cudaSuccess) ae = cudaMallocHost(&s->h_pf_state, sizeof(PFState));
+    if (ae != cudaSuccess) {
+      void** bufs[] = {&s->d_pf_w, &s->d_pf_chi, &s->d_pf_part, &s->d_pf_state};
+      for (void** b : bufs) {
+        if (*b) cudaFree(*b);
+        *b = nullptr;
+      }
+      if (s->h_pf_state) cudaFreeHost(s->h_pf_state);
+      s->h_pf_state = nullptr;
+      return fail(-3, "phase field: allocation: %s", cudaGetErrorString(ae));
+    }
   }
+  C* w = static_cast<C*>(s->d_pf_w);
+  T* chi = static_cast<T*>(s->d_pf_chi);
+  double* part = static_cast<double*>(s->d_pf_part);
+  PFState* dst = static_cast<PFState*>(s->d_pf_state);
+  PFState* hst = static_cast<PFState*>(s->h_pf_state);
+  cudaError_t e = cudaSuccess;
   const PFCoef c{1.0 / (lc * lc), gc * lc};
   const size_t smz = sizeof(C) * Lz * g.nz, smy = sizeof(C) * Ty * g.ny, smx = sizeof(C) * Tx * g.nx;
   pf_minmax_kernel<T><<<mmblk, 256, 0, st>>>(nv, d_h, part);
-  pf_setup_kernel<T><<<1, 32, 0, st>>>(mmblk, part, c, tolerance, maxiter, dst);
+  pf_setup_kernel<T><<<1, 256, 0, st>>>(mmblk, part, c, tolerance, maxiter, dst);
   pf_chi_kernel<T><<<mmblk, 256, 0, st>>>(nv, d_h, d_d, c, dst, chi);
   s->launches += 3;
   const dim3 gy((g.nz + Ty - 1) / Ty, g.nx), gx((g.nz + Tx - 1) / Tx, g.ny);
@@ -379,7 +414,7 @@ int phase_field(lsb_solver* s, const T* d_h, T* d_d, double gc, double lc, doubl
       pf_x_kernel<T><<<gx, tx, smx, st>>>(g, Tx, w, dst);
       pf_y_kernel<T><<<gy, ty, smy, st>>>(g, Ty, 1, w, dst);
       pf_zinv_kernel<T><<<zblocks, tz, smz, st>>>(g, Lz, w, d_h, c, d_d, chi, part, dst);
-      pf_finalize_kernel<<<1, 32, 0, st>>>(zblocks, part, tolerance, maxiter, dst);
+      pf_finalize_kernel<<<1, 256, 0, st>>>(zblocks, part, tolerance, maxiter, dst);
     }
     s->launches += 6LL * chunk;
     e = cudaMemcpyAsync(hst, dst, sizeof(PFState), cudaMemcpyDeviceToHost, st);
@@ -391,7 +426,6 @@ int phase_field(lsb_solver* s, const T* d_h, T* d_d, double gc, double lc, doubl
   if (e == cudaSuccess) e = cudaGetLastError();
   if (iters) *iters = done_iters;
   if (residual) *residual = e == cudaSuccess ? hst->resid : NAN;
-  cleanup();
   if (e != cudaSuccess) return fail(-2, "phase field: %s", cudaGetErrorString(e));
   return 0;
 }

@@ -62,6 +62,12 @@ struct lsb_solver {
   double dmg_k = 0.0;
   void* d_dmg_conv = nullptr;
   size_t dmg_conv_bytes = 0;
+  // phase-field work buffers (lsb_phase_field_solve), allocated on first use
+  void* d_pf_w = nullptr;
+  void* d_pf_chi = nullptr;
+  void* d_pf_part = nullptr;
+  void* d_pf_state = nullptr;
+  void* h_pf_state = nullptr;  // pinned
   bool use_e0ref = false;
   double* d_scratch = nullptr;   // 6 * max(1024, batch_cap)
   double* d_mean_scratch = nullptr;
@@ -83,9 +89,10 @@ struct lsb_solver {
     void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
                     d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
                     d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
-                    d_aa_alpha, d_e0ref, d_dmg_conv};
+                    d_aa_alpha, d_e0ref, d_dmg_conv, d_pf_w, d_pf_chi, d_pf_part, d_pf_state};
     for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
+    if (h_pf_state) cudaFreeHost(h_pf_state);
     if (graph_stream) cudaStreamDestroy(graph_stream);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);

@@ -164,3 +164,89 @@ def phase_field_solve(HH, d_old, gc, lc, grid_spec, tolerance=1e-6, maxiter=1000
             float(lc), float(tolerance), int(maxiter), d.element_size(), ctypes.byref(iters),
             ctypes.byref(res)), "lsb_phase_field_solve")
     return _out(d, as_t), int(iters.value)
+
+
+def benchmark(n=128, seed=0, depth=3):
+    """One staggered step of the reference's phase-field fracture driver
+    (tests/phasefield.py:165-214) on an n^3 cross-ply composite: phase-field solve from a
+    history field, damaged elasticity solve (Anderson depth ``depth``, rtol 1e-6, tension
+    along y), history update; the damaged solve is also timed against the linear solve of the
+    same problem. CUDA events on the current stream."""
+    import torch
+
+    from .. import GridSpec
+    from ..data import fibres
+
+    st = fibres.generate_layered_fibres(n, 4, 4.0, 0.45, seed=seed)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(n, n, n, float(n), float(n), float(n))
+    lm_d = torch.as_tensor(lm, device="cuda")
+    mu_d = torch.as_tensor(mu, device="cuda")
+    eb = np.array([0.0, 1e-3, 0.0, 0.0, 0.0, 0.0])
+    rng = np.random.default_rng(seed)
+    # a damage field concentrated in a band across the fibres
+    x = (np.arange(n) + 0.5) / n
+    band = np.exp(-((x - 0.5) / 0.05) ** 2)
+    d0 = torch.as_tensor((0.5 * band[None, :, None] * np.ones((n, n, n))).astype(np.float32),
+                         device="cuda")
+    hist = torch.as_tensor(rng.uniform(0.0, 1e-3, (n, n, n)).astype(np.float32), device="cuda")
+    s_lin = Solver(g, batch=1, depth=depth)
+    s_dmg = Solver(g, batch=1, depth=depth)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    def lin():
+        return s_lin.solve(lm_d, mu_d, eb, rtol=1e-6, atol=1e-20, maxiter=2000, rule=RULE_JAX,
+                           want_sigma=False)
+
+    def dmg():
+        return elasticity_solve(lm_d, mu_d, eb, d0, 1e-6, g, rtol=1e-6, depth=depth,
+                                maxiter=2000, solver=s_dmg)
+
+    def pf():
+        return phase_field_solve(hist, d0, 2.7e-3, 1.5, g, tolerance=1e-6, maxiter=10000)
+
+    for _ in range(2):  # warm-up (plans, graphs, x-pass tile choice, work buffers)
+        for f in (lin, dmg, pf):
+            f()
+    r_lin, ms_lin = timed(lin)
+    (eps, _, it_dmg), ms_dmg = timed(dmg)
+    (_, it_pf), ms_pf = timed(pf)
+    h2 = hist.clone()
+    _, ms_hist = timed(lambda: update_history(h2, lm_d, mu_d, eps))
+    s_lin.close()
+    s_dmg.close()
+    return {"grid": [n, n, n], "anderson_depth": depth, "load": "unit tension along y (1e-3)",
+            "linear_solve_ms": ms_lin, "linear_iters": int(r_lin.iters[0]),
+            "damaged_solve_ms": ms_dmg, "damaged_iters": it_dmg,
+            "damaged_ms_per_iter": ms_dmg / max(it_dmg, 1),
+            "linear_ms_per_iter": ms_lin / max(int(r_lin.iters[0]), 1),
+            "phase_field_ms": ms_pf, "phase_field_iters": it_pf,
+            "phase_field_ms_per_iter": ms_pf / max(it_pf, 1),
+            "history_update_ms": ms_hist}
+
+
+def main(argv=None):
+    """``python -m jaxmaterials_b200.solver.damage [--n 128]``: timings of one staggered
+    phase-field fracture step as one JSON line."""
+    import argparse
+    import json
+
+    p = argparse.ArgumentParser()
+    p.add_argument("--n", type=int, default=128)
+    p.add_argument("--depth", type=int, default=3)
+    a = p.parse_args(argv)
+    print(json.dumps(benchmark(a.n, depth=a.depth)))
+
+
+if __name__ == "__main__":
+    main()
