@@ -284,6 +284,24 @@ int lsb_phase_field_solve(lsb_solver *solver, const void *d_history, void *d_dam
                           double lc, double tolerance, int maxiter, int elem_size, int *iters,
                           double *residual);
 
+/* ---- Anisotropic stiffness (the derivation of doc/linear_elasticity.tex:372-402 and
+ * doc/anisotropic.py; the reference has no solver for it).
+ * From the next solve on, `solver` uses the stiffness field d_stiffness: device
+ * [structures][21][nv] (layout of the Lame fields, 21 entries per voxel) holding the
+ * independent entries C_0..C_20 of the symmetric 6 x 6 Voigt matrix in the numbering of
+ * doc/anisotropic.py:150-185 (C_0..C_5 the diagonal, then (0,1), (0,2), (1,2), (0,3), (0,4),
+ * (0,5), (1,3), (1,4), (1,5), (2,3), (2,4), (2,5), (3,4), (3,5), (4,5)), Voigt order (xx, yy,
+ * zz, xy, xz, yz), tensor shear: sigma_a = sum_b C_ab w_b eps_b, w = (1, 1, 1, 2, 2, 2).
+ * Gamma^0 follows from the reference stiffness C^0 through the inverse of the acoustic
+ * matrix K_ki = C^0_kjil xi_j xi_l; c0 (host double[21]) fixes C^0 for every structure,
+ * NULL takes (min + max) / 2 of every entry over each structure. The lambda/mu arguments of
+ * the solves then do not enter the law (they must still be valid device arrays of the Lame
+ * layout, e.g. two entries of the stiffness field). The generic passes run
+ * (no compile-time-size FP32 passes). NULL restores the isotropic law; cannot be combined
+ * with lsb_set_damage. */
+int lsb_set_anisotropic(lsb_solver *solver, const void *d_stiffness, int elem_size,
+                        const double *c0);
+
 #ifdef __cplusplus
 }
 #endif

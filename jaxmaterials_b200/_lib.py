@@ -95,6 +95,7 @@ SIGNATURES = {
     "lsb_phase_field_solve": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              ctypes.c_int, c_int_p, c_double_p]),
+    "lsb_set_anisotropic": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_double_p]),
     "lsb_voxelise_fibres": (ctypes.c_int, [ctypes.c_int, c_int_p, c_double_p, ctypes.c_double,
                                            ctypes.c_double, c_double_p, c_int_p, c_double_p,
                                            ctypes.c_int, c_void_p, c_void_p]),

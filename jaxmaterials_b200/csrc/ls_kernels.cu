@@ -17,6 +17,7 @@
 #include <cfloat>
 #include <cmath>
 
+#include "aniso.cuh"
 #include "damage.cuh"
 #include "fft_smem.cuh"
 #include "ls_kernels.cuh"
@@ -90,6 +91,8 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
   med += b / g.lame_group;
   const T* dmg = damage_field<T>(g);
   if (dmg) dmg += (size_t)(b / g.lame_group) * g.nv;
+  const T* cf = stiffness_field<T>(g);
+  if (cf) cf += (size_t)(b / g.lame_group) * 21 * g.nv;
 
   if (mode == 1 || mode == 3) {
     // Build conj(Z) with Z[k] = A[k] + i B[k] on the full line (Hermitian extension);
@@ -156,6 +159,10 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
     double sh[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) sh[c] = (c < 3 ? med->lmean * tr : 0.0) + 2.0 * med->mmean * e[c];
+    if (cf) {  // anisotropic: C^0 eps_bar
+      const double* c0 = g.c0 + (size_t)(b / g.lame_group) * 21;
+      aniso_stress<double>([&](int k) { return c0[k]; }, e, sh);
+    }
 #pragma unroll
     for (int c = 0; c < 6; ++c) shift[c] = (T)sh[c];
     if (blockIdx.x == 0 && tid == 0) {
@@ -197,7 +204,9 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
         for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + v] = e[c];
       }
       T s[6];
-      if (dmg) {
+      if (cf) {
+        aniso_stress<T>([&](int k) { return cf[(size_t)k * g.nv + v]; }, e, s);
+      } else if (dmg) {
         const T om = (T)1 - dmg[v];
         damaged_stress<T>(e, lambda[v], mu[v], om * om + (T)g.dmg_k, s);
       } else {
@@ -348,7 +357,36 @@ __global__ void __launch_bounds__(kMaxThreads) xpass_kernel(GridDesc g, int TT,
     }
     // normalised wave vector (fourier.py:61-85): FP64 with the 1e-12 guard
     double nrm = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-    if (nrm < 1.0e-12) nrm = 1.0;
+    const bool guarded = nrm < 1.0e-12;
+    if (guarded) nrm = 1.0;
+    if (g.c0) {
+      // anisotropic reference stiffness: r = -Gamma^0 tau through the inverse acoustic
+      // matrix (aniso.cuh); modes without a direction (the zero mode, the guarded ones)
+      // get r = 0, the limit of the isotropic closed form there
+      const double zd[3] = {x0 / nrm, x1 / nrm, x2 / nrm};
+      double nd[6];
+      const bool ok = !guarded && aniso_inverse_acoustic(g.c0 + (size_t)(b / g.lame_group) * 21, zd, nd);
+      T o[2][6];
+      if (ok) {
+        const T zt[3] = {(T)zd[0], (T)zd[1], (T)zd[2]};
+        T nt[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) nt[k] = (T)nd[k];
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          T tv[6];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) tv[c] = part ? s[c].y : s[c].x;
+          aniso_gamma<T>(nt, zt, tv, o[part]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) o[0][c] = o[1][c] = (T)0;
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) row[c * TT] = mk<C>(o[0][c], -o[1][c]);
+      continue;
+    }
     const T z0 = (T)(x0 / nrm), z1 = (T)(x1 / nrm), z2 = (T)(x2 / nrm);
     // r_hat = C_A A(xi) sigma_hat + C_B (xi xi : sigma_hat) xi xi   (fourier.cu:268-327)
     const T z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
@@ -776,13 +814,15 @@ template <typename T, typename TS>
 __global__ void stress_kernel(long long nv, int phase, int lame_group, const InstanceState* __restrict__ st,
                               const T* __restrict__ lambda, const T* __restrict__ mu,
                               const T* __restrict__ eps, TS* __restrict__ sigma,
-                              double* __restrict__ scratch, const T* __restrict__ dmg, T dmg_k) {
+                              double* __restrict__ scratch, const T* __restrict__ dmg, T dmg_k,
+                              const T* __restrict__ cf) {
   __shared__ double sh[6][32];
   const int b = blockIdx.y;
   if (st[b].phase != phase) return;
   lambda += (size_t)(b / lame_group) * nv;
   mu += (size_t)(b / lame_group) * nv;
   if (dmg) dmg += (size_t)(b / lame_group) * nv;
+  if (cf) cf += (size_t)(b / lame_group) * 21 * nv;
   const T* eb = eps + (size_t)b * 6 * nv;
   TS* sg = sigma ? sigma + (size_t)b * 6 * nv : nullptr;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -792,7 +832,9 @@ __global__ void stress_kernel(long long nv, int phase, int lame_group, const Ins
 #pragma unroll
     for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * nv + i];
     T s[6];
-    if (dmg) {
+    if (cf) {
+      aniso_stress<T>([&](int k) { return cf[(size_t)k * nv + i]; }, e, s);
+    } else if (dmg) {
       const T om = (T)1 - dmg[i];
       damaged_stress<T>(e, lambda[i], mu[i], om * om + dmg_k, s);
     } else {
@@ -1004,7 +1046,7 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
   dim3 grid(nblk, batch);
   stress_kernel<T, TS><<<grid, 256, 0, stream>>>(g.nv, phase, g.lame_group, st, lambda, mu, eps, sigma,
                                                   mean ? scratch : nullptr, damage_field<T>(g),
-                                                  (T)g.dmg_k);
+                                                  (T)g.dmg_k, stiffness_field<T>(g));
   if (mean) mean_final_kernel<<<6 * batch, 32, 0, stream>>>(nblk, g.nv, phase, st, scratch, mean);
 }
 

@@ -202,6 +202,7 @@ int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]) {
   if (!factorize(g.nx, g.px) || !factorize(g.ny, g.py) || !factorize(g.nz, g.pz))
     return fail(-1, "grid extent has too many prime factors");
   s->sh32 = plan_launch(g, sizeof(float2));
+  s->x_blocks_generic32 = s->sh32.x_blocks_per_instance;
   s->sh64 = plan_launch(g, sizeof(double2));
   s->fast32 = fast::supported(g);
   if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g, s->xvariant) * g.ny;
@@ -282,6 +283,7 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   const size_t B = (size_t)batch;
   // room for the partials of either x-pass tile variant
   const size_t xblk = (size_t)std::max({s->sh32.x_blocks_per_instance, s->sh64.x_blocks_per_instance,
+                                        s->x_blocks_generic32,
                                         s->fast32 ? fast::x_tiles(g, 1) * g.ny : 0});
   const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
   bool ok = alloc((void**)&s->d_eps32, sizeof(float) * B * 6 * g.nv) &&
@@ -347,7 +349,7 @@ template <typename T>
 void pass_z(lsb_solver* s, int mode, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
             const T* eps0, const AndersonArgs<T>& aa) {
   if constexpr (sizeof(T) == 4) {
-    if (s->fast32) {
+    if (use_fast32(s)) {
       fast::launch_zpass(s->g, mode, batch, lam, mu, eps, spec, s->d_epsbar, eps0, s->d_state,
                          s->d_medium, aa, s->stream);
       return;
@@ -360,7 +362,7 @@ void pass_z(lsb_solver* s, int mode, int batch, const T* lam, const T* mu, T* ep
 template <typename T>
 void pass_y(lsb_solver* s, bool inverse, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
-    if (s->fast32) {
+    if (use_fast32(s)) {
       fast::launch_ypass(s->g, inverse, batch, spec, s->d_state, s->stream);
       return;
     }
@@ -371,7 +373,7 @@ void pass_y(lsb_solver* s, bool inverse, int batch, cplx<T>* spec) {
 template <typename T>
 void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
-    if (s->fast32) {
+    if (use_fast32(s)) {
       fast::launch_xpass(s->g, s->xvariant, batch, spec, s->d_medium, s->d_state, s->d_partials,
                          s->stream);
       return;
@@ -450,7 +452,8 @@ template <typename T>
 int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
               const T* eps0, int init_mode, const SolveParams& sp, bool anderson,
               const T* inject = nullptr) {
-  const LaunchShape& sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
+  LaunchShape sh = sizeof(T) == 8 ? s->sh64 : s->sh32;
+  if (sizeof(T) == 4 && !use_fast32(s)) sh.x_blocks_per_instance = s->x_blocks_generic32;
   const int phase = sizeof(T) == 8 ? 1 : 0;
   GraphPhase gp(s);
   cudaStream_t st = s->stream;
@@ -514,8 +517,9 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
 // buffers; the passes only write the spectrum, the partials and the zero mode, all of
 // which the solve recomputes before use. Runs once per solver.
 int tune_xpass(lsb_solver* s, int batch) {
+  if (!use_fast32(s)) return 0;  // the generic passes have no tile variants
   s->xtuned = true;
-  if (!s->fast32 || fast::x_tiles(s->g, 0) == fast::x_tiles(s->g, 1)) return 0;
+  if (fast::x_tiles(s->g, 0) == fast::x_tiles(s->g, 1)) return 0;
   cudaStream_t st = s->stream;
   cudaEvent_t ev[2];
   LSB_CUDA(cudaEventCreate(&ev[0]));
@@ -571,6 +575,7 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   const int nstruct = structures_of(s, batch);
   if (nstruct < 0) return nstruct;
   LSB_TRY(prepare_damage(s, nstruct));
+  LSB_TRY(prepare_aniso(s, nstruct));
   LSB_TRY(ensure_history(s, maxiter + 8));
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);
   const bool fp64_start = s->precision == kPrecFP64;
@@ -652,6 +657,7 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   const int nstruct = structures_of(s, batch);
   if (nstruct < 0) return nstruct;
   LSB_TRY(prepare_damage(s, nstruct));
+  LSB_TRY(prepare_aniso(s, nstruct));
   LSB_TRY(ensure_history(s, maxiter + 8));
   LSB_TRY(ensure_fp64(s, 0));
   const SolveParams sp = make_params(s, rtol, atol, maxiter, rule);

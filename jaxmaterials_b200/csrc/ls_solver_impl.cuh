@@ -62,6 +62,17 @@ struct lsb_solver {
   double dmg_k = 0.0;
   void* d_dmg_conv = nullptr;
   size_t dmg_conv_bytes = 0;
+  // anisotropic stiffness (lsb_set_anisotropic): the caller's field, its element size, an
+  // optional caller C^0, the copy in the other precision and the per-structure C^0
+  const void* aniso_user = nullptr;
+  int aniso_elem = 4;
+  bool aniso_c0_given = false;
+  double aniso_c0[21] = {};
+  void* d_cf_conv = nullptr;
+  size_t cf_conv_bytes = 0;
+  double* d_c0 = nullptr;        // [batch_cap][21]
+  double* d_c0_part = nullptr;   // min/max partials of the C^0 reduction
+  int x_blocks_generic32 = 1;    // x-pass partials per instance of the generic FP32 pass
   // phase-field work buffers (lsb_phase_field_solve), allocated on first use
   void* d_pf_w = nullptr;
   void* d_pf_chi = nullptr;
@@ -89,7 +100,8 @@ struct lsb_solver {
     void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
                     d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
                     d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
-                    d_aa_alpha, d_e0ref, d_dmg_conv, d_pf_w, d_pf_chi, d_pf_part, d_pf_state};
+                    d_aa_alpha, d_e0ref, d_dmg_conv, d_pf_w, d_pf_chi, d_pf_part, d_pf_state,
+                    d_cf_conv, d_c0, d_c0_part};
     for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
     if (h_pf_state) cudaFreeHost(h_pf_state);
@@ -114,6 +126,11 @@ int upload_tables(lsb_solver* s);
 // Sets s->g.lame_group for a solve of `batch` instances and returns the number of Lame
 // field pairs the solve reads (negative with an error message when batch does not split).
 int structures_of(lsb_solver* s, int batch);
+// Points s->g at the anisotropic stiffness of lsb_set_anisotropic (both precisions) and
+// its reference stiffness C^0 for a solve over nstruct structures (aniso.cu).
+int prepare_aniso(lsb_solver* s, int nstruct);
+// The compile-time-size FP32 passes apply (every extent supported, isotropic law).
+inline bool use_fast32(const lsb_solver* s) { return s->fast32 && s->g.cf32 == nullptr; }
 // Full FP32-input solve (see lsb_solve); d_eps is the FP32 work buffer and output.
 int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
               const double* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,

@@ -72,7 +72,19 @@ struct GridDesc {
   const float* dmg32 = nullptr;
   const double* dmg64 = nullptr;
   double dmg_k = 0.0;
+  // Anisotropic stiffness (null: the isotropic lambda, mu law): C [structure][21][nv] in the
+  // numbering of aniso.cuh, per precision, and the reference stiffness C^0 [structure][21].
+  const float* cf32 = nullptr;
+  const double* cf64 = nullptr;
+  const double* c0 = nullptr;
 };
+
+template <typename T>
+__host__ __device__ inline const T* stiffness_field(const GridDesc& g);
+template <>
+__host__ __device__ inline const float* stiffness_field<float>(const GridDesc& g) { return g.cf32; }
+template <>
+__host__ __device__ inline const double* stiffness_field<double>(const GridDesc& g) { return g.cf64; }
 
 template <typename T>
 __host__ __device__ inline const T* damage_field(const GridDesc& g);

@@ -168,6 +168,30 @@ class Solver:
         _lib.check(self._lib.lsb_set_damage(self._h, ctypes.c_void_p(t.data_ptr()),
                                             t.element_size(), float(k)), "lsb_set_damage")
 
+    def set_anisotropic(self, stiffness, c0=None, dtype=np.float32):
+        """Anisotropic stiffness for the following solves (see
+        ``jaxmaterials_b200.solver.anisotropic``): entries of shape (21, nx, ny, nz) or (S, 21,
+        nx, ny, nz), kept on the device by this solver; c0 (21,) fixes the reference
+        stiffness (default: mid-range of every entry); ``None`` restores the isotropic law."""
+        import torch
+
+        if stiffness is None:
+            self._stiffness = None
+            _lib.check(self._lib.lsb_set_anisotropic(self._h, None, 4, None), "lsb_set_anisotropic")
+            return
+        tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+        t = torch.as_tensor(stiffness, dtype=tdt, device=self.device).contiguous()
+        g = self.grid_spec
+        if tuple(t.shape[-4:]) != (21, g.nx, g.ny, g.nz) or t.dim() not in (4, 5):
+            raise ValueError(f"stiffness must have shape (21, {g.nx}, {g.ny}, {g.nz}) or (S,) + that")
+        self._stiffness = t
+        c0p = None
+        if c0 is not None:
+            self._c0 = np.ascontiguousarray(np.asarray(c0, dtype=np.float64).reshape(21))
+            c0p = self._c0.ctypes.data_as(_lib.c_double_p)
+        _lib.check(self._lib.lsb_set_anisotropic(self._h, ctypes.c_void_p(t.data_ptr()),
+                                                 t.element_size(), c0p), "lsb_set_anisotropic")
+
     def set_graphs(self, on=True):
         """Replay each iteration as a CUDA graph (default) or launch kernel by kernel."""
         _lib.check(self._lib.lsb_set_graphs(self._h, 1 if on else 0), "lsb_set_graphs")

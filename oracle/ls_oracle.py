@@ -253,7 +253,7 @@ def lame_reference(lmbda, mu):
 
 def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, depth=0,
                        maxiter=32, dtype=np.float32, spectrum="half", workers=None,
-                       epsilon0=None, history=None, xizero_fn=None, stress=None):
+                       epsilon0=None, history=None, xizero_fn=None, stress=None, gamma=None):
     """Moulinec-Suquet fixed point with Anderson acceleration of depth ``depth``
     (``src/jaxmaterials/solver/lippmann_schwinger.py:146-265``).
 
@@ -263,7 +263,8 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
     ``history``, if a list, receives the criterion value after every evaluation.
     ``xizero_fn(grid, dtype)`` replaces ``get_xizero`` (e.g. ``get_xizero_cuda32`` for
     the reference CUDA library's construction). ``stress(lmbda, mu, eps)`` replaces the
-    linear law (the damage extension's ``elasticity_solve``, lippmann_schwinger.py:330-455).
+    linear law (the damage extension's ``elasticity_solve``, lippmann_schwinger.py:330-455);
+    ``gamma(sigma_hat, xizero)`` replaces the isotropic Gamma^0 (the anisotropic extension).
 
     Returns ``(epsilon, sigma, iterations)`` with sigma = sigma(epsilon); the loop stops
     when e <= atol or e <= rtol * e0 (e0 at the first iterate) or after maxiter updates.
@@ -317,7 +318,9 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
     it = 0
     scale = np.array([1.0, 1.0, 1.0, 2.0, 2.0, 2.0], dtype=dtype)
     while e > atol and e > rtol * e0 and it < maxiter:
-        r = np.asarray(inv(fourier_solve(sigma_hat, lmbda0, mu0, xizero)), dtype=dtype)
+        r_hat = (gamma(sigma_hat, xizero) if gamma is not None
+                 else fourier_solve(sigma_hat, lmbda0, mu0, xizero))
+        r = np.asarray(inv(r_hat), dtype=dtype)
         res = np.roll(res, 1, axis=0)
         res[0] = r
         a_mat = np.roll(a_mat, (1, 1), axis=(0, 1))
