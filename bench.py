@@ -50,6 +50,8 @@ def parse():
                    help="samples of the layered-fibre dataset generator leg (0: skip)")
     p.add_argument("--damage", type=int, default=128,
                    help="grid of the phase-field fracture step leg (0: skip)")
+    p.add_argument("--aniso", type=int, default=128,
+                   help="grid of the anisotropic C_eff leg (0: skip)")
     return p.parse_args()
 
 
@@ -113,6 +115,29 @@ def damage_run(n):
                          "kind": "port", "sample": f"3 damaged Anderson updates at {m}^3 "
                          "(oracle, FP32 fields, SciPy FFT on all cores)"},
     })
+    return res
+
+
+def aniso_run(n):
+    """C_eff of a two-phase anisotropic n^3 field through
+    jaxmaterials_b200.solver.anisotropic.benchmark, beside the oracle's NumPy iteration of
+    the same law (the derivation restated; the reference has no solver for it) on a bounded
+    sample as the CPU baseline."""
+    from jaxmaterials_b200.solver.anisotropic import benchmark, two_phase_stiffness
+    from oracle import aniso_oracle as A
+    from oracle import ls_oracle as O
+
+    res = benchmark(n)
+    m = 48
+    c = two_phase_stiffness(m, 1)
+    t = time.perf_counter()
+    A.lippmann_schwinger(c, np.eye(6)[0], O.Grid(m, m, m, float(m), float(m), float(m)),
+                         rtol=0.0, atol=0.0, depth=5, maxiter=3, dtype=np.float32)
+    per_vi = (time.perf_counter() - t) / (4 * m ** 3)
+    res["cpu_baseline"] = {"value": 1.0 / per_vi, "unit": "voxel-iterations/s",
+                           "cores": os.cpu_count(), "kind": "port",
+                           "sample": f"3 anisotropic Anderson updates of one load at {m}^3 "
+                                     "(oracle, FP32 fields, SciPy FFT on all cores)"}
     return res
 
 
@@ -540,6 +565,14 @@ def own_arm(args):
         except Exception as exc:  # reported in the line; the solver figures stand
             damage = {"error": f"{type(exc).__name__}: {exc}"}
 
+    aniso = None
+    if args.aniso > 0 and world == 1:
+        torch.cuda.empty_cache()
+        try:
+            aniso = aniso_run(args.aniso)
+        except Exception as exc:  # reported in the line; the solver figures stand
+            aniso = {"error": f"{type(exc).__name__}: {exc}"}
+
     ref = fixture_c_eff(args.depth if args.depth in (0, 5) else 5)
     c_eff_err = (float(np.linalg.norm(c_eff - ref) / np.linalg.norm(ref))
                  if ref is not None and rank == 0 else None)
@@ -566,6 +599,7 @@ def own_arm(args):
             "batched": batched,
             "generator": generator,
             "damage": damage,
+            "anisotropic": aniso,
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "c_eff_rel_err_vs_fp64": c_eff_err,
             "gpu_launches": int(launches),
