@@ -11,6 +11,7 @@
 // size and for FP64 fields.
 #include <cmath>
 
+#include "aniso.cuh"
 #include "damage.cuh"
 #include "fast_passes.cuh"
 #include "fft_smem.cuh"
@@ -174,7 +175,9 @@ __host__ __device__ constexpr int x_region() {
   return XSplit<NX>::E * x_row<NX, T>() > NX * T ? XSplit<NX>::E * x_row<NX, T>() : NX * T;
 }
 
-template <int NX, int V>
+// ANI: Gamma^0 of an anisotropic reference stiffness (aniso.cuh) instead of the isotropic
+// closed form.
+template <int NX, int V, bool ANI>
 __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_blocks<NX, V>()) xpass_fast(
     GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
     InstanceState* __restrict__ st, double* __restrict__ partials) {
@@ -291,6 +294,33 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
     // normalised wave vector: |xi| < 1e-12 (|xi|^2 < 1e-24) is replaced by 1 (fourier.py:84)
     const double n2 = x0 * x0 + x1 * x1 + x2 * x2;
     const double inv = n2 < 1.0e-24 ? 1.0 : rsqrt(n2);
+    if constexpr (ANI) {
+      // r = -Gamma^0 tau through the inverse acoustic matrix (FP64 per mode); modes without a
+      // direction get r = 0
+      const double zd[3] = {x0 * inv, x1 * inv, x2 * inv};
+      double nd[6];
+      float o[2][6];
+      if (!(n2 < 1.0e-24) &&
+          aniso_inverse_acoustic(g.c0 + (size_t)(b / g.lame_group) * 21, zd, nd)) {
+        const float zt[3] = {(float)zd[0], (float)zd[1], (float)zd[2]};
+        float nt[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) nt[k] = (float)nd[k];
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          float tv[6];
+#pragma unroll
+          for (int cc = 0; cc < 6; ++cc) tv[cc] = part ? s[cc].y : s[cc].x;
+          aniso_gamma<float>(nt, zt, tv, o[part]);
+        }
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < 6; ++cc) o[0][cc] = o[1][cc] = 0.f;
+      }
+#pragma unroll
+      for (int cc = 0; cc < 6; ++cc) buf[(size_t)cc * REG + kx * T + tt] = make_float2(o[0][cc], -o[1][cc]);
+      continue;
+    }
     const float z0 = (float)(x0 * inv), z1 = (float)(x1 * inv), z2 = (float)(x2 * inv);
     const float z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
     const float z01 = z0 * z1, z02 = z0 * z2, z12 = z1 * z2;
@@ -459,7 +489,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 // (not rewritten), 3 Anderson residual into the rings.
 // bulk: the block's global chunks are 16-byte aligned (TMA bulk copies); otherwise the
 // staging buffers are filled by ordinary loads.
-template <int NZ, bool DMG>
+// LAW: 0 isotropic (lambda, mu staged), 1 damage extension, 2 anisotropic stiffness (21
+// entries read per voxel from global memory; lambda and mu not staged).
+template <int NZ, int LAW>
 __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fast(
     GridDesc g, int mode, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
@@ -487,7 +519,7 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
   med += b / g.lame_group;
   const bool need_r = (mode == 1 || mode == 3);
   const bool need_e = (mode == 1 || mode == 2 || mode == 3);
-  const bool need_l = (mode != 3);
+  const bool need_l = (mode != 3) && LAW != 2;
 
   // ---- stage this block's inputs in shared memory
   if (bulk) {
@@ -589,6 +621,13 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
 #pragma unroll
     for (int c = 0; c < 6; ++c)
       shift[c] = (float)((c < 3 ? med->lmean * tr : 0.0) + 2.0 * med->mmean * e[c]);
+    if constexpr (LAW == 2) {  // anisotropic: C^0 eps_bar
+      const double* c0 = g.c0 + (size_t)(b / g.lame_group) * 21;
+      double sh[6];
+      aniso_stress<double>([&](int k) { return c0[k]; }, e, sh);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) shift[c] = (float)sh[c];
+    }
     if (blockIdx.x == 0 && tid == 0) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) st[b].shift[c] = (double)shift[c];
@@ -623,7 +662,10 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
         for (int c = 0; c < 6; ++c) eb[(size_t)c * g.nv + vx] = e[c];
       }
       float s[6];
-      if constexpr (DMG) {
+      if constexpr (LAW == 2) {
+        const float* cfb = g.cf32 + (size_t)(b / g.lame_group) * 21 * g.nv + vx;
+        aniso_stress<float>([&](int k) { return cfb[(size_t)k * g.nv]; }, e, s);
+      } else if constexpr (LAW == 1) {
         // the damage extension's law (damage field read per voxel, not staged)
         const float om = 1.f - g.dmg32[(size_t)(b / g.lame_group) * g.nv + vx];
         damaged_stress<float>(e, lst[idx], lst[L * NZ + idx], om * om + (float)g.dmg_k, s);
@@ -697,13 +739,15 @@ static size_t xsmem() {
 
 template <int N>
 static cudaError_t configure_n() {
-  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(zpass_fast<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(xpass_fast<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(xpass_fast<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
+  const int zs = (int)zsmem<N>();
+  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
+  return e;
 }
 
 cudaError_t configure() {
@@ -726,12 +770,15 @@ static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda,
   dim3 grid((unsigned)z_blocks_for<N>(g), batch);
   // every chunk offset is a multiple of 16 bytes when the base pointers are
   const int bulk = aligned16(lambda) && aligned16(mu) && aligned16(eps) && aligned16(spec) ? 1 : 0;
-  if (g.dmg32)
-    zpass_fast<N, true><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
-                                                                eps_bar, eps0, st, med, aa);
+  if (g.cf32)
+    zpass_fast<N, 2><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                             eps_bar, eps0, st, med, aa);
+  else if (g.dmg32)
+    zpass_fast<N, 1><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                             eps_bar, eps0, st, med, aa);
   else
-    zpass_fast<N, false><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
-                                                                 eps_bar, eps0, st, med, aa);
+    zpass_fast<N, 0><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                             eps_bar, eps0, st, med, aa);
 }
 
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
@@ -789,8 +836,11 @@ template <int N, int V>
 static void xlaunch(const GridDesc& g, int batch, float2* spec, const Medium* med, InstanceState* st,
                     double* partials, cudaStream_t s) {
   dim3 grid(x_blocks<N>(g, V), g.ny, batch);
-  xpass_fast<N, V><<<grid, 6 * XSplit<N>::P * x_cols_v<N, V>(), xsmem<N, V>(), s>>>(g, spec, med, st,
-                                                                                  partials);
+  const int threads = 6 * XSplit<N>::P * x_cols_v<N, V>();
+  if (g.c0)
+    xpass_fast<N, V, true><<<grid, threads, xsmem<N, V>(), s>>>(g, spec, med, st, partials);
+  else
+    xpass_fast<N, V, false><<<grid, threads, xsmem<N, V>(), s>>>(g, spec, med, st, partials);
 }
 
 template <int N>

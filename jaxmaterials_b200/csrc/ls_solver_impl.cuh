@@ -129,8 +129,8 @@ int structures_of(lsb_solver* s, int batch);
 // Points s->g at the anisotropic stiffness of lsb_set_anisotropic (both precisions) and
 // its reference stiffness C^0 for a solve over nstruct structures (aniso.cu).
 int prepare_aniso(lsb_solver* s, int nstruct);
-// The compile-time-size FP32 passes apply (every extent supported, isotropic law).
-inline bool use_fast32(const lsb_solver* s) { return s->fast32 && s->g.cf32 == nullptr; }
+// The compile-time-size FP32 passes apply (every extent supported).
+inline bool use_fast32(const lsb_solver* s) { return s->fast32; }
 // Full FP32-input solve (see lsb_solve); d_eps is the FP32 work buffer and output.
 int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
               const double* eps_bar, const float* d_eps0, float* d_eps, float* d_sigma,

@@ -37,8 +37,9 @@ def test_fixed_iterations_match_oracle_fp64(n, depth):
 
 @pytest.mark.parametrize("n", [(12, 10, 8), (32, 16, 16)])
 def test_fp32_matches_oracle(n):
-    """FP32 fields (on a power-of-two grid the solver leaves its compile-time-size passes for
-    the generic ones) after equal updates, and converged to the same solution."""
+    """FP32 fields (generic passes on the first grid, the compile-time-size passes' anisotropic
+    variants on the power-of-two one) after equal updates, and converged to the same
+    solution."""
     from jaxmaterials_b200 import GridSpec
     from jaxmaterials_b200.solver.anisotropic import lippmann_schwinger_anisotropic
     from oracle import aniso_oracle as A
@@ -78,8 +79,7 @@ def test_isotropic_stiffness_equals_isotropic_solver(n):
 
 
 def test_solver_returns_to_the_isotropic_law():
-    """A solver that ran an anisotropic solve gives the isotropic results afterwards (and its
-    compile-time-size passes again)."""
+    """A solver that ran an anisotropic solve gives the isotropic results afterwards."""
     import torch
 
     from jaxmaterials_b200 import GridSpec
