@@ -100,3 +100,21 @@ def test_solver_returns_to_the_isotropic_law():
     assert np.array_equal(r1.epsilon.cpu().numpy(), e0)
     s.close()
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("n", [(12, 10, 8), (32, 16, 16)])
+def test_grouped_structures_equal_separate_solves(n):
+    """Two structures x six loads in one batch (instance b reads structure b // 6, each with its
+    own C^0) give the same fields as separate solves."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver.anisotropic import lippmann_schwinger_anisotropic
+
+    g = GridSpec(*n, 1.0, 0.9, 0.8)
+    c = np.stack([two_phase_field(n, seed=1), two_phase_field(n, seed=2) * 1.7])
+    eb = np.tile(np.eye(6) * 1e-3, (2, 1))
+    e, s, it = lippmann_schwinger_anisotropic(c, eb, g, rtol=1e-6, depth=3, maxiter=300)
+    for k in range(2):
+        e1, s1, it1 = lippmann_schwinger_anisotropic(c[k], np.eye(6) * 1e-3, g, rtol=1e-6,
+                                                     depth=3, maxiter=300)
+        assert np.array_equal(it[6 * k:6 * k + 6], it1)
+        assert np.array_equal(e[6 * k:6 * k + 6], e1)

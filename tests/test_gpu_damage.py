@@ -185,3 +185,30 @@ def test_phase_field_matches_oracle(shape, dtype, tol):
                                   maxiter=500)
     assert abs(it - itr) <= (0 if dtype == np.float64 else 2)
     assert np.abs(d - dr).max() <= tol * np.abs(dr).max()
+
+
+def test_grouped_damage_fields_equal_separate_solves():
+    """Damage fields of shape (S, nx, ny, nz) follow the Lame grouping: two structures x two
+    loads in one batch equal separate solves."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import Solver
+
+    rng = np.random.default_rng(9)
+    n = (32, 16, 16)
+    g = GridSpec(*n, 1.0, 0.5, 0.5)
+    lm = (1.0 + rng.uniform(-0.3, 0.3, (2,) + n)).astype(np.float32)
+    mu = (1.0 + rng.uniform(-0.3, 0.3, (2,) + n)).astype(np.float32)
+    d = np.clip(rng.uniform(-0.5, 1.2, (2,) + n), 0, 1).astype(np.float32)
+    eb = np.array([[0, 1e-3, 0, 0, 0, 0], [1e-3, 0, 0, 0, 2e-4, 0]] * 2, dtype=np.float32)
+    s = Solver(g, batch=4, depth=3)
+    s.set_damage(d, 1e-6)
+    r = s.solve(lm, mu, eb, rtol=1e-6, maxiter=300)
+    e = r.epsilon.cpu().numpy()
+    for k in range(2):
+        s1 = Solver(g, batch=2, depth=3)
+        s1.set_damage(d[k], 1e-6)
+        r1 = s1.solve(lm[k], mu[k], eb[2 * k:2 * k + 2], rtol=1e-6, maxiter=300)
+        assert np.array_equal(r.iters[2 * k:2 * k + 2], r1.iters)
+        assert np.array_equal(e[2 * k:2 * k + 2], r1.epsilon.cpu().numpy())
+        s1.close()
+    s.close()
