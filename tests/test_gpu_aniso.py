@@ -35,7 +35,7 @@ def test_fixed_iterations_match_oracle_fp64(n, depth):
     assert relmax(s, s64) < 1e-10
 
 
-@pytest.mark.parametrize("n", [(12, 10, 8), (32, 16, 16)])
+@pytest.mark.parametrize("n", [(12, 10, 8), (32, 16, 16), (48, 96, 32)])
 def test_fp32_matches_oracle(n):
     """FP32 fields (generic passes on the first grid, the compile-time-size passes' anisotropic
     variants on the power-of-two one) after equal updates, and converged to the same
