@@ -52,7 +52,41 @@ def parse():
                    help="grid of the phase-field fracture step leg (0: skip)")
     p.add_argument("--aniso", type=int, default=128,
                    help="grid of the anisotropic C_eff leg (0: skip)")
+    p.add_argument("--c2-256", type=int, default=1, dest="c2_256",
+                   help="steps of the 256^3 config-2 leg (0: skip)")
+    p.add_argument("--comparators", type=int, default=1,
+                   help="time the cuFFT loop and the reference's CUDA library (0: skip)")
+    # fixed-iteration runs for profilers (no JSON line): every pass of every iteration does
+    # its full work (tolerances 0), on the seeded n^3 benchmark composite
+    p.add_argument("--profile-case", action="store_true",
+                   help="run --iters iterations of --batch load cases at --n^3 and exit")
+    p.add_argument("--n", type=int, default=128)
+    p.add_argument("--batch", type=int, default=2)
+    p.add_argument("--iters", type=int, default=3)
+    p.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"])
     return p.parse_args()
+
+
+def profile_case(args):
+    """A fixed number of iterations (tolerances 0) of `--batch` unit loads on the seeded
+    n^3 cross-ply composite (4 layers, r = 4, vf 0.45), for ncu launch lists and captures."""
+    import torch
+
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+    from jaxmaterials_b200.solver import Solver
+
+    n = args.n
+    st = fibres.generate_layered_fibres(n, 4, 4.0, 0.45, seed=0)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(n, n, n, float(n), float(n), float(n))
+    s = Solver(g, batch=args.batch, depth=args.depth, precision=args.precision)
+    eb = np.eye(6, dtype=np.float32)[np.arange(args.batch) % 6]
+    r = s.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=args.iters, want_sigma=False)
+    torch.cuda.synchronize()
+    print(f"n={n} batch={args.batch} depth={args.depth} iters={list(r.iters)} "
+          f"launches={s.kernel_launches()}")
+    s.close()
 
 
 def generator_run(count, seed):
@@ -337,6 +371,262 @@ def cpu_sample(lm, mu, g, depth, budget_s, threads):
     return total_t / (total_it * g.number_of_voxels), total_it
 
 
+def kernel_bytes(name, nv, nm, batch, depth):
+    """Algorithmic bytes of one launch of the named kernel over `batch` instances of one
+    structure (FP32 fields: real field 6 Nv 4 B, half spectrum 6 Nm 8 B, Lame pair 2 Nv 4 B;
+    every Anderson ring slot filled)."""
+    real, spec, lame = 6 * nv * 4, 6 * nm * 8, 2 * nv * 4
+    m1 = depth + 1
+    table = {
+        "x pass": batch * 2 * spec,                          # spectrum read + write
+        "finalize": 0,
+        "y pass inverse": batch * 2 * spec,
+        "y pass forward": batch * 2 * spec,
+        "z pass update": batch * (2 * spec + 2 * real) + lame,  # spectrum r/w, eps r/w
+        "z pass residual rings": batch * (spec + real + 2 * real),  # spectrum, eps in; r, g out
+        "anderson gram": batch * m1 * real,                  # every r slot
+        "anderson solve": 0,
+        "anderson combine": batch * (m1 * real + real),      # every g slot in, eps out
+        "z pass stress": batch * (real + spec) + lame,        # eps in, spectrum out
+    }
+    if name not in table:
+        raise KeyError(f"no algorithmic byte count for kernel {name!r}")
+    return table[name]
+
+
+def step_roofline(solver, lm_d, mu_d, g, batch, depth, workload):
+    """Every launch of one iteration of the timed step (CUDA events on the solver's stream,
+    full workload), its algorithmic bytes and fraction of the measured HBM peak; the
+    dominant launch is the line's roofline kernel."""
+    prof = solver.profile_step(lm_d, mu_d, batch=batch, reps=5)
+    nv, nm = g.number_of_voxels, g.number_of_modes
+    peak, peak_kind = measured_peak()
+    traffic_tab = {}
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic_tab = json.load(f)
+    kernels = []
+    for name, ms in prof:
+        b = kernel_bytes(name, nv, nm, batch, depth)
+        gbs = b / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+        kernels.append({"kernel": name, "ms": ms, "algorithmic_bytes": b, "GBs": gbs,
+                        "frac": gbs / peak, "traffic": traffic_tab.get(f"{workload}:{name}")})
+    top = max(kernels, key=lambda k: k["ms"])
+    step_ms = sum(k["ms"] for k in kernels)
+    step_bytes = sum(k["algorithmic_bytes"] for k in kernels)
+    survey_b = 152.0 if depth == 0 else 200.0 + 72.0 * depth
+    return {
+        "bound": "hbm",
+        "kernel": top["kernel"],
+        "achieved": top["GBs"],
+        "peak": peak,
+        "peak_source": peak_kind,
+        "unit": "GB/s",
+        "frac": top["frac"],
+        "traffic": top["traffic"],
+        "algorithmic_bytes_per_launch": top["algorithmic_bytes"],
+        "ms_per_launch": top["ms"],
+        "step": {"ms": step_ms, "algorithmic_bytes": step_bytes,
+                 "bytes_per_voxel_iter": step_bytes / (nv * batch),
+                 "GBs": step_bytes / (step_ms / 1000.0) / 1e9,
+                 "frac": step_bytes / (step_ms / 1000.0) / 1e9 / peak,
+                 "survey_bytes_per_voxel_iter": survey_b,
+                 "frac_at_survey_bytes": survey_b * nv * batch / (step_ms / 1000.0) / 1e9 / peak},
+        "kernels": kernels,
+    }
+
+
+def ceff_run(g, lm_d, mu_d, depth, steps, warmup, maxiter=5000, precision="mixed"):
+    """`steps` timed six-load C_eff solves (CUDA events on the current stream) after
+    `warmup` untimed ones; returns the figures and the last result."""
+    import torch
+    from jaxmaterials_b200.solver import CONVERGED, Solver
+
+    eye = np.eye(6, dtype=np.float32)
+    s = Solver(g, batch=6, depth=depth, precision=precision)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        r = s.solve(lm_d, mu_d, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    its, f64 = 0, 0
+    t0.record(stream)
+    for _ in range(steps):
+        r = s.solve(lm_d, mu_d, eye, rtol=1e-6, atol=1e-20, maxiter=maxiter, want_sigma=False)
+        its += int(r.iters.sum())
+        f64 += int(s.fp64_iters().sum())
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    nv = g.number_of_voxels
+    out = {"value": 6.0 * steps / (ms / 1000.0), "unit": "solves/s",
+           "ms_per_step": ms / steps, "iters_per_solve": its / (6 * steps),
+           "voxel_iter_per_s": its * nv / (ms / 1000.0),
+           "fp64_iteration_share": f64 / its if its else 0.0,
+           "all_converged": bool(np.all(r.status == CONVERGED))}
+    return out, r, s
+
+
+def c2_256_run(steps):
+    """Config 2's 256^3 grid (4 layers, r = 4, vf 0.45, six unit loads, tol 1e-6):
+    Anderson m = 5 and plain, each with its C_eff error against an FP64 Anderson solve of
+    the same structure by the library's FP64 path (lsb_solve_f64), and against the FP64
+    CPU oracle's C_eff where tests/golden/bench_c2_256.npz holds it."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.data import fibres
+    from jaxmaterials_b200.solver import Solver
+
+    st = fibres.config_structure("c2_256", seed=0)
+    lm, mu = fibres.lame_fields(st)
+    g = GridSpec(*st.n, *st.extents)
+    lm_d = torch.as_tensor(lm, device="cuda")
+    mu_d = torch.as_tensor(mu, device="cuda")
+    res = {"workload": f"c2_256: 256^3 cross-ply, 4 layers, r = 4, vf {st.volume_fraction:.3f}, "
+                       "6 unit loads, tol 1e-6, FP32 fields (mixed precision)",
+           "timing": "CUDA events around the timed steps, inputs resident in HBM"}
+    s64 = Solver(g, batch=6, depth=5, precision="fp64")
+    lm64 = lm_d.double()
+    mu64 = mu_d.double()
+    r64 = s64.solve(lm64, mu64, np.eye(6), rtol=1e-6, atol=1e-20, maxiter=5000, want_sigma=False)
+    c64 = np.asarray(r64.mean_sigma, np.float64)
+    res["fp64_iters_per_solve"] = float(np.mean(r64.iters))
+    s64.close()
+    del lm64, mu64
+    torch.cuda.empty_cache()
+    ref_oracle = None
+    path = os.path.join(ROOT, "tests", "golden", "bench_c2_256.npz")
+    if os.path.exists(path):
+        ref_oracle = np.load(path)["ceff_d5"]
+    for depth, key in ((5, "anderson"), (0, "plain")):
+        out, r, s = ceff_run(g, lm_d, mu_d, depth, steps, 1)
+        c = np.asarray(r.mean_sigma, np.float64)
+        out["c_eff_rel_err_vs_fp64_gpu"] = float(np.linalg.norm(c - c64) / np.linalg.norm(c64))
+        if ref_oracle is not None:
+            out["c_eff_rel_err_vs_fp64_oracle"] = float(
+                np.linalg.norm(c - ref_oracle) / np.linalg.norm(ref_oracle))
+        if depth == 5:
+            out["roofline"] = step_roofline(s, lm_d, mu_d, g, 6, depth, "c2_256")
+            out["roofline"].pop("kernels")
+        s.close()
+        torch.cuda.empty_cache()
+        res[key] = out
+    if ref_oracle is not None:
+        res["fp64_gpu_vs_oracle"] = float(np.linalg.norm(c64 - ref_oracle) / np.linalg.norm(ref_oracle))
+    return res
+
+
+def comparators_run(g, lm, mu, lm_d, mu_d, plain_iters, plain_ms_per_iter):
+    """The same 128^3 six-load workload on (a) this solver's plain loop with its FFT stages
+    replaced by cuFFT R2C/C2R batch 6 (libcufft_comparator.so: the pointwise kernels are
+    this project's), and (b) the reference's own CUDA library (cuFFT + its SIMT kernels,
+    built from its sources into oracle/_ref, called through its C ABI with host buffers,
+    lambda first), against this solver's plain iteration."""
+    import ctypes
+
+    import torch
+
+    out = {"own_plain_ms_per_iter": plain_ms_per_iter}
+    lib_path = os.path.join(ROOT, "jaxmaterials_b200", "libcufft_comparator.so")
+    try:
+        lib = ctypes.CDLL(lib_path)
+        lib.cmp_cufft_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_int]
+        lib.cmp_cufft_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.cmp_cufft_destroy.argtypes = [ctypes.c_void_p]
+        lib.cmp_cufft_last_error.restype = ctypes.c_char_p
+        h = ctypes.c_void_p()
+        vox = np.array(g.shape, np.int32)
+        ext = np.array([g.Lx, g.Ly, g.Lz], np.float64)
+        if lib.cmp_cufft_create(ctypes.byref(h), vox.ctypes.data, ext.ctypes.data, 6) != 0:
+            raise RuntimeError(lib.cmp_cufft_last_error().decode())
+        eps = torch.empty((6, 6) + g.shape, dtype=torch.float32, device="cuda")
+        eb = np.eye(6, dtype=np.float64)
+        l0 = 0.5 * (float(lm.min()) + float(lm.max()))
+        m0 = 0.5 * (float(mu.min()) + float(mu.max()))
+        ms = np.zeros(1, np.float32)
+        crit = np.zeros(6)
+        mean = np.zeros((6, 6))
+        iters = int(round(plain_iters))
+        torch.cuda.synchronize()
+        for rep in range(2):  # the first run warms up the plans
+            rc = lib.cmp_cufft_run(h, ctypes.c_void_p(lm_d.data_ptr()), ctypes.c_void_p(mu_d.data_ptr()),
+                                   6, eb.ctypes.data, l0, m0, ctypes.c_void_p(eps.data_ptr()),
+                                   iters if rep else 4, ms.ctypes.data, crit.ctypes.data,
+                                   mean.ctypes.data)
+            if rc != 0:
+                raise RuntimeError(lib.cmp_cufft_last_error().decode())
+        lib.cmp_cufft_destroy(h)
+        ref = fixture_c_eff(0)
+        out["cufft_loop"] = {
+            "ms_per_iter": float(ms[0]), "iterations": iters,
+            "solves_per_s_at_own_plain_iters": 6.0 / (float(ms[0]) * plain_iters / 1000.0),
+            "own_speedup_per_iter": float(ms[0]) / plain_ms_per_iter,
+            "last_relative_criterion": [float(c) for c in crit],
+            "c_eff_rel_err_vs_fp64_oracle": (float(np.linalg.norm(mean - ref) / np.linalg.norm(ref))
+                                             if ref is not None else None),
+            "what": "stress kernel, cufftExecR2C batch 36, Gamma^0 + FP64 criterion kernel, "
+                    "cufftExecC2R batch 36, update kernel; fixed iteration count, CUDA events",
+        }
+    except Exception as exc:  # reported in the line; the solver figures stand
+        out["cufft_loop"] = {"error": f"{type(exc).__name__}: {exc}"}
+    ref_lib = os.path.join(ROOT, "oracle", "_ref", "liblippmannschwinger.so")
+    if not os.path.exists(ref_lib):
+        out["reference_cuda_library"] = {"unavailable": "oracle/_ref/liblippmannschwinger.so not built"}
+        return out
+    try:
+        rl = ctypes.CDLL(ref_lib)
+        F = ctypes.POINTER(ctypes.c_float)
+        rl.lippmann_schwinger_solve.argtypes = [F, F, F, F, F, ctypes.POINTER(ctypes.c_int), F,
+                                                ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                                ctypes.c_int]
+        rl.lippmann_schwinger_solve.restype = ctypes.c_int
+        lmc = np.ascontiguousarray(lm, np.float32)
+        muc = np.ascontiguousarray(mu, np.float32)
+        eps_h = np.empty((6,) + g.shape, np.float32)
+        sig_h = np.empty_like(eps_h)
+        vox = np.array(g.shape, np.int32)
+        ext = np.array([g.Lx, g.Ly, g.Lz], np.float32)
+        maxiter = int(round(plain_iters)) + 40
+        p = lambda a: a.ctypes.data_as(F)
+        times, its, means = [], [], []
+        for k in range(6):
+            eb = np.zeros(6, np.float32)
+            eb[k] = 1.0
+            t = time.perf_counter()
+            it = rl.lippmann_schwinger_solve(p(lmc), p(muc), p(eb), p(eps_h), p(sig_h),
+                                             vox.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                             p(ext), 1e-6, 1e-20, maxiter, 0)
+            times.append(time.perf_counter() - t)
+            its.append(int(it))
+            means.append(sig_h.astype(np.float64).mean(axis=(1, 2, 3)))
+        ref = fixture_c_eff(0)
+        c = np.array(means)
+        sec = float(np.sum(times))
+        out["reference_cuda_library"] = {
+            "solves_per_s": 6.0 / sec,
+            "ms_per_iter": 1000.0 * sec / max(1, sum(its)),
+            "iters": its,
+            "converged": [i < maxiter for i in its],
+            "maxiter": maxiter,
+            "own_speedup_per_iter": 1000.0 * sec / max(1, sum(its)) / plain_ms_per_iter,
+            "c_eff_rel_err_vs_fp64_oracle": (float(np.linalg.norm(c - ref) / np.linalg.norm(ref))
+                                             if ref is not None else None),
+            "what": "reference lippmann_schwinger_solve (cuFFT + SIMT kernels, per-call plans "
+                    "and allocations, host buffers), one call per load case, lambda first, "
+                    "rtol 1e-6; wall clock per call; its FP32 iteration may stall above 1e-6 "
+                    "and then runs to maxiter",
+        }
+    except Exception as exc:
+        out["reference_cuda_library"] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -435,9 +725,11 @@ def own_arm(args):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
+    fp64_iters = 0
     for _ in range(args.steps):
         r = step(lm_d, mu_d)
         iters_total += int(r.iters.sum())
+        fp64_iters += int(s.fp64_iters().sum())
         c_eff = r.mean_sigma
     t1.record(stream)
     barrier()
@@ -468,8 +760,10 @@ def own_arm(args):
         pms = float(pms.item())
         plain = {"value": 6.0 * args.steps * world / (pms / 1000.0), "unit": "solves/s",
                  "iters_per_solve": pits / (6 * args.steps),
+                 "ms_per_iteration": pms / args.steps / (pits / (6 * args.steps)),
                  "voxel_iter_per_s": pits * world * g.number_of_voxels / (pms / 1000.0),
                  "all_converged": bool(np.all(rp.status == CONVERGED))}
+        plain["roofline"] = step_roofline(sp_, lm_d, mu_d, g, 6, 0, WORKLOAD)
         sp_.close()
     ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
     it_t = torch.tensor([iters_total], device=dev, dtype=torch.float64)
@@ -500,29 +794,11 @@ def own_arm(args):
         dist.all_reduce(ems, op=dist.ReduceOp.MAX)
     e2e = 6.0 * args.steps * world / (float(ems.item()) / 1000.0)
 
-    # ---- per-pass timing for the roofline (same stream, CUDA events, full workload); the
-    # passes shared by the plain and the Anderson iteration
-    passes = s.profile_passes(lm_d, mu_d, batch=6, reps=5)
-    nv, nm, b = g.number_of_voxels, g.number_of_modes, 6
-    spec = 6 * nm * 8
-    real = 6 * nv * 4
-    alg = {
-        "xpass": b * 2 * spec,
-        "ypass_inverse": b * 2 * spec,
-        "ypass_forward": b * 2 * spec,
-        "zpass": b * (2 * spec + 2 * real) + 2 * nv * 4,
-        "finalize": 0,
-    }
-    top = max(passes, key=passes.get)
-    peak, peak_kind = measured_peak()
-    achieved = alg[top] / (passes[top] / 1000.0) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            traffic = json.load(f).get(f"{WORKLOAD}:{top}")
-    loop_ms = sum(passes.values())
-    loop_gbs = 152.0 * nv * b / (loop_ms / 1000.0) / 1e9
+    # ---- every launch of one iteration of the timed step, for the roofline (same stream,
+    # CUDA events, full workload)
+    roof = step_roofline(s, lm_d, mu_d, g, 6, args.depth, WORKLOAD)
+    nv = g.number_of_voxels
+    fp64_share = fp64_iters / max(1, iters_total)
 
     s.close()
     batched = None
@@ -573,6 +849,23 @@ def own_arm(args):
         except Exception as exc:  # reported in the line; the solver figures stand
             aniso = {"error": f"{type(exc).__name__}: {exc}"}
 
+    comparators = None
+    if args.comparators > 0 and world == 1 and plain is not None:
+        torch.cuda.empty_cache()
+        try:
+            comparators = comparators_run(g, lm, mu, lm_d, mu_d, plain["iters_per_solve"],
+                                          plain["ms_per_iteration"])
+        except Exception as exc:  # reported in the line; the solver figures stand
+            comparators = {"error": f"{type(exc).__name__}: {exc}"}
+
+    c2_256 = None
+    if args.c2_256 > 0 and world == 1:
+        torch.cuda.empty_cache()
+        try:
+            c2_256 = c2_256_run(args.c2_256)
+        except Exception as exc:  # reported in the line; the solver figures stand
+            c2_256 = {"error": f"{type(exc).__name__}: {exc}"}
+
     ref = fixture_c_eff(args.depth if args.depth in (0, 5) else 5)
     c_eff_err = (float(np.linalg.norm(c_eff - ref) / np.linalg.norm(ref))
                  if ref is not None and rank == 0 else None)
@@ -595,7 +888,10 @@ def own_arm(args):
             "voxel_iter_per_s": vips,
             "iters_per_solve": float(iters_total) / (6 * args.steps),
             "all_converged": converged,
+            "fp64_iteration_share": fp64_share,
             "plain": plain,
+            "c2_256": c2_256,
+            "comparators": comparators,
             "batched": batched,
             "generator": generator,
             "damage": damage,
@@ -603,21 +899,7 @@ def own_arm(args):
             "c_eff_diag": [float(c_eff[k, k]) for k in range(6)],
             "c_eff_rel_err_vs_fp64": c_eff_err,
             "gpu_launches": int(launches),
-            "roofline": {
-                "bound": "hbm",
-                "kernel": top,
-                "achieved": achieved,
-                "peak": peak,
-                "peak_source": peak_kind,
-                "unit": "GB/s",
-                "frac": achieved / peak,
-                "traffic": traffic,
-                "algorithmic_bytes_per_launch": alg[top],
-                "ms_per_launch": passes[top],
-                "passes_ms": passes,
-                "loop_at_152B_per_voxel_iter_GBs": loop_gbs,
-                "loop_frac_of_peak": loop_gbs / peak,
-            },
+            "roofline": roof,
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 2 * nv * 4,
                     "d2h_bytes_per_step": 36 * 8},
             "clocks": clocks.summary(),
@@ -643,7 +925,9 @@ def own_arm(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile_case:
+        profile_case(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         own_arm(args)

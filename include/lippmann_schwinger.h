@@ -56,7 +56,10 @@ enum {
   LSB_CONVERGED = 1,
   LSB_MAXITER = 2,
   LSB_NONFINITE = 3,
-  LSB_STALLED = 4 /* FP32 round-off floor above the tolerance (LSB_PREC_FP32 only) */
+  LSB_STALLED = 4, /* FP32 round-off floor above the tolerance (LSB_PREC_FP32 only) */
+  LSB_TIMEOUT = 5  /* a kernel's bounded wait for its own asynchronous copies ran out and the
+                    * instance was abandoned; the solver's device buffers are then suspect:
+                    * destroy the solver and create a new one */
 };
 
 /* Field precision of the iteration (norms and the stop decision are always FP64):
@@ -156,13 +159,22 @@ int lsb_history(lsb_solver *solver, double *out, int len);
 /* No reference counterpart: number of kernels this solver has enqueued so far. */
 long long lsb_kernel_launches(lsb_solver *solver);
 
-/* No reference counterpart: times every pass of one iteration with CUDA events on the
- * solver's stream, averaged over `reps` iterations that never stop (tolerances 0).
- * ms_out (host float[5]) = x pass (forward DFT, residual, Gamma^0, inverse DFT),
- * finalize, inverse y pass, z pass (C2R, update, stress, R2C), forward y pass.
- * d_eps (device float[batch*6*nv]) is used as the strain work buffer. */
-int lsb_profile_passes(lsb_solver *solver, int batch, const float *d_lambda,
-                       const float *d_mu, float *d_eps, int reps, float *ms_out);
+/* No reference counterpart: updates of each instance of the last solve that ran with FP64
+ * fields (after a mixed-precision switch, or all of them for an FP64 solve); out is host
+ * int[batch of that solve]. */
+int lsb_fp64_iters(lsb_solver *solver, int *out);
+
+/* No reference counterpart: times every kernel of one FP32 iteration, as the solve runs it
+ * (Anderson when the solver's depth > 0, plain otherwise), with CUDA events on the
+ * solver's stream, averaged over `reps` iterations that never stop (tolerances 0), after
+ * depth + 2 untimed iterations that fill the Anderson rings. Writes the mean milliseconds
+ * of each launch to ms_out (host float[max_kernels]) and their kernel names, comma
+ * separated, to names (host char[names_len]); returns the number of launches per
+ * iteration (or a negative error). d_eps (device float[batch*6*nv]) is the strain work
+ * buffer. */
+int lsb_profile_step(lsb_solver *solver, int batch, const float *d_lambda, const float *d_mu,
+                     float *d_eps, int reps, float *ms_out, int max_kernels, char *names,
+                     int names_len);
 
 /* Effective stiffness from the six unit macroscopic strains (the caller in
  * src/jaxmaterials/data/data.py:178-186): row k of c_eff (host double[36]) is the mean
@@ -193,17 +205,22 @@ int lsb_c_eff_batch(int nstruct, const int *voxels, const double *extents,
  * synchronisation. Inputs and outputs are the caller's (device pointers as in lsb_solve,
  * eps_bar host float[batch*6]); all other scratch comes from one static device array of
  * LSB_NOALLOC_SCRATCH_BYTES bytes per GPU, kept until the process exits (a 32^3 grid
- * with 6 load cases needs about 5.5 MB of it). Larger grids or batches are rejected with
- * an error. The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that call before any stream capture on the device. Every
- * call reuses the array: calls whose GPU work overlaps in time race and must not be
- * issued. FP32 fields, plain iteration, stop rule LSB_RULE_CUDA, FP32 stall detection
- * (status LSB_STALLED), no criterion history; runs on the legacy default stream. */
+ * with 6 load cases needs about 5.5 MB of it). Grids whose scratch does not fit, and
+ * batches above LSB_NOALLOC_MAX_BATCH instances, are rejected with an error. The first
+ * call on a device (and the first after its context was reset) looks up the array's
+ * address (cudaGetSymbolAddress); make that call before any stream capture on the device.
+ * All work is ordered on `stream` (the twiddle tables are uploaded on it, only when the
+ * grid differs from the previous call's), and the call returns once that stream has
+ * finished the solve. Every call reuses the array: calls whose GPU work overlaps in time
+ * race and must not be issued. FP32 fields, plain iteration, stop rule LSB_RULE_CUDA,
+ * FP32 stall detection (status LSB_STALLED), no criterion history. */
 #define LSB_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define LSB_NOALLOC_MAX_BATCH 64
 int lsb_solve_noalloc(const int voxels[3], const double extents[3], int batch,
                       const float *d_lambda, const float *d_mu, const float *eps_bar,
                       float *d_eps, float *d_sigma, double *mean_sigma, float rtol,
-                      float atol, int maxiter, int *iters, int *status, double *residual);
+                      float atol, int maxiter, int *iters, int *status, double *residual,
+                      void *stream);
 
 /* No reference counterpart (the reference differentiates only forward-mode through
  * JAX, src/driver.py:73-76). Gradient of a loss L of the effective stiffness M (row k =

@@ -53,15 +53,17 @@ SIGNATURES = {
                                      c_int_p, c_double_p]),
     "lsb_history": (ctypes.c_int, [c_void_p, c_double_p, ctypes.c_int]),
     "lsb_kernel_launches": (ctypes.c_longlong, [c_void_p]),
-    "lsb_profile_passes": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p,
-                                          ctypes.c_int, c_float_p]),
+    "lsb_fp64_iters": (ctypes.c_int, [c_void_p, c_int_p]),
+    "lsb_profile_step": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p,
+                                        ctypes.c_int, c_float_p, ctypes.c_int, ctypes.c_char_p,
+                                        ctypes.c_int]),
     "lsb_c_eff": (ctypes.c_int, [c_float_p, c_float_p, c_int_p, c_double_p, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_int, ctypes.c_int, c_double_p,
                                  c_int_p]),
     "lsb_solve_noalloc": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_int, c_void_p, c_void_p,
                                          c_float_p, c_void_p, c_void_p, c_double_p,
                                          ctypes.c_float, ctypes.c_float, ctypes.c_int, c_int_p,
-                                         c_int_p, c_double_p]),
+                                         c_int_p, c_double_p, c_void_p]),
     "lsb_ceff_gradient": (ctypes.c_int, [c_int_p, c_void_p, c_double_p, c_void_p, c_void_p,
                                          c_void_p]),
     "lsb_ceff_gradient_f64": (ctypes.c_int, [c_int_p, c_void_p, c_double_p, c_void_p, c_void_p,

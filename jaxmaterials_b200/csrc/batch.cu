@@ -32,16 +32,24 @@ struct Bucket {
   double voxels_total = 0.0;
 };
 
-// Device bytes one structure (6 instances) needs in a solver of the given configuration.
-size_t bytes_per_structure(long long nv, long long nm, int depth, int precision) {
-  const size_t inst32 = 24 * (size_t)nv + 48 * (size_t)nm +
-                        (depth > 0 ? 2 * (size_t)(depth + 1) * 24 * nv : 0) + 6 * 1024 * 8;
+// Device bytes one structure (6 instances) needs in a solver of the given configuration:
+// fields, spectra and Anderson rings, the criterion history (maxiter + 8 values per
+// instance), and upper bounds of the x-pass and Gram-row partials (one value per (ky, kz)
+// column and per (x, y) line and slot).
+size_t bytes_per_structure(const int v[3], int depth, int precision, int maxiter) {
+  const size_t nv = (size_t)v[0] * v[1] * v[2];
+  const size_t nm = (size_t)v[0] * v[1] * (v[2] / 2 + 1);
+  const size_t partials = 8 * ((size_t)v[1] * (v[2] / 2 + 1) +
+                               (depth > 0 ? (size_t)v[0] * v[1] * (depth + 1) : 0));
+  const size_t history = 8 * ((size_t)maxiter + 8);
+  const size_t inst32 = 24 * nv + 48 * nm + (depth > 0 ? 2 * (size_t)(depth + 1) * 24 * nv : 0) +
+                        6 * 1024 * 8 + partials + history;
   size_t inst64 = 0;
   if (precision != LSB_PREC_FP32) {
-    inst64 = 48 * (size_t)nv + 96 * (size_t)nm;
+    inst64 = 48 * nv + 96 * nm;
     if (precision == LSB_PREC_FP64 && depth > 0) inst64 += 2 * (size_t)(depth + 1) * 48 * nv;
   }
-  const size_t lame = 8 * (size_t)nv + (precision != LSB_PREC_FP32 ? 16 * (size_t)nv : 0);
+  const size_t lame = 8 * nv + (precision != LSB_PREC_FP32 ? 16 * nv : 0);
   return 6 * (inst32 + inst64) + lame;
 }
 
@@ -60,9 +68,8 @@ void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int prec
   };
   cudaSetDevice(device);
   const long long nv = (long long)bk.voxels[0] * bk.voxels[1] * bk.voxels[2];
-  const long long nm = (long long)bk.voxels[0] * bk.voxels[1] * (bk.voxels[2] / 2 + 1);
   const int n = (int)bk.members.size();
-  const size_t per = bytes_per_structure(nv, nm, depth, precision);
+  const size_t per = bytes_per_structure(bk.voxels, depth, precision, maxiter);
   int chunk = (int)std::max<size_t>(1, std::min<size_t>(budget / per, (size_t)n));
   const int nchunks = (n + chunk - 1) / chunk;
   chunk = (n + nchunks - 1) / nchunks;
@@ -172,15 +179,25 @@ extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* ext
   double total = 0.0;
   for (const Bucket& b : buckets) total += b.voxels_total;
 
+  // Buckets whose share of the budget holds at least one structure run concurrently, one
+  // host thread each; the others run afterwards one at a time with the whole budget.
   std::vector<BucketResult> res(buckets.size());
   std::vector<std::thread> threads;
+  std::vector<size_t> serial;
   for (size_t b = 0; b < buckets.size(); ++b) {
     const size_t share = (size_t)((double)budget * buckets[b].voxels_total / total);
+    if (share < bytes_per_structure(buckets[b].voxels, depth, precision, maxiter)) {
+      serial.push_back(b);
+      continue;
+    }
     threads.emplace_back(run_bucket, std::cref(buckets[b]), device, share, depth, precision,
                          (double)rtol, (double)atol, maxiter, lambda, mu, c_eff, iters, status,
                          &res[b]);
   }
   for (auto& t : threads) t.join();
+  for (size_t b : serial)
+    run_bucket(buckets[b], device, budget, depth, precision, (double)rtol, (double)atol, maxiter,
+               lambda, mu, c_eff, iters, status, &res[b]);
   for (size_t b = 0; b < buckets.size(); ++b)
     if (res[b].rc)
       return fail(res[b].rc, "bucket %dx%dx%d: %s", buckets[b].voxels[0], buckets[b].voxels[1],

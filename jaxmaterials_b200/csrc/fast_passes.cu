@@ -543,12 +543,14 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
       }
     }
     if (!mbar_wait(mbar)) {
-      // the copies did not land in time: report and leave this instance stopped
+      // the copies did not land in time: report and leave this instance stopped; wait once
+      // more (bounded) for them before the block's shared memory is released, and record
+      // when even that wait ran out (the instance's buffers are then suspect)
       if (tid == 0) {
         st[b].status = kTimeout;
         st[b].done = 1;
       }
-      mbar_wait(mbar);
+      if (!mbar_wait(mbar) && tid == 0) st[b].copies_lost = 1;
       return;
     }
   } else {

@@ -507,6 +507,7 @@ __global__ void finalize_kernel(int nblk, int phase, InstanceState* __restrict__
       // continue from this iterate with FP64 fields; no FP32 update for this evaluation
       s.phase = 1;
       s.switched = 1;
+      s.switch_iter = s.iter;
       s.best_eval = s.evals;
     } else {
       s.done = 1;

@@ -214,32 +214,41 @@ int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]) {
   return 0;
 }
 
-int upload_tables(lsb_solver* s) {
+int upload_tables(lsb_solver* s, TableUpload how) {
   GridDesc& g = s->g;
   const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
-  // twiddles exp(-2 pi i k / n) and the sin/cos tables of the modified wave vectors,
-  // both evaluated in FP64 (fourier.py:29-31: xi_d / 2 = pi k_d / N_d)
-  std::vector<float2> tw32;
-  std::vector<double2> tw64;
-  for (int n : {g.nx, g.ny, g.nz})
-    for (int k = 0; k < n; ++k) {
-      double a = -2.0 * M_PI * (double)k / (double)n;
-      double c = std::cos(a), sn = std::sin(a);
-      tw32.push_back(make_float2((float)c, (float)sn));
-      tw64.push_back(make_double2(c, sn));
-    }
-  std::vector<double> tab;
-  auto add_tab = [&](int n, int count) {
-    for (int k = 0; k < count; ++k) tab.push_back(std::sin((2.0 * M_PI * k / n) / 2.0));
-    for (int k = 0; k < count; ++k) tab.push_back(std::cos((2.0 * M_PI * k / n) / 2.0));
-  };
-  add_tab(g.nx, g.nx);
-  add_tab(g.ny, g.ny);
-  add_tab(g.nz, g.nzh);
-  if (cudaMemcpy(s->d_tw32, tw32.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(s->d_tw64, tw64.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(s->d_tables, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-    return fail(-2, "upload of twiddle tables failed");
+  if (how != TableUpload::kNone) {
+    // twiddles exp(-2 pi i k / n) and the sin/cos tables of the modified wave vectors,
+    // both evaluated in FP64 (fourier.py:29-31: xi_d / 2 = pi k_d / N_d)
+    std::vector<float2> tw32;
+    std::vector<double2> tw64;
+    for (int n : {g.nx, g.ny, g.nz})
+      for (int k = 0; k < n; ++k) {
+        double a = -2.0 * M_PI * (double)k / (double)n;
+        double c = std::cos(a), sn = std::sin(a);
+        tw32.push_back(make_float2((float)c, (float)sn));
+        tw64.push_back(make_double2(c, sn));
+      }
+    std::vector<double> tab;
+    auto add_tab = [&](int n, int count) {
+      for (int k = 0; k < count; ++k) tab.push_back(std::sin((2.0 * M_PI * k / n) / 2.0));
+      for (int k = 0; k < count; ++k) tab.push_back(std::cos((2.0 * M_PI * k / n) / 2.0));
+    };
+    add_tab(g.nx, g.nx);
+    add_tab(g.ny, g.ny);
+    add_tab(g.nz, g.nzh);
+    // (an asynchronous copy from pageable memory returns once the data is staged, so the
+    // vectors may go out of scope)
+    auto copy = [&](void* dst, const void* src, size_t bytes) {
+      return how == TableUpload::kAsync
+                 ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream)
+                 : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    if (copy(s->d_tw32, tw32.data(), sizeof(float2) * ntw) != cudaSuccess ||
+        copy(s->d_tw64, tw64.data(), sizeof(double2) * ntw) != cudaSuccess ||
+        copy(s->d_tables, tab.data(), sizeof(double) * tab.size()) != cudaSuccess)
+      return fail(-2, "upload of twiddle tables failed");
+  }
   g.px.tw = s->d_tw32;
   g.py.tw = s->d_tw32 + g.nx;
   g.pz.tw = s->d_tw32 + g.nx + g.ny;
@@ -444,6 +453,69 @@ struct GraphPhase {
   }
 };
 
+// Records an event on the solver's stream after each launch of one iteration (profiling).
+struct StepTimer {
+  cudaStream_t st;
+  std::vector<cudaEvent_t> ev;        // ev[0] before the first launch, ev[k] after launch k
+  std::vector<const char*> names;     // names[k - 1]: kernel of launch k
+  size_t next = 1;
+  void mark(const char* name) {
+    if (next < ev.size()) cudaEventRecord(ev[next], st);
+    if (names.size() < next) names.push_back(name);
+    ++next;
+  }
+};
+
+// Blocks per instance of the Anderson Gram-row kernel (its partials fit the z-block-sized
+// buffer).
+int gram_blocks(const lsb_solver* s) {
+  return (int)std::max<long long>(
+      1, std::min<long long>({(long long)s->aa_zblocks, 592LL, (s->g.nv + 255) / 256}));
+}
+
+// One iteration of precision T: x pass, criterion and stop decision, inverse y pass, then
+// either the plain update (z pass mode 1) or the Anderson update (residual rings, Gram
+// row, coefficients, combine, stress of the combined iterate), and the forward y pass.
+template <typename T>
+void enqueue_iteration(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<T>* spec,
+                       const AndersonArgs<T>& aa, const SolveParams& sp, const LaunchShape& sh,
+                       int phase, const T* inject, StepTimer* tm) {
+  cudaStream_t st = s->stream;
+  auto mark = [&](const char* name) {
+    if (tm) tm->mark(name);
+  };
+  pass_x<T>(s, batch, spec);
+  mark("x pass");
+  launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
+  mark("finalize");
+  pass_y<T>(s, true, batch, spec);
+  mark("y pass inverse");
+  if (aa.depth > 0) {
+    const int gblk = gram_blocks(s);
+    pass_z<T>(s, 3, batch, lam, mu, eps, spec, nullptr, aa);
+    mark("z pass residual rings");
+    launch_anderson_gram<T>(s->g.nv, gblk, s->depth, phase, batch, s->d_state, aa.r,
+                            s->d_aa_partials, st);
+    mark("anderson gram");
+    launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
+                          s->d_aa_mat, s->d_aa_alpha, st);
+    mark("anderson solve");
+    launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g, s->d_aa_alpha,
+                               eps, st, inject);
+    mark("anderson combine");
+    pass_z<T>(s, 2, batch, lam, mu, eps, spec, nullptr, aa);
+    mark("z pass stress");
+  } else {
+    pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
+    mark("z pass update");
+  }
+  pass_y<T>(s, false, batch, spec);
+  mark("y pass forward");
+}
+
+// Kernels launched by one iteration.
+inline long long iteration_launches(bool mix) { return mix ? 9LL : 5LL; }
+
 // Runs the loop of precision T for every instance in its phase until none is left there.
 // init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
 // With `anderson` the update is Anderson mixing of depth s->depth (rings of precision T).
@@ -459,31 +531,12 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   cudaStream_t st = s->stream;
   const AndersonArgs<T> aa = anderson_args<T>(s, anderson && s->depth > 0);
   const bool mix = aa.depth > 0;
-  // blocks per instance of the Gram-row kernel (its partials fit the z-block-sized buffer)
-  const int gblk = (int)std::max<long long>(
-      1, std::min<long long>({(long long)s->aa_zblocks, 592LL, (s->g.nv + 255) / 256}));
   pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0, aa);
   pass_y<T>(s, false, batch, spec);
   s->launches += 2;
   LSB_CUDA(cudaGetLastError());
   auto iteration = [&]() {
-    pass_x<T>(s, batch, spec);
-    launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
-    pass_y<T>(s, true, batch, spec);
-    if (mix) {
-      // residual into the rings, Gram row, coefficients, combine, stress + forward z
-      pass_z<T>(s, 3, batch, lam, mu, eps, spec, nullptr, aa);
-      launch_anderson_gram<T>(s->g.nv, gblk, s->depth, phase, batch, s->d_state, aa.r,
-                              s->d_aa_partials, st);
-      launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
-                            s->d_aa_mat, s->d_aa_alpha, st);
-      launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g,
-                                 s->d_aa_alpha, eps, st, inject);
-      pass_z<T>(s, 2, batch, lam, mu, eps, spec, nullptr, aa);
-    } else {
-      pass_z<T>(s, 1, batch, lam, mu, eps, spec, nullptr, aa);
-    }
-    pass_y<T>(s, false, batch, spec);
+    enqueue_iteration<T>(s, batch, lam, mu, eps, spec, aa, sp, sh, phase, inject, nullptr);
   };
   gp.capture(iteration);
   long long launched = 0;
@@ -499,7 +552,7 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
       }
     }
     launched += n;
-    s->launches += (mix ? 9LL : 5LL) * n;
+    s->launches += iteration_launches(mix) * n;
     LSB_CUDA(cudaGetLastError());
     LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch,
                              cudaMemcpyDeviceToHost, st));
@@ -822,14 +875,25 @@ int lsb_set_damage(lsb_solver* solver, const void* d_damage, int elem_size, doub
 
 long long lsb_kernel_launches(lsb_solver* solver) { return solver ? solver->launches : -1; }
 
-int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
-                       float* d_eps, int reps, float* ms_out) {
+int lsb_fp64_iters(lsb_solver* solver, int* out) {
+  if (!solver || !out) return fail(-1, "null argument");
+  for (int b = 0; b < solver->last_batch; ++b) {
+    const InstanceState& st = solver->h_state[b];
+    out[b] = st.switched ? st.iter - st.switch_iter : (st.phase == 1 ? st.iter : 0);
+  }
+  return 0;
+}
+
+int lsb_profile_step(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu,
+                     float* d_eps, int reps, float* ms_out, int max_kernels, char* names,
+                     int names_len) {
   g_last_error.clear();
-  if (!s || !d_lambda || !d_mu || !d_eps || !ms_out) return fail(-1, "null argument");
+  if (!s || !d_lambda || !d_mu || !d_eps || !ms_out || !names) return fail(-1, "null argument");
   if (batch < 1 || batch > s->batch_cap) return fail(-1, "batch %d outside [1, %d]", batch, s->batch_cap);
-  if (reps < 1) return fail(-1, "reps must be >= 1");
+  if (reps < 1 || max_kernels < 1 || names_len < 1) return fail(-1, "reps, max_kernels and names_len must be >= 1");
   const GridDesc& g = s->g;
-  const LaunchShape& sh = s->sh32;
+  LaunchShape sh = s->sh32;
+  if (!use_fast32(s)) sh.x_blocks_per_instance = s->x_blocks_generic32;
   cudaStream_t st = s->stream;
   // tolerances 0 and no stall detection: every pass does its full work
   SolveParams sp = make_params(s, 0.0, 0.0, 0x3fffffff, LSB_RULE_CUDA);
@@ -840,37 +904,44 @@ int lsb_profile_passes(lsb_solver* s, int batch, const float* d_lambda, const fl
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eb.data(), sizeof(double) * eb.size(), cudaMemcpyHostToDevice, st));
   const int nstruct = structures_of(s, batch);
   if (nstruct < 0) return nstruct;
+  LSB_TRY(prepare_damage(s, nstruct));
+  LSB_TRY(prepare_aniso(s, nstruct));
   launch_reset_state(batch, 0, s->d_state, st);
   launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
-  const AndersonArgs<float> aa0 = anderson_args<float>(s, false);
-  pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa0);
+  if (!s->xtuned) LSB_TRY(tune_xpass(s, batch));
+  const AndersonArgs<float> aa = anderson_args<float>(s, s->depth > 0);
+  pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa);
   pass_y<float>(s, false, batch, s->d_spec32);
-  cudaEvent_t ev[6];
-  for (auto& e : ev) LSB_CUDA(cudaEventCreate(&e));
-  double acc[5] = {0, 0, 0, 0, 0};
+  // warm-up iterations: the Anderson rings fill up, so that the timed ones do full work
+  for (int i = 0; i < s->depth + 2; ++i)
+    enqueue_iteration<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, aa, sp, sh, 0, nullptr, nullptr);
+  StepTimer tm{st};
+  tm.ev.resize((size_t)max_kernels + 1);
+  for (auto& e : tm.ev) LSB_CUDA(cudaEventCreate(&e));
+  std::vector<double> acc(max_kernels, 0.0);
+  size_t count = 0;
   for (int r = 0; r < reps; ++r) {
-    cudaEventRecord(ev[0], st);
-    pass_x<float>(s, batch, s->d_spec32);
-    cudaEventRecord(ev[1], st);
-    launch_finalize(sh, 0, batch, s->d_state, s->d_partials, nullptr, 0, sp, st);
-    cudaEventRecord(ev[2], st);
-    pass_y<float>(s, true, batch, s->d_spec32);
-    cudaEventRecord(ev[3], st);
-    pass_z<float>(s, 1, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa0);
-    cudaEventRecord(ev[4], st);
-    pass_y<float>(s, false, batch, s->d_spec32);
-    cudaEventRecord(ev[5], st);
-    LSB_CUDA(cudaEventSynchronize(ev[5]));
-    for (int k = 0; k < 5; ++k) {
+    tm.next = 1;
+    cudaEventRecord(tm.ev[0], st);
+    enqueue_iteration<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, aa, sp, sh, 0, nullptr, &tm);
+    count = std::min(tm.next - 1, (size_t)max_kernels);
+    LSB_CUDA(cudaEventSynchronize(tm.ev[count]));
+    for (size_t k = 0; k < count; ++k) {
       float ms = 0.f;
-      cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      cudaEventElapsedTime(&ms, tm.ev[k], tm.ev[k + 1]);
       acc[k] += ms;
     }
   }
-  for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& e : tm.ev) cudaEventDestroy(e);
   LSB_CUDA(cudaGetLastError());
-  for (int k = 0; k < 5; ++k) ms_out[k] = (float)(acc[k] / reps);
-  return 0;
+  std::string joined;
+  for (size_t k = 0; k < count; ++k) {
+    ms_out[k] = (float)(acc[k] / reps);
+    if (k) joined += ",";
+    joined += tm.names[k];
+  }
+  std::snprintf(names, (size_t)names_len, "%s", joined.c_str());
+  return (int)count;
 }
 
 int lsb_history(lsb_solver* solver, double* out, int len) {

@@ -120,9 +120,12 @@ int fail(int code, const char* fmt, ...);
 bool factorize(int n, Plan1D& p);
 // Fills s->g from voxels/extents, plans the launches and checks block sizes.
 int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]);
+// How upload_tables fills the table buffers: blocking copies, copies on s->stream, or no
+// copy (the buffers already hold this grid's tables).
+enum class TableUpload { kBlocking, kAsync, kNone };
 // Uploads the twiddle and sin/cos tables into s->d_tw32/d_tw64/d_tables and points the
 // plans of s->g at them (the buffers must be sized for the grid).
-int upload_tables(lsb_solver* s);
+int upload_tables(lsb_solver* s, TableUpload how = TableUpload::kBlocking);
 // Sets s->g.lame_group for a solve of `batch` instances and returns the number of Lame
 // field pairs the solve reads (negative with an error message when batch does not split).
 int structures_of(lsb_solver* s, int batch);

@@ -135,6 +135,8 @@ struct InstanceState {
   int best_eval;  // evaluation at which best_e last improved significantly
   int switched;   // 1 once the instance moved from FP32 to FP64
   int aa_base;    // iteration count when the Anderson history (re)started
+  int copies_lost;  // a block gave up waiting for its asynchronous copies twice (kTimeout)
+  int switch_iter;  // updates done in FP32 before the switch to FP64 fields (switched = 1)
   double e0;      // criterion at the first iterate
   double e0_ref;  // > 0: the stop threshold is rtol * e0_ref instead of rtol * e0
   double e;       // last criterion value

@@ -7,8 +7,8 @@ same NumPy generator calls (inverse transform of a normal density clipped to [r_
 :26-72), the initial fibre lattice is built the same way (:102-118), and the shaking moves
 (:174-203) run in ``libfibres.so``, which reproduces the reference's C++ library bit for bit.
 The reference compiles its C++ with g++ every time a ``FibreDistribution2d`` is created; here
-the library is built once with the package, and there is no silent fallback when it is
-missing (``fast_code=False`` selects the reference's NumPy path explicitly).
+the library is built once with the package, and there is no fallback when it is missing
+(the reference's NumPy shaking path, ``fast_code=False``, is not provided).
 
 ``place_batch`` moves many independent fibre sets in one call on all host cores.
 """
@@ -107,7 +107,8 @@ class FibreDistribution2d:
     """Fibres in a periodic 2-d box (distributions_fibres.py:75-295): iterating yields
     (positions (n, 2), radii (n,)), the regular start lattice shaken with freshly drawn radii.
     The C++ generator state persists across iterations of one instance, as in the
-    reference."""
+    reference. ``fast_code`` is accepted for the reference's signature; only the native
+    path (True) exists."""
 
     def __init__(self, domain_size, volume_fraction=0.55,
                  r_fibre_dist=FibreRadiusDistribution(r_avg=7.5e-3, r_min=5.0e-3,
@@ -117,88 +118,24 @@ class FibreDistribution2d:
         self.domain_size = np.asarray(domain_size, dtype=np.float64)
         self._volume_fraction = volume_fraction
         self._r_fibre_dist = r_fibre_dist
-        self._rng = np.random.default_rng(seed=seed)
         self._initial_fibre_locations = initial_lattice(self.domain_size, r_fibre_dist.r_avg,
                                                         volume_fraction)
-        self._fast_code = fast_code
-        if fast_code:
-            self._lib = _lib.load_fibres()
-            self._state_len = ctypes.c_uint()
-            self._state = ctypes.create_string_buffer(_STATE_BYTES)
-            self._lib.initialise_rng(RNG_SEED, ctypes.byref(self._state_len), self._state)
+        if not fast_code:
+            raise ValueError("only the native shaking path (fast_code=True) is provided")
+        self._lib = _lib.load_fibres()
+        self._state_len = ctypes.c_uint()
+        self._state = ctypes.create_string_buffer(_STATE_BYTES)
+        self._lib.initialise_rng(RNG_SEED, ctypes.byref(self._state_len), self._state)
 
     def __iter__(self):
         while True:
             r = self._r_fibre_dist.draw(self._initial_fibre_locations.shape[0])
             x = np.array(self._initial_fibre_locations)
-            if self._fast_code:
-                r = np.ascontiguousarray(r, dtype=np.float64)
-                x = np.ascontiguousarray(x, dtype=np.float64)
-                self._lib.move_fibres(
-                    r.shape[0], self.domain_size.ctypes.data_as(_lib.c_double_p),
-                    r.ctypes.data_as(_lib.c_double_p), x.ctypes.data_as(_lib.c_double_p),
-                    NUM_REPEATS, EPS_FIBRES, IT_MAX_OVLAP, ctypes.byref(self._state_len),
-                    self._state)
-            else:
-                x = self._move_fibres(x, r, NUM_REPEATS, IT_MAX_OVLAP, EPS_FIBRES)
+            r = np.ascontiguousarray(r, dtype=np.float64)
+            x = np.ascontiguousarray(x, dtype=np.float64)
+            self._lib.move_fibres(
+                r.shape[0], self.domain_size.ctypes.data_as(_lib.c_double_p),
+                r.ctypes.data_as(_lib.c_double_p), x.ctypes.data_as(_lib.c_double_p),
+                NUM_REPEATS, EPS_FIBRES, IT_MAX_OVLAP, ctypes.byref(self._state_len),
+                self._state)
             yield (x, r)
-
-    def _move_fibres(self, x, r, num_repeats=NUM_REPEATS, it_max_ovlap=IT_MAX_OVLAP,
-                     eps_fibres=EPS_FIBRES):
-        """The reference's NumPy shaking path (distributions_fibres.py:205-266): the same
-        algorithm driven by this instance's NumPy generator."""
-        n = r.shape[0]
-        labels = self._rng.permutation(range(n))
-        overlap = True
-        sweep = 0
-        while overlap or sweep < num_repeats:
-            overlap = False
-            for j in range(n):
-                me = labels[j]
-                p = x[me, :]
-                d = self._dist_periodic(p, x)
-                d[me] = np.inf
-                radius = np.mean(sorted(d)[:3])
-                gap, trials, fewest = 0, 0, np.inf
-                while gap < eps_fibres:
-                    u_r = self._rng.uniform(low=0, high=radius)
-                    u_t = self._rng.uniform(low=0, high=2 * np.pi)
-                    trial = p + u_r * np.asarray([np.cos(u_t), np.sin(u_t)])
-                    for k in range(2):
-                        while trial[k] < 0:
-                            trial[k] += self.domain_size[k]
-                        while trial[k] > self.domain_size[k]:
-                            trial[k] -= self.domain_size[k]
-                    d = self._dist_periodic(trial, x) - r[me] - r
-                    d[me] = np.inf
-                    gap = np.min(d)
-                    overlaps = np.count_nonzero(d < 0)
-                    if overlaps < fewest:
-                        best, fewest = trial, overlaps
-                    trials += 1
-                    if trials > it_max_ovlap:
-                        trial = best
-                        overlap = True
-                        break
-                x[me, :] = trial[:]
-            sweep += 1
-        return x
-
-    def _dist_periodic(self, p, q):
-        """Minimum-image distances from p to every row of q."""
-        n = q.shape[0]
-        out = np.empty(n, dtype=np.float64)
-        if self._fast_code:
-            p = np.ascontiguousarray(p, dtype=np.float64)
-            q = np.ascontiguousarray(q, dtype=np.float64)
-            self._lib.dist_periodic(n, p.ctypes.data_as(_lib.c_double_p),
-                                    q.ctypes.data_as(_lib.c_double_p),
-                                    self.domain_size.ctypes.data_as(_lib.c_double_p),
-                                    out.ctypes.data_as(_lib.c_double_p))
-            return out
-        d = np.empty(shape=(9, n))
-        for j, off in enumerate(itertools.product(
-                [-self.domain_size[0], 0, +self.domain_size[0]],
-                [-self.domain_size[1], 0, +self.domain_size[1]])):
-            d[j, :] = np.sqrt(np.sum((p + np.asarray(off) - q) ** 2, axis=1))
-        return np.min(d, axis=0)

@@ -36,11 +36,13 @@ __all__ = [
     "MAXITER",
     "NONFINITE",
     "STALLED",
+    "TIMEOUT",
     "RULE_CUDA",
     "RULE_JAX",
 ]
 
-CONVERGED, MAXITER, NONFINITE, STALLED = 1, 2, 3, 4
+# TIMEOUT: a kernel's bounded wait for its own copies ran out; recreate the Solver
+CONVERGED, MAXITER, NONFINITE, STALLED, TIMEOUT = 1, 2, 3, 4, 5
 RULE_CUDA, RULE_JAX = 0, 1
 PRECISIONS = {"fp32": 0, "mixed": 1, "fp64": 2}
 
@@ -313,9 +315,17 @@ class Solver:
         """Kernels enqueued by this solver so far."""
         return int(self._lib.lsb_kernel_launches(self._h))
 
-    def profile_passes(self, lmbda, mu, batch=None, reps=5):
-        """Average CUDA-event time (ms) of each pass of one iteration:
-        dict with keys xpass, finalize, ypass_inverse, zpass, ypass_forward."""
+    def fp64_iters(self):
+        """Updates of each instance of the last solve that ran with FP64 fields."""
+        out = np.zeros(self._last_batch, dtype=np.int32)
+        _lib.check(self._lib.lsb_fp64_iters(self._h, out.ctypes.data_as(_lib.c_int_p)),
+                   "lsb_fp64_iters")
+        return out
+
+    def profile_step(self, lmbda, mu, batch=None, reps=5):
+        """Average CUDA-event time (ms) of every launch of one FP32 iteration as the solve
+        runs it (Anderson when depth > 0, plain otherwise): list of (kernel name, ms) in
+        launch order."""
         import torch
 
         g = self.grid_spec
@@ -324,14 +334,16 @@ class Solver:
         m = self._as_device(mu, g.shape)
         _lib.check(self._lib.lsb_set_lame_group(self._h, 0), "lsb_set_lame_group")
         work = torch.empty((b, 6) + g.shape, dtype=torch.float32, device=self.device)
-        ms = np.zeros(5, dtype=np.float32)
+        ms = np.zeros(32, dtype=np.float32)
+        names = ctypes.create_string_buffer(1024)
         stream = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._lib.lsb_set_stream(self._h, ctypes.c_void_p(stream)), "lsb_set_stream")
-        _lib.check(self._lib.lsb_profile_passes(
+        n = self._lib.lsb_profile_step(
             self._h, b, ctypes.c_void_p(lm.data_ptr()), ctypes.c_void_p(m.data_ptr()),
-            ctypes.c_void_p(work.data_ptr()), int(reps), _fptr(ms)), "lsb_profile_passes")
-        return dict(zip(["xpass", "finalize", "ypass_inverse", "zpass", "ypass_forward"],
-                        [float(v) for v in ms]))
+            ctypes.c_void_p(work.data_ptr()), int(reps), _fptr(ms), ms.shape[0], names,
+            len(names))
+        _lib.check(n if n < 0 else 0, "lsb_profile_step")
+        return list(zip(names.value.decode().split(","), [float(v) for v in ms[:n]]))
 
     def history(self):
         """Criterion after every evaluation of the last solve, shape (B, maxiter + 1)."""

@@ -2,7 +2,7 @@
 
 Run from the repository root in an environment that holds the reference checkout:
 
-    python tests/golden/make_damage_golden.py /root/reference
+    python tests/golden/make_damage_golden.py <reference checkout>   (or JAXMATERIALS_REF in the environment)
 
 Imports ``src/jaxmaterials/solver/lippmann_schwinger.py`` (with ``tests/golden/_jaxshim``
 standing in for jax, NumPy doing the arithmetic) and runs, unchanged,
@@ -81,4 +81,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["JAXMATERIALS_REF"])

@@ -3,7 +3,7 @@ Python code (and, through it, its C++ fibre library, which it compiles with g++)
 
 Run from the repository root in an environment that holds the reference checkout:
 
-    python tests/golden/make_fibres_golden.py /root/reference
+    python tests/golden/make_fibres_golden.py <reference checkout>   (or JAXMATERIALS_REF in the environment)
 
 ``src/jaxmaterials/data/distributions_fibres.py`` and ``src/jaxmaterials/data/data.py`` are
 imported and executed unchanged. data.py imports modules that are not installed here and
@@ -94,4 +94,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["JAXMATERIALS_REF"])

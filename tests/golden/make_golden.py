@@ -2,7 +2,7 @@
 
 Run from the repository root in an environment that holds the reference checkout:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>   (or JAXMATERIALS_REF in the environment)
 
 JAX is not installed here, so ``tests/golden/_jaxshim`` provides a NumPy-backed stand-in
 for the handful of jax calls the reference solver makes; the reference modules
@@ -132,4 +132,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["JAXMATERIALS_REF"])

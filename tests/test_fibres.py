@@ -58,14 +58,26 @@ def test_fibre_sets_match_reference(fibres_lib, gold, case):
         assert np.array_equal(x, gold[f"d2_{case}_x{draw}"])
 
 
-def test_numpy_path_matches_reference(fibres_lib, gold):
-    from jaxmaterials_b200.data.distributions_fibres import FibreDistribution2d
+def test_numpy_path_matches_reference(gold):
+    """The oracle's restatement of the reference's NumPy shaking path (fast_code=False)
+    reproduces the reference's positions bit for bit."""
+    from jaxmaterials_b200.data.distributions_fibres import initial_lattice
+    from oracle import fibres_oracle
 
-    fd = FibreDistribution2d(tuple(gold["np_box"]), volume_fraction=0.3,
-                             r_fibre_dist=radius_dist(7), seed=5, fast_code=False)
-    x, r = next(iter(fd))
+    box = np.asarray(gold["np_box"], dtype=np.float64)
+    rd = radius_dist(7)
+    x0 = initial_lattice(box, rd.r_avg, 0.3)
+    r = rd.draw(x0.shape[0])
+    x = fibres_oracle.move_fibres(np.random.default_rng(5), np.array(x0), r, box)
     assert np.array_equal(r, gold["np_r"])
     assert np.array_equal(x, gold["np_x"])
+
+
+def test_numpy_shaking_path_is_not_in_the_product():
+    from jaxmaterials_b200.data.distributions_fibres import FibreDistribution2d
+
+    with pytest.raises(ValueError):
+        FibreDistribution2d((0.1, 0.1), fast_code=False)
 
 
 def test_constant_radii(gold):
