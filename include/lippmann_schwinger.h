@@ -109,6 +109,14 @@ int lsb_set_warm_history(lsb_solver *solver, int on);
  * 0 or 1 fixes it, -1 only queries. Returns the variant in use (0 before tuning). */
 int lsb_tile_variant(lsb_solver *solver, int variant);
 
+/* No reference counterpart. Layout of the FP32 spectrum between the y and x passes:
+ * on = 1 (the default where it applies: every extent in {16, 32, 48, 64, 96, 128}) keeps
+ * it in contiguous x tiles of 8 kz columns in a second spectrum buffer, so that the x pass
+ * reads one contiguous chunk per component and tile; on = 0 keeps the cuFFT layout
+ * throughout and the strided x pass (lsb_tile_variant). Both give bit-identical results.
+ * Returns 1 if the tiled layout is in use after the call, 0 if not. */
+int lsb_set_tiled(lsb_solver *solver, int on);
+
 /* No reference counterpart. on != 0 (default): each phase of a solve captures one
  * iteration's launches into a CUDA graph on a stream of the solver's own (ordered after
  * the work already on the solver's stream, and that stream waits for it) and replays it;

@@ -45,6 +45,30 @@ __device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y
 
 __device__ __forceinline__ bool active32(const InstanceState& s) { return !s.done && s.phase == 0; }
 
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Bounded wait on a one-shot mbarrier (phase 0). Returns false if the copies did not
+// complete within the limit.
+__device__ __forceinline__ bool mbar_wait(unsigned mbar) {
+  for (long long spin = 0; spin < (1LL << 24); ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done) : "r"(mbar), "r"(0u) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
 // Step A of the four-step transform: DFT over e of v[e] = x[p + P e], then the twiddle.
 template <int N, int E = Split<N>::E>
 __device__ __forceinline__ void step_a(float2* v, int p, const float2* __restrict__ tw) {
@@ -63,6 +87,21 @@ __device__ __forceinline__ void step_a_smem(float2* v, int p, const float2* tw) 
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) v[k1] = cmul(v[k1], tw[p * k1]);
   }
+}
+
+// ----------------------------------------------------------------------------- tiled layout
+// The tiled spectrum layout (grids with nx <= 128 and nz/2+1 = 8 k + 1, ny = 8 k'), written
+// by the forward y pass and read by the inverse y pass, and in place by this x pass: per
+// instance and component,
+//   full tiles   [ky][j][x][t]   kz = 8 j + t, j < NF = (nz/2+1 - 1) / 8
+//   tail         [ky / 8][x][ky % 8]   the z Nyquist column kz = nz/2
+// (tile_offset below). Every tile of the x pass is then one contiguous chunk of 8 nx complex
+// values per component, fetched with one bulk copy.
+constexpr int kTW = 8;
+
+__host__ __device__ __forceinline__ size_t tile_offset(int nx, int ny, int nf, int x, int ky, int kz) {
+  if (kz < nf * kTW) return ((size_t)(ky * nf + kz / kTW) * nx + x) * kTW + (kz % kTW);
+  return (size_t)ny * nf * nx * kTW + ((size_t)(ky / kTW) * nx + x) * kTW + (ky % kTW);
 }
 
 // ----------------------------------------------------------------------------- y pass
@@ -96,9 +135,17 @@ __host__ __device__ constexpr int y_min_blocks() {
   return N == 256 ? 3 : 1024 / (32 * ((y_threads<N>() + 31) / 32));
 }
 
-template <int NY>
-__global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fast(GridDesc g, int inverse,
+// TILED: the x-pass side of the transform is the tiled layout in `tspec` (see xpass_tiled):
+// the forward pass reads `spec` (cuFFT layout) and writes `tspec`, the inverse pass reads
+// `tspec` and writes `spec`. Otherwise both sides are `spec`, transformed in place.
+// (the tiled form keeps a second base pointer and index terms: three quarters of the
+// resident blocks, so that it does not spill)
+template <int NY, bool TILED>
+__global__ void __launch_bounds__(y_threads<NY>(),
+                                  TILED ? (3 * y_min_blocks<NY>() / 4 > 2 ? 3 * y_min_blocks<NY>() / 4 : 2)
+                                        : y_min_blocks<NY>()) ypass_fast(GridDesc g, int inverse,
                                                                float2* __restrict__ spec,
+                                                               float2* __restrict__ tspec,
                                                                const InstanceState* __restrict__ st) {
   constexpr int E = YSplit<NY>::E, P = YSplit<NY>::P, NJ = (E + P - 1) / P;
   constexpr int YT = y_cols<NY>();
@@ -120,11 +167,21 @@ __global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fas
     valid = kz < nzh;
   }
   float2* base = spec + ((size_t)bc * g.nx + x) * (size_t)NY * nzh + kz;
+  // tiled side: element ky of this column sits at tb + (ky >> sh) * ta + (ky & mk)
+  // (tile_offset: full columns step by a tile row per ky, the Nyquist column by 8 ky groups)
+  const int nf = (nzh - 1) / kTW;
+  const bool ncol = kz >= nf * kTW;
+  float2* tb = tspec + (size_t)bc * g.nm + tile_offset(g.nx, NY, nf, x, 0, kz);
+  const int sh = ncol ? 3 : 0, mk = ncol ? kTW - 1 : 0;
+  const int ta = ncol ? g.nx * kTW : nf * g.nx * kTW;
+  auto tptr = [&](int ky) { return tb + (size_t)((ky >> sh) * ta + (ky & mk)); };
   const float2* tw = g.py.tw;
   float2 v[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    float2 a = valid ? base[(size_t)(p + P * e) * nzh] : make_float2(0.f, 0.f);
+    const int ky = p + P * e;
+    float2 a = make_float2(0.f, 0.f);
+    if (valid) a = (TILED && inverse) ? *tptr(ky) : base[(size_t)ky * nzh];
     v[e] = inverse ? conj2(a) : a;
   }
   step_a<NY, E>(v, p, tw);
@@ -141,7 +198,12 @@ __global__ void __launch_bounds__(y_threads<NY>(), y_min_blocks<NY>()) ypass_fas
     Bfly<P>::run(w);
     if (valid) {
 #pragma unroll
-      for (int k2 = 0; k2 < P; ++k2) base[(size_t)(k1 + E * k2) * nzh] = inverse ? conj2(w[k2]) : w[k2];
+      for (int k2 = 0; k2 < P; ++k2) {
+        const int ky = k1 + E * k2;
+        const float2 o = inverse ? conj2(w[k2]) : w[k2];
+        if (TILED && !inverse) *tptr(ky) = o;
+        else base[(size_t)ky * nzh] = o;
+      }
     }
   }
 }
@@ -168,74 +230,23 @@ __host__ __device__ constexpr int x_cols_v() {
 }
 template <int NX, int V>
 __host__ __device__ constexpr int x_min_blocks() { return x_cols_v<NX, V>() < x_cols<NX>() ? 4 : 2; }
-template <int NX, int T>
-__host__ __device__ constexpr int x_row() { return XSplit<NX>::P * T + T; }
-template <int NX, int T>
+template <int NX, int T, typename SP = XSplit<NX>>
+__host__ __device__ constexpr int x_row() { return SP::P * T + T; }
+template <int NX, int T, typename SP = XSplit<NX>>
 __host__ __device__ constexpr int x_region() {
-  return XSplit<NX>::E * x_row<NX, T>() > NX * T ? XSplit<NX>::E * x_row<NX, T>() : NX * T;
+  return SP::E * x_row<NX, T, SP>() > NX * T ? SP::E * x_row<NX, T, SP>() : NX * T;
 }
 
-// ANI: Gamma^0 of an anisotropic reference stiffness (aniso.cuh) instead of the isotropic
-// closed form.
-template <int NX, int V, bool ANI>
-__global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_blocks<NX, V>()) xpass_fast(
-    GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
-    InstanceState* __restrict__ st, double* __restrict__ partials) {
-  constexpr int E = XSplit<NX>::E, P = XSplit<NX>::P, T = x_cols_v<NX, V>(), RS = x_row<NX, T>(),
-                REG = x_region<NX, T>();
-  static_assert((6 * P * T) % 32 == 0, "the x pass reduces over whole warps");
-  constexpr int NJ = (E + P - 1) / P;
-  extern __shared__ __align__(16) unsigned char xfraw[];
-  float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
-  __shared__ double red[32];
-  __shared__ double colf[3][T];  // per-column wave-vector factors
-  // shared-memory copies of the x twiddles and wave-vector tables (read per element / mode;
-  // from shared memory the x pass is 6% faster at 128^3 than from the L1/global path)
-  __shared__ float2 stw[NX];           // exp(-2 pi i k / NX)
-  __shared__ double ssx[NX], scx[NX];  // sin, cos(pi kx / NX)
-  const int b = blockIdx.z;
-  if (!active32(st[b])) return;
-  const int tid = threadIdx.x;
-  const int t = tid % T, p = (tid / T) % P, c = tid / (T * P);
-  const int nzh = g.nzh;
-  // With nz/2+1 = T k + 1 the last tile takes the z Nyquist column for T consecutive ky
-  // instead of one column per ky (as the y pass); its surplus blocks only report a zero
-  // partial.
-  const bool tail = nzh % T == 1 && (int)blockIdx.x == nzh / T;
-  if (tail && (int)blockIdx.y * T >= g.ny) {
-    if (tid == 0) partials[(size_t)b * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = 0.0;
-    return;
-  }
-  auto col_ky = [&](int tt) { return tail ? (int)blockIdx.y * T + tt : (int)blockIdx.y; };
-  auto col_kz = [&](int tt) { return tail ? nzh - 1 : (int)blockIdx.x * T + tt; };
-  const int ky = col_ky(t);
-  const int kz = col_kz(t);
-  const bool valid = kz < nzh;
-  const size_t xstride = (size_t)g.ny * nzh;
-  float2* gcol = spec + (size_t)b * 6 * g.nm + (size_t)c * g.nm + (size_t)ky * nzh + kz;
-  const float2* tw = g.px.tw;
-  float2* tr = buf + (size_t)c * REG;   // this component's region
+// Pieces of the x pass shared by its two forms (strided rows of the cuFFT layout, and
+// contiguous tiles of the tiled layout). One block owns T columns (kz or ky varies with
+// the column index tt) and all NX rows of the six components; component c's shared region
+// `tr` holds either the natural layout [kx][t] or the transposed layout [k1][p][t].
 
-  if (tid < T) {
-    // tilde(xi)_d = (2 n_d / L_d) * sin/cos products (fourier.py:9-58); the ky and kz
-    // factors of this block's columns, FP64
-    const int kzz = col_kz(tid) < nzh ? col_kz(tid) : 0;
-    const int kyy = col_ky(tid);
-    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
-    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
-    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
-  }
-
-  // forward: load, step A, transpose
-  float2 v[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = valid ? gcol[(size_t)(p + P * e) * xstride] : make_float2(0.f, 0.f);
-  for (int i = tid; i < NX; i += blockDim.x) {
-    stw[i] = tw[i];
-    ssx[i] = g.sx[i];
-    scx[i] = g.cx[i];
-  }
-  __syncthreads();
+// Forward x DFT of this thread's column values v (natural order x = p + P e): step A,
+// transpose, step B; leaves X[kx] in the natural layout of tr.
+template <int NX, int T, typename SP = XSplit<NX>>
+__device__ __forceinline__ void x_forward(float2* tr, float2* v, int p, int t, const float2* stw) {
+  constexpr int E = SP::E, P = SP::P, RS = x_row<NX, T, SP>(), NJ = (E + P - 1) / P;
   step_a_smem<NX, E>(v, p, stw);
 #pragma unroll
   for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
@@ -260,9 +271,20 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
       for (int k2 = 0; k2 < P; ++k2) tr[((p + P * j) + E * k2) * T + t] = o[j * P + k2];
     }
   __syncthreads();
+}
 
-  // residual partials, zero mode, Gamma^0 (written conjugated for the inverse transform)
-  const float c_a = med[b / g.lame_group].c_a, c_b = med[b / g.lame_group].c_b;
+// Per mode of the block's tile (all six components in the regions of buf): the FP64
+// Hermitian-weighted |xi~ . sigma_hat|^2 (returned, this thread's share), the FP64 zero
+// mode, and r_hat = -Gamma^0 sigma_hat written back conjugated for the inverse transform.
+// col_ky / col_kz map a column index to its (ky, kz); colf holds the columns' ky and kz
+// wave-vector factors.
+template <int NX, int T, int REG, bool ANI, typename CY, typename CZ>
+__device__ __forceinline__ double x_modes(float2* buf, const double (*colf)[T], const double* ssx,
+                                          const double* scx, const GridDesc& g, const Medium& md,
+                                          InstanceState* st, int b, CY col_ky, CZ col_kz) {
+  const int tid = threadIdx.x;
+  const int nzh = g.nzh;
+  const float c_a = md.c_a, c_b = md.c_b;
   double acc = 0.0;
   for (int idx = tid; idx < NX * T; idx += blockDim.x) {
     const int kx = idx / T, tt = idx % T;
@@ -347,8 +369,15 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
     for (int cc = 0; cc < 6; ++cc) buf[(size_t)cc * REG + kx * T + tt] = make_float2(r[0][cc], -r[1][cc]);
   }
   __syncthreads();
+  return acc;
+}
 
-  // inverse (forward transform of the conjugate): step A from the natural layout
+// Inverse x DFT (forward transform of the conjugate held in tr, natural layout): step A,
+// transpose, step B; out(k, w) receives the conjugated output for row k = k1 + E k2.
+template <int NX, int T, typename SP, typename OUT>
+__device__ __forceinline__ void x_inverse(float2* tr, int p, int t, const float2* stw, OUT out) {
+  constexpr int E = SP::E, P = SP::P, RS = x_row<NX, T, SP>();
+  float2 v[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = tr[(p + P * e) * T + t];
   step_a_smem<NX, E>(v, p, stw);
@@ -357,20 +386,21 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
   for (int k1 = 0; k1 < E; ++k1) tr[k1 * RS + p * T + t] = v[k1];
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < NJ; ++j) {
+  for (int j = 0; j < (E + P - 1) / P; ++j) {
     const int k1 = p + P * j;
     if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
     for (int q = 0; q < P; ++q) w[q] = tr[k1 * RS + q * T + t];
     Bfly<P>::run(w);
-    if (valid) {
 #pragma unroll
-      for (int k2 = 0; k2 < P; ++k2) gcol[(size_t)(k1 + E * k2) * xstride] = conj2(w[k2]);
-    }
+    for (int k2 = 0; k2 < P; ++k2) out(k1 + E * k2, conj2(w[k2]));
   }
+}
 
-  // deterministic block reduction of the residual partial
+// Deterministic block reduction of the residual partial into *out (thread 0 writes).
+__device__ __forceinline__ void x_block_sum(double acc, double* red, double* out) {
+  const int tid = threadIdx.x;
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if ((tid & 31) == 0) red[tid >> 5] = acc;
@@ -379,11 +409,164 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
     double w = (tid < (int)(blockDim.x + 31) / 32) ? red[tid] : 0.0;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) w += __shfl_xor_sync(0xffffffffu, w, off);
-    if (tid == 0) {
-      const int nblk = gridDim.x * gridDim.y;
-      partials[(size_t)b * nblk + blockIdx.y * gridDim.x + blockIdx.x] = w;
-    }
+    if (tid == 0) *out = w;
   }
+}
+
+// ANI: Gamma^0 of an anisotropic reference stiffness (aniso.cuh) instead of the isotropic
+// closed form.
+template <int NX, int V, bool ANI>
+__global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_blocks<NX, V>()) xpass_fast(
+    GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
+    InstanceState* __restrict__ st, double* __restrict__ partials) {
+  constexpr int E = XSplit<NX>::E, P = XSplit<NX>::P, T = x_cols_v<NX, V>(), REG = x_region<NX, T>();
+  static_assert((6 * P * T) % 32 == 0, "the x pass reduces over whole warps");
+  extern __shared__ __align__(16) unsigned char xfraw[];
+  float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
+  __shared__ double red[32];
+  __shared__ double colf[3][T];  // per-column wave-vector factors
+  // shared-memory copies of the x twiddles and wave-vector tables (read per element / mode;
+  // from shared memory the x pass is 6% faster at 128^3 than from the L1/global path)
+  __shared__ float2 stw[NX];           // exp(-2 pi i k / NX)
+  __shared__ double ssx[NX], scx[NX];  // sin, cos(pi kx / NX)
+  const int b = blockIdx.z;
+  if (!active32(st[b])) return;
+  const int tid = threadIdx.x;
+  const int t = tid % T, p = (tid / T) % P, c = tid / (T * P);
+  const int nzh = g.nzh;
+  // With nz/2+1 = T k + 1 the last tile takes the z Nyquist column for T consecutive ky
+  // instead of one column per ky (as the y pass); its surplus blocks only report a zero
+  // partial.
+  const bool tail = nzh % T == 1 && (int)blockIdx.x == nzh / T;
+  if (tail && (int)blockIdx.y * T >= g.ny) {
+    if (tid == 0) partials[(size_t)b * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x] = 0.0;
+    return;
+  }
+  auto col_ky = [&](int tt) { return tail ? (int)blockIdx.y * T + tt : (int)blockIdx.y; };
+  auto col_kz = [&](int tt) { return tail ? nzh - 1 : (int)blockIdx.x * T + tt; };
+  const int ky = col_ky(t);
+  const int kz = col_kz(t);
+  const bool valid = kz < nzh;
+  const size_t xstride = (size_t)g.ny * nzh;
+  float2* gcol = spec + (size_t)b * 6 * g.nm + (size_t)c * g.nm + (size_t)ky * nzh + kz;
+  const float2* tw = g.px.tw;
+  float2* tr = buf + (size_t)c * REG;   // this component's region
+
+  if (tid < T) {
+    // tilde(xi)_d = (2 n_d / L_d) * sin/cos products (fourier.py:9-58); the ky and kz
+    // factors of this block's columns, FP64
+    const int kzz = col_kz(tid) < nzh ? col_kz(tid) : 0;
+    const int kyy = col_ky(tid);
+    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
+    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
+    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
+  }
+
+  // forward: load, step A, transpose
+  float2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = valid ? gcol[(size_t)(p + P * e) * xstride] : make_float2(0.f, 0.f);
+  for (int i = tid; i < NX; i += blockDim.x) {
+    stw[i] = tw[i];
+    ssx[i] = g.sx[i];
+    scx[i] = g.cx[i];
+  }
+  __syncthreads();
+  x_forward<NX, T>(tr, v, p, t, stw);
+  const double acc = x_modes<NX, T, REG, ANI>(buf, colf, ssx, scx, g, med[b / g.lame_group], st, b,
+                                              col_ky, col_kz);
+  x_inverse<NX, T, XSplit<NX>>(tr, p, t, stw, [&](int k, float2 w) {
+    if (valid) gcol[(size_t)k * xstride] = w;
+  });
+  x_block_sum(acc, red, partials + (size_t)b * gridDim.x * gridDim.y + blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ----------------------------------------------------------------------------- tiled x pass
+// Split of the tiled x pass's transform: that of the strided pass, except 48 = 8 x 6 (six
+// threads per column, so that 6 components x 8 columns make whole warps).
+template <int N>
+struct XTSplit { static constexpr int E = XSplit<N>::E, P = XSplit<N>::P; };
+template <>
+struct XTSplit<48> { static constexpr int E = 8, P = 6; };
+template <int NX>
+__host__ __device__ constexpr int xt_threads() { return 6 * XTSplit<NX>::P * kTW; }
+template <int NX>
+__host__ __device__ constexpr int xt_min_blocks() { return xt_threads<NX>() <= 192 ? 4 : 2; }
+
+// Block = one tile (full tile of ky, or a tail group of 8 ky) of one instance; thread
+// (c, p, t) with t fastest.
+template <int NX, bool ANI>
+__global__ void __launch_bounds__(xt_threads<NX>(), xt_min_blocks<NX>()) xpass_tiled(
+    GridDesc g, float2* __restrict__ spec, const Medium* __restrict__ med,
+    InstanceState* __restrict__ st, double* __restrict__ partials) {
+  using SP = XTSplit<NX>;
+  constexpr int E = SP::E, P = SP::P, T = kTW, REG = x_region<NX, T, SP>();
+  static_assert((6 * P * T) % 32 == 0, "the x pass reduces over whole warps");
+  extern __shared__ __align__(128) unsigned char xtraw[];
+  float2* buf = reinterpret_cast<float2*>(xtraw);  // 6 regions of REG values
+  __shared__ double red[32];
+  __shared__ double colf[3][T];
+  __shared__ float2 stw[NX];
+  __shared__ double ssx[NX], scx[NX];
+  __shared__ __align__(8) unsigned long long mbar_word;
+  const int b = blockIdx.y;
+  if (!active32(st[b])) return;
+  const int tid = threadIdx.x;
+  const int t = tid % T, p = (tid / T) % P, c = tid / (T * P);
+  const int nzh = g.nzh, nf = (nzh - 1) / T;
+  const int tile = blockIdx.x;
+  const bool tail = tile >= g.ny * nf;
+  const int ky_full = tail ? 0 : tile / nf, j = tail ? 0 : tile % nf, grp = tail ? tile - g.ny * nf : 0;
+  auto col_ky = [&](int tt) { return tail ? grp * T + tt : ky_full; };
+  auto col_kz = [&](int tt) { return tail ? nzh - 1 : j * T + tt; };
+  const size_t chunk = tail ? (size_t)g.ny * nf * NX * T + (size_t)grp * NX * T
+                            : (size_t)(ky_full * nf + j) * NX * T;
+  float2* sb = spec + (size_t)b * 6 * g.nm;
+  float2* tr = buf + (size_t)c * REG;
+  const unsigned mbar = smem_u32(&mbar_word);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    constexpr unsigned bytes = NX * T * 8;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(6 * bytes) : "memory");
+    for (int cc = 0; cc < 6; ++cc) bulk_g2s(buf + (size_t)cc * REG, sb + (size_t)cc * g.nm + chunk, bytes, mbar);
+  }
+  if (tid < T) {
+    const int kzz = col_kz(tid), kyy = col_ky(tid);
+    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
+    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
+    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
+  }
+  for (int i = tid; i < NX; i += blockDim.x) {
+    stw[i] = g.px.tw[i];
+    ssx[i] = g.sx[i];
+    scx[i] = g.cx[i];
+  }
+  if (!mbar_wait(mbar)) {
+    // the copies did not land in time: report, leave the instance stopped, and wait once
+    // more (bounded) before the shared memory is released
+    if (tid == 0) {
+      st[b].status = kTimeout;
+      st[b].done = 1;
+    }
+    if (!mbar_wait(mbar) && tid == 0) st[b].copies_lost = 1;
+    if (tid == 0) partials[(size_t)b * gridDim.x + tile] = 0.0;
+    return;
+  }
+  __syncthreads();
+  float2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = tr[(p + P * e) * T + t];
+  __syncthreads();
+  x_forward<NX, T, SP>(tr, v, p, t, stw);
+  const double acc = x_modes<NX, T, REG, ANI>(buf, colf, ssx, scx, g, med[b / g.lame_group], st, b,
+                                              col_ky, col_kz);
+  float2* gout = sb + (size_t)c * g.nm + chunk;
+  x_inverse<NX, T, SP>(tr, p, t, stw, [&](int k, float2 w) { gout[(size_t)k * T + t] = w; });
+  x_block_sum(acc, red, partials + (size_t)b * gridDim.x + tile);
 }
 
 // ----------------------------------------------------------------------------- z pass
@@ -426,10 +609,6 @@ __host__ __device__ constexpr ZLayout z_layout() {
   return ZLayout{0, zb, zb + rs, zb + rs + es, zb + rs + es + ls};
 }
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
 // In-place four-step FFT of the 3L lines of zbuf (natural order in and out).
 template <int NZ>
 __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const float2* __restrict__ tw) {
@@ -463,26 +642,6 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
       for (int k2 = 0; k2 < P; ++k2) line[(p + P * j) + E * k2] = o[j * P + k2];
     }
   __syncthreads();
-}
-
-// Bounded wait on a one-shot mbarrier (phase 0). Returns false if the copies did not
-// complete within the limit.
-__device__ __forceinline__ bool mbar_wait(unsigned mbar) {
-  for (long long spin = 0; spin < (1LL << 24); ++spin) {
-    unsigned done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done) : "r"(mbar), "r"(0u) : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned mbar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
 // Modes as the generic z pass: 0 init from eps_bar/eps0, 1 plain update, 2 keep eps
@@ -728,6 +887,19 @@ int x_tiles(const GridDesc& g, int variant) {
   }
 }
 
+bool tiled_supported(const GridDesc& g) {
+  return supported(g) && g.nx <= 128 && g.ny % kTW == 0 && (g.nzh - 1) % kTW == 0;
+}
+
+int x_tiles_tiled(const GridDesc& g) { return g.ny * ((g.nzh - 1) / kTW) + g.ny / kTW; }
+
+size_t tile_index(const GridDesc& g, int x, int ky, int kz) {
+  return tile_offset(g.nx, g.ny, (g.nzh - 1) / kTW, x, ky, kz);
+}
+
+template <int N>
+static size_t xtsmem() { return (size_t)6 * x_region<N, kTW, XTSplit<N>>() * sizeof(float2); }
+
 template <int N>
 static size_t zsmem() { return z_layout<N>().total; }
 template <int N>
@@ -749,6 +921,10 @@ static cudaError_t configure_n() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
+  if constexpr (N <= 128) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_tiled<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xtsmem<N>());
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_tiled<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xtsmem<N>());
+  }
   return e;
 }
 
@@ -813,24 +989,27 @@ int z_blocks(const GridDesc& g) {
 }
 
 template <int N>
-static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
-                    cudaStream_t s) {
+static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+                    const InstanceState* st, cudaStream_t s) {
   // with a one-column tail, full tiles + one tail tile (see ypass_fast)
   constexpr int YT = y_cols<N>();
   dim3 grid(g.nzh % YT == 1 ? g.nzh / YT + 1 : (g.nzh + YT - 1) / YT, g.nx, 6 * batch);
-  ypass_fast<N><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, st);
+  if (tspec)
+    ypass_fast<N, true><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, tspec, st);
+  else
+    ypass_fast<N, false><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, spec, st);
 }
 
-void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
-                  cudaStream_t s) {
+void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+                  const InstanceState* st, cudaStream_t s) {
   switch (g.ny) {
-    case 16: ylaunch<16>(g, inverse, batch, spec, st, s); break;
-    case 32: ylaunch<32>(g, inverse, batch, spec, st, s); break;
-    case 48: ylaunch<48>(g, inverse, batch, spec, st, s); break;
-    case 96: ylaunch<96>(g, inverse, batch, spec, st, s); break;
-    case 64: ylaunch<64>(g, inverse, batch, spec, st, s); break;
-    case 128: ylaunch<128>(g, inverse, batch, spec, st, s); break;
-    default: ylaunch<256>(g, inverse, batch, spec, st, s); break;
+    case 16: ylaunch<16>(g, inverse, batch, spec, tspec, st, s); break;
+    case 32: ylaunch<32>(g, inverse, batch, spec, tspec, st, s); break;
+    case 48: ylaunch<48>(g, inverse, batch, spec, tspec, st, s); break;
+    case 96: ylaunch<96>(g, inverse, batch, spec, tspec, st, s); break;
+    case 64: ylaunch<64>(g, inverse, batch, spec, tspec, st, s); break;
+    case 128: ylaunch<128>(g, inverse, batch, spec, tspec, st, s); break;
+    default: ylaunch<256>(g, inverse, batch, spec, tspec, st, s); break;
   }
 }
 
@@ -850,6 +1029,30 @@ static void xlaunch_v(int variant, const GridDesc& g, int batch, float2* spec, c
                       InstanceState* st, double* partials, cudaStream_t s) {
   if (variant) xlaunch<N, 1>(g, batch, spec, med, st, partials, s);
   else xlaunch<N, 0>(g, batch, spec, med, st, partials, s);
+}
+
+template <int N>
+static void xtlaunch(const GridDesc& g, int batch, float2* tspec, const Medium* med, InstanceState* st,
+                     double* partials, cudaStream_t s) {
+  if constexpr (N <= 128) {
+    dim3 grid((unsigned)x_tiles_tiled(g), batch);
+    if (g.c0)
+      xpass_tiled<N, true><<<grid, xt_threads<N>(), xtsmem<N>(), s>>>(g, tspec, med, st, partials);
+    else
+      xpass_tiled<N, false><<<grid, xt_threads<N>(), xtsmem<N>(), s>>>(g, tspec, med, st, partials);
+  }
+}
+
+void launch_xpass_tiled(const GridDesc& g, int batch, float2* tspec, const Medium* med,
+                        InstanceState* st, double* partials, cudaStream_t s) {
+  switch (g.nx) {
+    case 16: xtlaunch<16>(g, batch, tspec, med, st, partials, s); break;
+    case 32: xtlaunch<32>(g, batch, tspec, med, st, partials, s); break;
+    case 48: xtlaunch<48>(g, batch, tspec, med, st, partials, s); break;
+    case 96: xtlaunch<96>(g, batch, tspec, med, st, partials, s); break;
+    case 64: xtlaunch<64>(g, batch, tspec, med, st, partials, s); break;
+    default: xtlaunch<128>(g, batch, tspec, med, st, partials, s); break;
+  }
 }
 
 void launch_xpass(const GridDesc& g, int variant, int batch, float2* spec, const Medium* med,

@@ -16,8 +16,19 @@ int z_blocks(const GridDesc& g);
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
                   float* eps, float2* spec, const double* eps_bar, const float* eps0,
                   InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s);
-void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, const InstanceState* st,
-                  cudaStream_t s);
+// tspec != nullptr: the x-pass side is the tiled layout in tspec (the forward pass writes
+// it, the inverse pass reads it); otherwise the transform runs in place on spec.
+void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+                  const InstanceState* st, cudaStream_t s);
+// The tiled spectrum layout between the y and x passes applies (nx <= 128, ny and nz/2 a
+// multiple of 8, every extent supported).
+bool tiled_supported(const GridDesc& g);
+// x-pass blocks per instance over the tiled layout (every tile one block).
+int x_tiles_tiled(const GridDesc& g);
+// Offset of mode (x, ky, kz) of one component in the tiled layout.
+size_t tile_index(const GridDesc& g, int x, int ky, int kz);
+void launch_xpass_tiled(const GridDesc& g, int batch, float2* tspec, const Medium* med,
+                        InstanceState* st, double* partials, cudaStream_t s);
 void launch_xpass(const GridDesc& g, int variant, int batch, float2* spec, const Medium* med,
                   InstanceState* st, double* partials, cudaStream_t s);
 

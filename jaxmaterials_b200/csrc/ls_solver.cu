@@ -205,7 +205,9 @@ int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]) {
   s->x_blocks_generic32 = s->sh32.x_blocks_per_instance;
   s->sh64 = plan_launch(g, sizeof(double2));
   s->fast32 = fast::supported(g);
-  if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g, s->xvariant) * g.ny;
+  s->tiled = s->tiled_allowed && s->fast32 && fast::tiled_supported(g);
+  if (s->tiled) s->sh32.x_blocks_per_instance = fast::x_tiles_tiled(g);
+  else if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g, s->xvariant) * g.ny;
   if (!shape_fits(s->sh32) || !shape_fits(s->sh64))
     return fail(-1, "grid %dx%dx%d needs FFT blocks above %d threads", g.nx, g.ny, g.nz, kMaxThreads);
   cudaError_t e = configure_kernels();
@@ -293,10 +295,12 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   // room for the partials of either x-pass tile variant
   const size_t xblk = (size_t)std::max({s->sh32.x_blocks_per_instance, s->sh64.x_blocks_per_instance,
                                         s->x_blocks_generic32,
-                                        s->fast32 ? fast::x_tiles(g, 1) * g.ny : 0});
+                                        s->fast32 ? fast::x_tiles(g, 1) * g.ny : 0,
+                                        s->fast32 && fast::tiled_supported(g) ? fast::x_tiles_tiled(g) : 0});
   const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
   bool ok = alloc((void**)&s->d_eps32, sizeof(float) * B * 6 * g.nv) &&
             alloc((void**)&s->d_spec32, sizeof(float2) * B * 6 * g.nm) &&
+            (!s->tiled || alloc((void**)&s->d_tspec32, sizeof(float2) * B * 6 * g.nm)) &&
             alloc((void**)&s->d_partials, sizeof(double) * B * xblk) &&
             alloc((void**)&s->d_state, sizeof(InstanceState) * B) &&
             alloc((void**)&s->d_medium, sizeof(Medium) * B) &&
@@ -372,7 +376,8 @@ template <typename T>
 void pass_y(lsb_solver* s, bool inverse, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
     if (use_fast32(s)) {
-      fast::launch_ypass(s->g, inverse, batch, spec, s->d_state, s->stream);
+      fast::launch_ypass(s->g, inverse, batch, spec, s->tiled ? s->d_tspec32 : nullptr, s->d_state,
+                         s->stream);
       return;
     }
   }
@@ -383,6 +388,11 @@ template <typename T>
 void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
     if (use_fast32(s)) {
+      if (s->tiled) {
+        fast::launch_xpass_tiled(s->g, batch, s->d_tspec32, s->d_medium, s->d_state, s->d_partials,
+                                 s->stream);
+        return;
+      }
       fast::launch_xpass(s->g, s->xvariant, batch, spec, s->d_medium, s->d_state, s->d_partials,
                          s->stream);
       return;
@@ -572,6 +582,7 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
 int tune_xpass(lsb_solver* s, int batch) {
   if (!use_fast32(s)) return 0;  // the generic passes have no tile variants
   s->xtuned = true;
+  if (s->tiled) return 0;        // one form of the x pass over the tiled layout
   if (fast::x_tiles(s->g, 0) == fast::x_tiles(s->g, 1)) return 0;
   cudaStream_t st = s->stream;
   cudaEvent_t ev[2];
@@ -807,9 +818,24 @@ int lsb_tile_variant(lsb_solver* solver, int variant) {
     if (!solver->fast32) return solver->xvariant;
     solver->xvariant = variant;
     solver->xtuned = true;
-    solver->sh32.x_blocks_per_instance = fast::x_tiles(solver->g, variant) * solver->g.ny;
+    if (!solver->tiled)
+      solver->sh32.x_blocks_per_instance = fast::x_tiles(solver->g, variant) * solver->g.ny;
   }
   return solver->xvariant;
+}
+
+int lsb_set_tiled(lsb_solver* solver, int on) {
+  if (!solver) return fail(-1, "null solver");
+  lsb_solver* s = solver;
+  const bool want = on != 0 && s->fast32 && fast::tiled_supported(s->g);
+  if (want && !s->d_tspec32) {
+    if (!s->owns_memory) return fail(-1, "this solver cannot allocate the tiled spectrum");
+    LSB_CUDA(cudaMalloc(&s->d_tspec32, sizeof(float2) * (size_t)s->batch_cap * 6 * s->g.nm));
+  }
+  s->tiled = want;
+  if (s->tiled) s->sh32.x_blocks_per_instance = fast::x_tiles_tiled(s->g);
+  else if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(s->g, s->xvariant) * s->g.ny;
+  return s->tiled ? 1 : 0;
 }
 
 int lsb_set_warm_history(lsb_solver* solver, int on) {

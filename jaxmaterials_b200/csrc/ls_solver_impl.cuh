@@ -21,6 +21,10 @@ struct lsb_solver {
   // k > 0 = instance b uses structure b / k of [structure][nv] Lame arrays
   int lame_group = 0;
   bool fast32 = false;   // FP32 passes with compile-time lengths (fast_passes.cu)
+  // the fast passes keep the spectrum between the y and x passes in the tiled layout
+  // (d_tspec32); tiled_allowed = false keeps the strided x pass (no second spectrum buffer)
+  bool tiled = false;
+  bool tiled_allowed = true;
   int xvariant = 0;      // x-pass tile variant of the fast passes (chosen by timing)
   bool xtuned = false;   // xvariant has been chosen
   bool warm_history = false;  // d_eps0 enters the Anderson history instead of starting it
@@ -35,6 +39,7 @@ struct lsb_solver {
   // FP32 work buffers
   float* d_eps32 = nullptr;      // [batch][6][nv] (used when the caller passes no strain buffer)
   float2* d_spec32 = nullptr;    // [batch][6][nm]
+  float2* d_tspec32 = nullptr;   // [batch][6][nm], tiled layout (tiled solvers only)
   // FP64 work buffers, allocated on first use
   double* d_eps64 = nullptr;
   double2* d_spec64 = nullptr;
@@ -97,7 +102,7 @@ struct lsb_solver {
 
   ~lsb_solver() {
     if (!owns_memory) return;
-    void* bufs[] = {d_eps32, d_spec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
+    void* bufs[] = {d_eps32, d_spec32, d_tspec32, d_eps64, d_spec64, d_lame64, d_partials, d_state, d_medium,
                     d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
                     d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
                     d_aa_alpha, d_e0ref, d_dmg_conv, d_pf_w, d_pf_chi, d_pf_part, d_pf_state,

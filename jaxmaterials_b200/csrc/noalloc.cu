@@ -146,6 +146,7 @@ extern "C" int lsb_solve_noalloc(const int voxels[3], const double extents[3], i
   s.precision = kPrecFP32;
   s.h_state = g_host_state;
   s.stream = static_cast<cudaStream_t>(stream);
+  s.tiled_allowed = false;  // one spectrum buffer: the strided x pass
   rc = plan_grid(&s, voxels, extents);
   if (rc) return rc;
   const GridDesc& g = s.g;

@@ -144,6 +144,11 @@ class Solver:
         return _lib.check(self._lib.lsb_tile_variant(self._h, -1 if variant is None else int(variant)),
                           "lsb_tile_variant")
 
+    def set_tiled(self, on=True):
+        """Tiled spectrum layout between the y and x passes (the default where it applies;
+        results are bit-identical either way). Returns whether it is in use."""
+        return bool(_lib.check(self._lib.lsb_set_tiled(self._h, 1 if on else 0), "lsb_set_tiled"))
+
     def set_warm_history(self, on=True):
         """With on, a warm start (``epsilon0``) enters the Anderson history as the second
         iterate instead of starting the iteration (needs depth >= 1)."""

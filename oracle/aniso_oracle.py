@@ -7,9 +7,11 @@ doc/anisotropic.py:150-185, stress sigma_a = sum_b C_ab w_b eps_b (w = 1, 1, 1, 
 acoustic matrix K_ki = C^0_kjil xi_j xi_l of the normalised modified wave vector,
 Gamma^0 tau = sym(xi (x) K^-1 tau xi) (doc/anisotropic.py:98-128, for an isotropic C^0 equal
 to fourier.py:115-186), r = -Gamma^0 tau, zero where xi has no direction. The reference has
-no anisotropic solver, so this oracle is pinned only through the isotropic reduction (an
-isotropic stiffness reproduces ls_oracle, which is pinned to the reference) and through
-its formulas' properties (parity unpinned for genuinely anisotropic materials).
+no anisotropic solver; it derives these formulas symbolically in doc/anisotropic.py. This
+oracle is pinned to that derivation: its stress law, acoustic matrix and Gamma^0 equal the
+reference's sympy expressions evaluated in FP64 on seeded stiffnesses and wave vectors
+(tests/golden/reference_aniso.npz, made by tests/golden/make_aniso_golden.py), and an
+isotropic stiffness reproduces ls_oracle, which is pinned to the reference's solver.
 """
 
 import numpy as np
@@ -53,8 +55,9 @@ def stress(c21, eps):
     return np.einsum("ab...,b...->a...", m, w * eps).astype(eps.dtype)
 
 
-def gamma_solve(tau_hat, c0, xizero):
-    """r_hat = -Gamma^0 tau_hat for a constant reference stiffness c0 (21,)."""
+def acoustic_matrix(c0, xizero):
+    """K_ki = C^0_kjil xi_j xi_l (doc/anisotropic.py:46-95) for a constant reference
+    stiffness c0 (21,) and wave vectors xizero (3, ...); shape (..., 3, 3)."""
     m = matrix_from_c21(np.asarray(c0, dtype=np.float64))
     c4 = np.zeros((3, 3, 3, 3))
     for p in range(3):
@@ -63,7 +66,13 @@ def gamma_solve(tau_hat, c0, xizero):
                 for s in range(3):
                     c4[p, q, r, s] = m[voigt_of(p, q), voigt_of(r, s)]
     z = np.asarray(xizero, dtype=np.float64)
-    k = np.einsum("kjil,j...,l...->...ki", c4, z, z)
+    return np.einsum("kjil,j...,l...->...ki", c4, z, z)
+
+
+def gamma_solve(tau_hat, c0, xizero):
+    """r_hat = -Gamma^0 tau_hat for a constant reference stiffness c0 (21,)."""
+    z = np.asarray(xizero, dtype=np.float64)
+    k = acoustic_matrix(c0, z)
     nrm2 = np.sum(z * z, axis=0)
     ok = nrm2 > 0.5  # unit vectors; the zero mode and guarded modes have |xi| ~ 0
     kk = np.where(ok[..., None, None], k, np.eye(3))

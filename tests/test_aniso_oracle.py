@@ -1,8 +1,15 @@
-"""The anisotropic oracle (oracle/aniso_oracle.py): it reduces to the pinned isotropic oracle
-for isotropic stiffnesses, and its Gamma^0 has the defining properties of the Green operator
-of the reference medium (no GPU)."""
+"""The anisotropic oracle (oracle/aniso_oracle.py): its stress law, acoustic matrix and
+Gamma^0 equal the reference's own symbolic derivation (doc/anisotropic.py, evaluated by
+tests/golden/make_aniso_golden.py into tests/golden/reference_aniso.npz); it reduces to
+the pinned isotropic oracle for isotropic stiffnesses, and its Gamma^0 has the defining
+properties of the Green operator of the reference medium (no GPU)."""
+
+import os
 
 import numpy as np
+import pytest
+
+from tests.conftest import ROOT
 
 from tests.aniso_materials import c21_of_tensor, fibre_tensor, two_phase_field
 
@@ -66,3 +73,40 @@ def test_anisotropic_solve_converges_and_c_eff_is_symmetric():
     w = np.diag([1, 1, 1, 2, 2, 2])
     b = ceff @ w  # symmetric in the energy pairing
     assert np.abs(b - b.T).max() < 1e-6 * np.abs(b).max()
+
+
+@pytest.fixture(scope="module")
+def aniso_gold():
+    with np.load(os.path.join(ROOT, "tests", "golden", "reference_aniso.npz")) as d:
+        return {k: d[k] for k in d.files}
+
+
+def test_stress_law_matches_reference_derivation(aniso_gold):
+    from oracle import aniso_oracle as A
+
+    g = aniso_gold
+    got = A.stress(g["c21"].T, g["eps"].T).T
+    assert np.abs(got - g["sigma"]).max() < 1e-13 * np.abs(g["sigma"]).max()
+
+
+def test_acoustic_matrix_matches_reference_derivation(aniso_gold):
+    from oracle import aniso_oracle as A
+
+    g = aniso_gold
+    for s in range(g["c0"].shape[0]):
+        k = A.acoustic_matrix(g["c0"][s], g["xi"][s])
+        assert np.abs(k - g["K"][s]).max() < 1e-13 * np.abs(g["K"][s]).max()
+
+
+def test_gamma_matches_reference_derivation(aniso_gold):
+    """Column b of Gamma^0 (Voigt pairs, the reference's Gamma^0_klij) is -r for
+    tau = e_b / w_b, since (Gamma^0 tau)_a = sum_b Gamma_ab w_b tau_b with tensor shear."""
+    from oracle import aniso_oracle as A
+
+    g = aniso_gold
+    w = np.array([1.0, 1.0, 1.0, 2.0, 2.0, 2.0])
+    for s in range(g["c0"].shape[0]):
+        tau = np.diag(1.0 / w)                       # column b: e_b / w_b
+        z = np.repeat(g["xi"][s][:, None], 6, axis=1)
+        cols = -A.gamma_solve(tau, g["c0"][s], z)    # (6, 6): [a, b]
+        assert np.abs(cols - g["gamma"][s]).max() < 1e-12 * np.abs(g["gamma"][s]).max()

@@ -462,6 +462,7 @@ def test_x_tile_variants_agree(ls, n):
     out = []
     for v in (0, 1):
         s = Solver(g, batch=1)
+        s.set_tiled(False)  # the variants belong to the strided x pass
         assert s.tile_variant(v) == v
         r = s.solve(lm, mu, EPS_BAR, rtol=1e-20, atol=1e-5, maxiter=12, want_sigma=False)
         out.append((r.epsilon.clone(), r.iters.copy()))
@@ -470,6 +471,34 @@ def test_x_tile_variants_agree(ls, n):
     s = Solver(g, batch=1)
     s.solve(lm, mu, EPS_BAR, rtol=1e-20, atol=1e-5, maxiter=2, want_sigma=False)
     assert s.tile_variant() in (0, 1)
+
+
+@pytest.mark.parametrize("depth", [0, 3])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 48), (32, 16, 96), (48, 32, 64), (96, 48, 16)])
+def test_tiled_layout_matches_strided(ls, n, depth):
+    """The tiled spectrum layout between the y and x passes gives the fields of the strided
+    x pass: bit for bit where both passes split the x transform alike, and to FP32
+    round-off for nx = 48 (8 x 6 against 16 x 3); fixed number of updates."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import Solver
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    eb = np.tile(EPS_BAR, (2, 1))
+    out = []
+    for tiled in (True, False):
+        s = Solver(g, batch=2, depth=depth)
+        assert s.set_tiled(tiled) == tiled
+        s.tile_variant(0)
+        r = s.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=12)
+        out.append((r.epsilon.clone(), r.sigma.clone(), r.iters.copy()))
+        s.close()
+    assert (out[0][2] == out[1][2]).all()
+    if n[0] == 48:
+        assert relmax(out[0][0].cpu().numpy(), out[1][0].cpu().numpy()) < 2e-6
+    else:
+        assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
 
 
 @pytest.mark.parametrize("depth", [0, 3])
