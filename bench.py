@@ -388,6 +388,10 @@ def kernel_bytes(name, nv, nm, batch, depth):
         "anderson solve": 0,
         "anderson combine": batch * (m1 * real + real),      # every g slot in, eps out
         "z pass stress": batch * (real + spec) + lame,        # eps in, spectrum out
+        # fused slab pass: the z pass's bytes (the y transforms stay on chip)
+        "slab update": batch * (2 * spec + 2 * real) + lame,
+        "slab residual rings": batch * (spec + real + 2 * real),
+        "slab stress": batch * (real + spec) + lame,
     }
     if name not in table:
         raise KeyError(f"no algorithmic byte count for kernel {name!r}")

@@ -11,6 +11,8 @@
 // size and for FP64 fields.
 #include <cmath>
 
+#include <cooperative_groups.h>
+
 #include "aniso.cuh"
 #include "damage.cuh"
 #include "fast_passes.cuh"
@@ -93,14 +95,14 @@ __device__ __forceinline__ void step_a_smem(float2* v, int p, const float2* tw) 
 // The tiled spectrum layout (grids with nx <= 128 and nz/2+1 = 8 k + 1, ny = 8 k'), written
 // by the forward y pass and read by the inverse y pass, and in place by this x pass: per
 // instance and component,
-//   full tiles   [ky][j][x][t]   kz = 8 j + t, j < NF = (nz/2+1 - 1) / 8
+//   full tiles   [j][ky][x][t]   kz = 8 j + t, j < NF = (nz/2+1 - 1) / 8
 //   tail         [ky / 8][x][ky % 8]   the z Nyquist column kz = nz/2
 // (tile_offset below). Every tile of the x pass is then one contiguous chunk of 8 nx complex
 // values per component, fetched with one bulk copy.
 constexpr int kTW = 8;
 
 __host__ __device__ __forceinline__ size_t tile_offset(int nx, int ny, int nf, int x, int ky, int kz) {
-  if (kz < nf * kTW) return ((size_t)(ky * nf + kz / kTW) * nx + x) * kTW + (kz % kTW);
+  if (kz < nf * kTW) return ((size_t)((kz / kTW) * ny + ky) * nx + x) * kTW + (kz % kTW);
   return (size_t)ny * nf * nx * kTW + ((size_t)(ky / kTW) * nx + x) * kTW + (ky % kTW);
 }
 
@@ -154,16 +156,20 @@ __global__ void __launch_bounds__(y_threads<NY>(),
   if (!active32(st[bc / 6])) return;
   const int t = threadIdx.x % YT, p = threadIdx.x / YT;
   const int nzh = g.nzh;
+  // grid: (kz tiles, x) for the in-place form; (x, kz tiles) for the tiled form, so that
+  // consecutive blocks write neighbouring tile rows
+  const int bx = TILED ? (int)blockIdx.y : (int)blockIdx.x;
+  const int by = TILED ? (int)blockIdx.x : (int)blockIdx.y;
   int kz, x;
   bool valid;
-  if (nzh % YT == 1 && (int)blockIdx.x == nzh / YT) {
-    if ((int)blockIdx.y * YT >= g.nx) return;
+  if (nzh % YT == 1 && bx == nzh / YT) {
+    if (by * YT >= g.nx) return;
     kz = nzh - 1;
-    x = blockIdx.y * YT + t;
+    x = by * YT + t;
     valid = x < g.nx;
   } else {
-    kz = blockIdx.x * YT + t;
-    x = blockIdx.y;
+    kz = bx * YT + t;
+    x = by;
     valid = kz < nzh;
   }
   float2* base = spec + ((size_t)bc * g.nx + x) * (size_t)NY * nzh + kz;
@@ -173,7 +179,7 @@ __global__ void __launch_bounds__(y_threads<NY>(),
   const bool ncol = kz >= nf * kTW;
   float2* tb = tspec + (size_t)bc * g.nm + tile_offset(g.nx, NY, nf, x, 0, kz);
   const int sh = ncol ? 3 : 0, mk = ncol ? kTW - 1 : 0;
-  const int ta = ncol ? g.nx * kTW : nf * g.nx * kTW;
+  const int ta = g.nx * kTW;
   auto tptr = [&](int ky) { return tb + (size_t)((ky >> sh) * ta + (ky & mk)); };
   const float2* tw = g.py.tw;
   float2 v[E];
@@ -516,11 +522,11 @@ __global__ void __launch_bounds__(xt_threads<NX>(), xt_min_blocks<NX>()) xpass_t
   const int nzh = g.nzh, nf = (nzh - 1) / T;
   const int tile = blockIdx.x;
   const bool tail = tile >= g.ny * nf;
-  const int ky_full = tail ? 0 : tile / nf, j = tail ? 0 : tile % nf, grp = tail ? tile - g.ny * nf : 0;
+  const int ky_full = tail ? 0 : tile % g.ny, j = tail ? 0 : tile / g.ny, grp = tail ? tile - g.ny * nf : 0;
   auto col_ky = [&](int tt) { return tail ? grp * T + tt : ky_full; };
   auto col_kz = [&](int tt) { return tail ? nzh - 1 : j * T + tt; };
   const size_t chunk = tail ? (size_t)g.ny * nf * NX * T + (size_t)grp * NX * T
-                            : (size_t)(ky_full * nf + j) * NX * T;
+                            : (size_t)(j * g.ny + ky_full) * NX * T;
   float2* sb = spec + (size_t)b * 6 * g.nm;
   float2* tr = buf + (size_t)c * REG;
   const unsigned mbar = smem_u32(&mbar_word);
@@ -860,6 +866,297 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
   }
 }
 
+// ----------------------------------------------------------------------------- slab pass
+// The inverse y pass, the z pass and the forward y pass of one x-plane of one instance in
+// one kernel: a thread-block cluster of CS = nz / 16 blocks holds the plane's half
+// spectrum, 6 x ny x (nz/2+1) complex values, in distributed shared memory, rank r owning
+// the kz columns of tile r (8 columns, read from and written to the tiled layout as one
+// 64-byte row per (component, ky)) and, on the last rank, the z Nyquist column; and the
+// ny / CS rows y in [r ny / CS, (r+1) ny / CS) for the z transforms.
+//   phase A  inverse y DFT of the rank's columns (in place in shared memory)
+//   phase B  per batch of R rows: gather the rows' half spectra from the ranks' columns,
+//            inverse z transform (two components per complex line), the pointwise stage
+//            of the mode, forward z transform, scatter the half spectra back
+//   phase C  forward y DFT of the rank's columns, store
+// Modes as the z pass: 0 init (eps from eps_bar or eps0), 1 plain update, 2 stress of the
+// eps in memory (after the Anderson combine), 3 Anderson residual into the rings (phases A
+// and B, no forward transforms). The arithmetic is that of ypass_fast and zpass_fast
+// (same splits, same order), so the fields equal theirs bit for bit; the spectrum never
+// leaves the plane between the y and z transforms, which saves their two HBM round trips.
+namespace cg = cooperative_groups;
+
+constexpr int kSlabKW = kTW + 1;  // local columns per rank: one tile and the Nyquist slot
+constexpr int kSlabR = 8;         // rows per batch of phase B
+
+template <int NZ>
+__host__ __device__ constexpr int slab_ranks() { return NZ / 2 / kTW; }
+template <int NZ>
+__host__ __device__ constexpr int slab_threads() { return 3 * kSlabR * Split<NZ>::P; }
+
+struct SlabLayout {  // byte offsets inside the slab kernel's dynamic shared memory
+  size_t cols, zbuf, total;
+};
+template <int NY, int NZ>
+__host__ __device__ constexpr SlabLayout slab_layout() {
+  constexpr size_t cols = (size_t)6 * NY * kSlabKW * 8;
+  constexpr size_t zb = (size_t)3 * kSlabR * z_ld<NZ>() * 8;
+  return SlabLayout{0, cols, cols + zb};
+}
+
+// In-place y DFT of the ncols columns of `cols` ([6][NY][kSlabKW], column q = (c, kk) with
+// kk < kw) by groups of P threads; forward, or inverse through the conjugates. Same
+// arithmetic as ypass_fast.
+template <int NY>
+__device__ __forceinline__ void slab_ydft(float2* cols, int kw, bool inverse, const float2* __restrict__ tw) {
+  constexpr int E = YSplit<NY>::E, P = YSplit<NY>::P, NJ = (E + P - 1) / P;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int per_round = nt / P;
+  const int ncols = 6 * kw;
+  const int p = tid % P, qq = tid / P;
+  for (int base = 0; base < ncols; base += per_round) {
+    const int q = base + qq;
+    const bool on = qq < per_round && q < ncols;
+    float2* col = cols + (on ? ((size_t)(q / kw) * NY * kSlabKW + (q % kw)) : 0);
+    float2 v[E];
+    if (on) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const float2 a = col[(size_t)(p + P * e) * kSlabKW];
+        v[e] = inverse ? conj2(a) : a;
+      }
+    }
+    __syncthreads();
+    if (on) {
+      step_a<NY, E>(v, p, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) col[(size_t)(k1 * P + p) * kSlabKW] = v[k1];
+    }
+    __syncthreads();
+    float2 o[NJ * P];
+    if (on) {
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) {
+        const int k1 = p + P * j;
+        if (k1 >= E) break;
+        float2 w[P];
+#pragma unroll
+        for (int q2 = 0; q2 < P; ++q2) w[q2] = col[(size_t)(k1 * P + q2) * kSlabKW];
+        Bfly<P>::run(w);
+#pragma unroll
+        for (int k2 = 0; k2 < P; ++k2) o[j * P + k2] = inverse ? conj2(w[k2]) : w[k2];
+      }
+    }
+    __syncthreads();
+    if (on) {
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) {
+        const int k1 = p + P * j;
+        if (k1 >= E) break;
+#pragma unroll
+        for (int k2 = 0; k2 < P; ++k2) col[(size_t)(k1 + E * k2) * kSlabKW] = o[j * P + k2];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int NY, int NZ, int MODE>
+__global__ void __launch_bounds__(slab_threads<NZ>(), 1) slab_fast(
+    GridDesc g, const float* __restrict__ lambda, const float* __restrict__ mu,
+    float* __restrict__ eps, float2* __restrict__ tspec, const double* __restrict__ eps_bar,
+    const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med,
+    AndersonArgs<float> aa) {
+  constexpr int CS = slab_ranks<NZ>(), NZH = NZ / 2 + 1, LD = z_ld<NZ>(), R = kSlabR;
+  constexpr int P = Split<NZ>::P, ROWS = NY / CS, NF = NZ / 2 / kTW;
+  constexpr SlabLayout LY = slab_layout<NY, NZ>();
+  static_assert(ROWS % R == 0, "rows per rank must be whole batches");
+  extern __shared__ __align__(128) unsigned char slraw[];
+  float2* cols = reinterpret_cast<float2*>(slraw + LY.cols);  // [6][NY][kSlabKW]
+  float2* zbuf = reinterpret_cast<float2*>(slraw + LY.zbuf);  // 3R lines of LD values
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int x = blockIdx.y, b = blockIdx.z;
+  // uniform over the cluster (all ranks read the same state): no rank reaches a cluster
+  // barrier that the others skip
+  if (!active32(st[b])) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int nx = g.nx;
+  const long long nv = g.nv;
+  const int kw = rank == CS - 1 ? kTW + 1 : kTW;  // used local columns
+  float2* tb = tspec + (size_t)b * 6 * g.nm;
+  float* eb = eps + (size_t)b * 6 * nv;
+  const size_t tail0 = (size_t)NY * NF * nx * kTW;
+  constexpr bool kInverse = MODE == 1 || MODE == 3;
+  constexpr bool kForward = MODE != 3;
+
+  // ---- phase A: the rank's columns (tile `rank`, and the Nyquist column on the last rank)
+  if constexpr (kInverse) {
+    for (int i = tid; i < 6 * NY * (kTW / 2); i += nt) {
+      const int c = i / (NY * (kTW / 2)), rem = i % (NY * (kTW / 2));
+      const int ky = rem / (kTW / 2), h = rem % (kTW / 2);
+      const float4 v = *reinterpret_cast<const float4*>(
+          tb + (size_t)c * g.nm + ((size_t)(rank * NY + ky) * nx + x) * kTW + 2 * h);
+      float2* d = cols + ((size_t)c * NY + ky) * kSlabKW + 2 * h;
+      d[0] = make_float2(v.x, v.y);
+      d[1] = make_float2(v.z, v.w);
+    }
+    if (rank == CS - 1) {
+      for (int i = tid; i < 6 * NY; i += nt) {
+        const int c = i / NY, ky = i % NY;
+        cols[((size_t)c * NY + ky) * kSlabKW + kTW] =
+            tb[(size_t)c * g.nm + tail0 + ((size_t)(ky / kTW) * nx + x) * kTW + (ky % kTW)];
+      }
+    }
+    __syncthreads();
+    slab_ydft<NY>(cols, kw, true, g.py.tw);
+  }
+  cluster.sync();
+
+  // ---- phase B: rows of this rank, R at a time
+  const int q = tid / P, p = tid % P;
+  const float inv_nv = (float)(1.0 / (double)nv);
+  float shift[6];
+  if constexpr (MODE == 0) {
+    const double* e = eps_bar + 6 * b;
+    const double tr = e[0] + e[1] + e[2];
+    const Medium& md = med[b / g.lame_group];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) shift[c] = (float)((c < 3 ? md.lmean * tr : 0.0) + 2.0 * md.mmean * e[c]);
+    if (x == 0 && rank == 0 && tid == 0) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) st[b].shift[c] = (double)shift[c];
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) shift[c] = (float)st[b].shift[c];
+  }
+  const float* lam = lambda + (size_t)(b / g.lame_group) * nv;
+  const float* muf = mu + (size_t)(b / g.lame_group) * nv;
+  int slot = 0;
+  float *rb = nullptr, *gb = nullptr;
+  if constexpr (MODE == 3) {
+    const int M1 = aa.depth + 1;
+    slot = (st[b].iter - 1 - st[b].aa_base) % M1;
+    rb = aa.r + (size_t)b * M1 * 6 * nv + (size_t)slot * 6 * nv;
+    gb = aa.g + (size_t)b * M1 * 6 * nv + (size_t)slot * 6 * nv;
+  }
+  // owner rank and local column of half-spectrum column k
+  auto owner = [&](int k) { return k < NF * kTW ? k / kTW : CS - 1; };
+  auto local = [&](int k) { return k < NF * kTW ? k % kTW : kTW; };
+  for (int y0 = rank * ROWS; y0 < (rank + 1) * ROWS; y0 += R) {
+    if constexpr (kInverse) {
+      // gather (conj of the Hermitian extension of A + i B, as the z pass)
+      for (int idx = tid; idx < 3 * R * NZH; idx += nt) {
+        const int pr = idx / (R * NZH), rem = idx % (R * NZH);
+        const int l = rem / NZH, k = rem % NZH;
+        const float2* src = cluster.map_shared_rank(cols, (unsigned)owner(k));
+        float2 A = src[((size_t)(2 * pr) * NY + y0 + l) * kSlabKW + local(k)];
+        float2 B = src[((size_t)(2 * pr + 1) * NY + y0 + l) * kSlabKW + local(k)];
+        const bool selfconj = (k == 0) || (2 * k == NZ);
+        if (selfconj) { A.y = 0.f; B.y = 0.f; }
+        float2* Z = zbuf + (size_t)(pr * R + l) * LD;
+        Z[k] = make_float2(A.x - B.y, -(A.y + B.x));
+        if (!selfconj) Z[NZ - k] = make_float2(A.x + B.y, A.y - B.x);
+      }
+      __syncthreads();
+      zline_fft<NZ>(zbuf, q, p, g.pz.tw);
+    }
+    // pointwise stage of the mode
+    for (int idx = tid; idx < R * NZ; idx += nt) {
+      const int l = idx / NZ, n = idx % NZ;
+      const size_t vx = ((size_t)x * NY + y0 + l) * NZ + n;
+      float e[6];
+      if constexpr (MODE == 3) {
+#pragma unroll
+        for (int pr = 0; pr < 3; ++pr) {
+          const float2 w = zbuf[(size_t)(pr * R + l) * LD + n];
+          const float r0 = w.x * inv_nv, r1 = -w.y * inv_nv;
+          const size_t o0 = (size_t)(2 * pr) * nv + vx, o1 = (size_t)(2 * pr + 1) * nv + vx;
+          rb[o0] = r0;
+          rb[o1] = r1;
+          gb[o0] = eb[o0] + r0;
+          gb[o1] = eb[o1] + r1;
+        }
+        continue;
+      } else {
+        if constexpr (MODE == 1) {
+#pragma unroll
+          for (int pr = 0; pr < 3; ++pr) {
+            const float2 w = zbuf[(size_t)(pr * R + l) * LD + n];
+            e[2 * pr] = eb[(size_t)(2 * pr) * nv + vx] + w.x * inv_nv;
+            e[2 * pr + 1] = eb[(size_t)(2 * pr + 1) * nv + vx] - w.y * inv_nv;
+          }
+        } else if constexpr (MODE == 2) {
+#pragma unroll
+          for (int c = 0; c < 6; ++c) e[c] = eb[(size_t)c * nv + vx];
+        } else {
+          if (eps0 != nullptr) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) e[c] = eps0[((size_t)b * 6 + c) * nv + vx];
+          } else {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) e[c] = (float)eps_bar[b * 6 + c];
+          }
+        }
+        if constexpr (MODE != 2) {
+#pragma unroll
+          for (int c = 0; c < 6; ++c) eb[(size_t)c * nv + vx] = e[c];
+        }
+        const float lmv = lam[vx], tmu = 2.f * muf[vx];
+        const float ltr = lmv * (e[0] + e[1] + e[2]);
+        float sg[6];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sg[c] = tmu * e[c] + ltr;
+#pragma unroll
+        for (int c = 3; c < 6; ++c) sg[c] = tmu * e[c];
+        // (the inverse transform's line is fully read above by this same thread before
+        // being overwritten: both index the line by (pr, l, n) of this idx)
+#pragma unroll
+        for (int pr = 0; pr < 3; ++pr)
+          zbuf[(size_t)(pr * R + l) * LD + n] =
+              make_float2(sg[2 * pr] - shift[2 * pr], sg[2 * pr + 1] - shift[2 * pr + 1]);
+      }
+    }
+    __syncthreads();
+    if constexpr (kForward) {
+      zline_fft<NZ>(zbuf, q, p, g.pz.tw);
+      // scatter the two half spectra of every line back to the owners' columns
+      for (int idx = tid; idx < 3 * R * NZH; idx += nt) {
+        const int pr = idx / (R * NZH), rem = idx % (R * NZH);
+        const int l = rem / NZH, k = rem % NZH;
+        const float2* Z = zbuf + (size_t)(pr * R + l) * LD;
+        const float2 zk = Z[k];
+        const float2 zm = Z[k == 0 ? 0 : NZ - k];
+        float2* dst = cluster.map_shared_rank(cols, (unsigned)owner(k));
+        dst[((size_t)(2 * pr) * NY + y0 + l) * kSlabKW + local(k)] =
+            make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        dst[((size_t)(2 * pr + 1) * NY + y0 + l) * kSlabKW + local(k)] =
+            make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+      }
+      __syncthreads();
+    }
+  }
+  cluster.sync();
+  if constexpr (!kForward) return;  // (after the barrier: no rank still reads this one's columns)
+
+  // ---- phase C: forward y DFT of the rank's columns, store
+  slab_ydft<NY>(cols, kw, false, g.py.tw);
+  for (int i = tid; i < 6 * NY * (kTW / 2); i += nt) {
+    const int c = i / (NY * (kTW / 2)), rem = i % (NY * (kTW / 2));
+    const int ky = rem / (kTW / 2), h = rem % (kTW / 2);
+    const float2* sv = cols + ((size_t)c * NY + ky) * kSlabKW + 2 * h;
+    *reinterpret_cast<float4*>(tb + (size_t)c * g.nm + ((size_t)(rank * NY + ky) * nx + x) * kTW + 2 * h) =
+        make_float4(sv[0].x, sv[0].y, sv[1].x, sv[1].y);
+  }
+  if (rank == CS - 1) {
+    for (int i = tid; i < 6 * NY; i += nt) {
+      const int c = i / NY, ky = i % NY;
+      tb[(size_t)c * g.nm + tail0 + ((size_t)(ky / kTW) * nx + x) * kTW + (ky % kTW)] =
+          cols[((size_t)c * NY + ky) * kSlabKW + kTW];
+    }
+  }
+}
+
 // ----------------------------------------------------------------------------- host side
 static bool pow2_supported(int n) {
   return n == 16 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128 || n == 256;
@@ -893,6 +1190,63 @@ bool tiled_supported(const GridDesc& g) {
 
 int x_tiles_tiled(const GridDesc& g) { return g.ny * ((g.nzh - 1) / kTW) + g.ny / kTW; }
 
+bool slab_supported(const GridDesc& g) {
+  const int n = g.nz;
+  return tiled_supported(g) && g.ny == n && n <= 128;
+}
+
+template <int N>
+static size_t slab_smem() { return slab_layout<N, N>().total; }
+
+template <int N, int MODE>
+static cudaError_t slab_launch_n(const GridDesc& g, int batch, const float* lambda, const float* mu,
+                                 float* eps, float2* tspec, const double* eps_bar, const float* eps0,
+                                 InstanceState* st, const Medium* med, const AndersonArgs<float>& aa,
+                                 cudaStream_t s) {
+  constexpr int CS = slab_ranks<N>();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CS, g.nx, batch);
+  cfg.blockDim = dim3(slab_threads<N>());
+  cfg.dynamicSmemBytes = slab_smem<N>();
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, slab_fast<N, N, MODE>, g, lambda, mu, eps, tspec, eps_bar, eps0, st,
+                            med, aa);
+}
+
+template <int N>
+static cudaError_t slab_launch_m(const GridDesc& g, int mode, int batch, const float* lambda,
+                                 const float* mu, float* eps, float2* tspec, const double* eps_bar,
+                                 const float* eps0, InstanceState* st, const Medium* med,
+                                 const AndersonArgs<float>& aa, cudaStream_t s) {
+  switch (mode) {
+    case 0: return slab_launch_n<N, 0>(g, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    case 1: return slab_launch_n<N, 1>(g, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    case 2: return slab_launch_n<N, 2>(g, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    default: return slab_launch_n<N, 3>(g, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+  }
+}
+
+cudaError_t launch_slab(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
+                        float* eps, float2* tspec, const double* eps_bar, const float* eps0,
+                        InstanceState* st, const Medium* med, const AndersonArgs<float>& aa,
+                        cudaStream_t s) {
+  switch (g.nz) {
+    case 16: return slab_launch_m<16>(g, mode, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    case 32: return slab_launch_m<32>(g, mode, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    case 48: return slab_launch_m<48>(g, mode, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    case 64: return slab_launch_m<64>(g, mode, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    case 96: return slab_launch_m<96>(g, mode, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+    default: return slab_launch_m<128>(g, mode, batch, lambda, mu, eps, tspec, eps_bar, eps0, st, med, aa, s);
+  }
+}
+
 size_t tile_index(const GridDesc& g, int x, int ky, int kz) {
   return tile_offset(g.nx, g.ny, (g.nzh - 1) / kTW, x, ky, kz);
 }
@@ -922,6 +1276,11 @@ static cudaError_t configure_n() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
   if constexpr (N <= 128) {
+    const int ss = (int)slab_smem<N>();
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(slab_fast<N, N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(slab_fast<N, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(slab_fast<N, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(slab_fast<N, N, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_tiled<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xtsmem<N>());
     if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_tiled<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xtsmem<N>());
   }
@@ -995,7 +1354,8 @@ static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, fl
   constexpr int YT = y_cols<N>();
   dim3 grid(g.nzh % YT == 1 ? g.nzh / YT + 1 : (g.nzh + YT - 1) / YT, g.nx, 6 * batch);
   if (tspec)
-    ypass_fast<N, true><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, tspec, st);
+    ypass_fast<N, true><<<dim3(grid.y, grid.x, grid.z), y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec,
+                                                                                tspec, st);
   else
     ypass_fast<N, false><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, spec, st);
 }

@@ -29,6 +29,15 @@ int x_tiles_tiled(const GridDesc& g);
 size_t tile_index(const GridDesc& g, int x, int ky, int kz);
 void launch_xpass_tiled(const GridDesc& g, int batch, float2* tspec, const Medium* med,
                         InstanceState* st, double* partials, cudaStream_t s);
+// The fused slab pass applies (tiled layout, ny == nz <= 128).
+bool slab_supported(const GridDesc& g);
+// Inverse y, z pass of `mode` (0 init, 1 plain update, 2 stress of eps, 3 Anderson residual
+// rings) and forward y (modes 0-2) of every x-plane, over the tiled layout in tspec; one
+// thread-block cluster per plane and instance. Isotropic law only.
+cudaError_t launch_slab(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
+                        float* eps, float2* tspec, const double* eps_bar, const float* eps0,
+                        InstanceState* st, const Medium* med, const AndersonArgs<float>& aa,
+                        cudaStream_t s);
 void launch_xpass(const GridDesc& g, int variant, int batch, float2* spec, const Medium* med,
                   InstanceState* st, double* partials, cudaStream_t s);
 

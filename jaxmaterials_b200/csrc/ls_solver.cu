@@ -206,6 +206,7 @@ int plan_grid(lsb_solver* s, const int voxels[3], const double extents[3]) {
   s->sh64 = plan_launch(g, sizeof(double2));
   s->fast32 = fast::supported(g);
   s->tiled = s->tiled_allowed && s->fast32 && fast::tiled_supported(g);
+  s->slab = s->slab_allowed && s->tiled && fast::slab_supported(g);
   if (s->tiled) s->sh32.x_blocks_per_instance = fast::x_tiles_tiled(g);
   else if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(g, s->xvariant) * g.ny;
   if (!shape_fits(s->sh32) || !shape_fits(s->sh64))
@@ -356,6 +357,27 @@ SolveParams make_params(const lsb_solver* s, double rtol, double atol, int maxit
   return sp;
 }
 
+// The fused slab pass runs this FP32 solve's y and z passes (isotropic law only).
+inline bool use_slab(const lsb_solver* s) { return s->slab && !s->g.cf32 && !s->g.dmg32; }
+
+template <typename T>
+void pass_slab(lsb_solver* s, int mode, int batch, const T* lam, const T* mu, T* eps,
+               const T* eps0, const AndersonArgs<T>& aa) {
+  if constexpr (sizeof(T) == 4) {
+    const cudaError_t e = fast::launch_slab(s->g, mode, batch, lam, mu, eps, s->d_tspec32, s->d_epsbar,
+                                            eps0, s->d_state, s->d_medium, aa, s->stream);
+    if (e != cudaSuccess && s->launch_error == cudaSuccess) s->launch_error = e;
+  }
+}
+
+// The first launch error recorded since the last call (cleared), or cudaGetLastError().
+inline cudaError_t take_launch_error(lsb_solver* s) {
+  const cudaError_t e = s->launch_error;
+  s->launch_error = cudaSuccess;
+  const cudaError_t last = cudaGetLastError();
+  return e != cudaSuccess ? e : last;
+}
+
 // Pass dispatch: FP32 fields use the compile-time-size passes when every extent is a
 // supported power of two, the generic passes otherwise.
 template <typename T>
@@ -498,6 +520,28 @@ void enqueue_iteration(lsb_solver* s, int batch, const T* lam, const T* mu, T* e
   mark("x pass");
   launch_finalize(sh, phase, batch, s->d_state, s->d_partials, s->d_history, s->history_len, sp, st);
   mark("finalize");
+  if (sizeof(T) == 4 && use_slab(s)) {
+    if (aa.depth > 0) {
+      const int gblk = gram_blocks(s);
+      pass_slab<T>(s, 3, batch, lam, mu, eps, nullptr, aa);
+      mark("slab residual rings");
+      launch_anderson_gram<T>(s->g.nv, gblk, s->depth, phase, batch, s->d_state, aa.r,
+                              s->d_aa_partials, st);
+      mark("anderson gram");
+      launch_anderson_solve(gblk, s->depth, phase, batch, s->d_state, s->d_aa_partials,
+                            s->d_aa_mat, s->d_aa_alpha, st);
+      mark("anderson solve");
+      launch_anderson_combine<T>(s->g.nv, s->depth, phase, batch, s->d_state, aa.g, s->d_aa_alpha,
+                                 eps, st, inject);
+      mark("anderson combine");
+      pass_slab<T>(s, 2, batch, lam, mu, eps, nullptr, aa);
+      mark("slab stress");
+    } else {
+      pass_slab<T>(s, 1, batch, lam, mu, eps, nullptr, aa);
+      mark("slab update");
+    }
+    return;
+  }
   pass_y<T>(s, true, batch, spec);
   mark("y pass inverse");
   if (aa.depth > 0) {
@@ -524,7 +568,9 @@ void enqueue_iteration(lsb_solver* s, int batch, const T* lam, const T* mu, T* e
 }
 
 // Kernels launched by one iteration.
-inline long long iteration_launches(bool mix) { return mix ? 9LL : 5LL; }
+inline long long iteration_launches(bool mix, bool slab) {
+  return slab ? (mix ? 7LL : 3LL) : (mix ? 9LL : 5LL);
+}
 
 // Runs the loop of precision T for every instance in its phase until none is left there.
 // init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
@@ -541,10 +587,16 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   cudaStream_t st = s->stream;
   const AndersonArgs<T> aa = anderson_args<T>(s, anderson && s->depth > 0);
   const bool mix = aa.depth > 0;
-  pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0, aa);
-  pass_y<T>(s, false, batch, spec);
-  s->launches += 2;
-  LSB_CUDA(cudaGetLastError());
+  const bool slab = sizeof(T) == 4 && use_slab(s);
+  if (slab) {
+    pass_slab<T>(s, init_mode, batch, lam, mu, eps, eps0, aa);
+    s->launches += 1;
+  } else {
+    pass_z<T>(s, init_mode, batch, lam, mu, eps, spec, eps0, aa);
+    pass_y<T>(s, false, batch, spec);
+    s->launches += 2;
+  }
+  LSB_CUDA(take_launch_error(s));
   auto iteration = [&]() {
     enqueue_iteration<T>(s, batch, lam, mu, eps, spec, aa, sp, sh, phase, inject, nullptr);
   };
@@ -562,8 +614,8 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
       }
     }
     launched += n;
-    s->launches += iteration_launches(mix) * n;
-    LSB_CUDA(cudaGetLastError());
+    s->launches += iteration_launches(mix, slab) * n;
+    LSB_CUDA(take_launch_error(s));
     LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch,
                              cudaMemcpyDeviceToHost, st));
     LSB_CUDA(cudaStreamSynchronize(st));
@@ -688,7 +740,7 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   launch_stress<float, float>(g, 0, batch, s->d_state, d_lambda, d_mu, d_eps, d_sigma,
                               s->d_mean_scratch, s->d_mean, st);
   s->launches += 2;
-  LSB_CUDA(cudaGetLastError());
+  LSB_CUDA(take_launch_error(s));
   if (mean_sigma)
     LSB_CUDA(cudaMemcpyAsync(mean_sigma, s->d_mean, sizeof(double) * 6 * batch, cudaMemcpyDeviceToHost, st));
   LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch, cudaMemcpyDeviceToHost, st));
@@ -737,7 +789,7 @@ int solve_f64(lsb_solver* s, int batch, const double* d_lambda, const double* d_
   launch_stress<double, double>(g, 1, batch, s->d_state, d_lambda, d_mu, d_eps, d_sigma,
                                 s->d_mean_scratch, s->d_mean, st);
   s->launches += 2;
-  LSB_CUDA(cudaGetLastError());
+  LSB_CUDA(take_launch_error(s));
   if (mean_sigma)
     LSB_CUDA(cudaMemcpyAsync(mean_sigma, s->d_mean, sizeof(double) * 6 * batch, cudaMemcpyDeviceToHost, st));
   LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch, cudaMemcpyDeviceToHost, st));
@@ -824,6 +876,13 @@ int lsb_tile_variant(lsb_solver* solver, int variant) {
   return solver->xvariant;
 }
 
+int lsb_set_slab(lsb_solver* solver, int on) {
+  if (!solver) return fail(-1, "null solver");
+  solver->slab_allowed = on != 0;
+  solver->slab = solver->slab_allowed && solver->tiled && fast::slab_supported(solver->g);
+  return solver->slab ? 1 : 0;
+}
+
 int lsb_set_tiled(lsb_solver* solver, int on) {
   if (!solver) return fail(-1, "null solver");
   lsb_solver* s = solver;
@@ -833,6 +892,7 @@ int lsb_set_tiled(lsb_solver* solver, int on) {
     LSB_CUDA(cudaMalloc(&s->d_tspec32, sizeof(float2) * (size_t)s->batch_cap * 6 * s->g.nm));
   }
   s->tiled = want;
+  s->slab = s->tiled && s->slab_allowed && fast::slab_supported(s->g);
   if (s->tiled) s->sh32.x_blocks_per_instance = fast::x_tiles_tiled(s->g);
   else if (s->fast32) s->sh32.x_blocks_per_instance = fast::x_tiles(s->g, s->xvariant) * s->g.ny;
   return s->tiled ? 1 : 0;
@@ -936,8 +996,12 @@ int lsb_profile_step(lsb_solver* s, int batch, const float* d_lambda, const floa
   launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   if (!s->xtuned) LSB_TRY(tune_xpass(s, batch));
   const AndersonArgs<float> aa = anderson_args<float>(s, s->depth > 0);
-  pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa);
-  pass_y<float>(s, false, batch, s->d_spec32);
+  if (use_slab(s)) {
+    pass_slab<float>(s, 0, batch, d_lambda, d_mu, d_eps, nullptr, aa);
+  } else {
+    pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa);
+    pass_y<float>(s, false, batch, s->d_spec32);
+  }
   // warm-up iterations: the Anderson rings fill up, so that the timed ones do full work
   for (int i = 0; i < s->depth + 2; ++i)
     enqueue_iteration<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, aa, sp, sh, 0, nullptr, nullptr);
@@ -959,7 +1023,7 @@ int lsb_profile_step(lsb_solver* s, int batch, const float* d_lambda, const floa
     }
   }
   for (auto& e : tm.ev) cudaEventDestroy(e);
-  LSB_CUDA(cudaGetLastError());
+  LSB_CUDA(take_launch_error(s));
   std::string joined;
   for (size_t k = 0; k < count; ++k) {
     ms_out[k] = (float)(acc[k] / reps);

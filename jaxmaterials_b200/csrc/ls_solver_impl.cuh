@@ -25,6 +25,11 @@ struct lsb_solver {
   // (d_tspec32); tiled_allowed = false keeps the strided x pass (no second spectrum buffer)
   bool tiled = false;
   bool tiled_allowed = true;
+  // the fused slab pass (inverse y + z + forward y per x-plane) replaces the y and z passes
+  // of FP32 solves over the tiled layout with the isotropic law
+  bool slab = false;
+  bool slab_allowed = true;
+  cudaError_t launch_error = cudaSuccess;  // first failed cluster launch since the last check
   int xvariant = 0;      // x-pass tile variant of the fast passes (chosen by timing)
   bool xtuned = false;   // xvariant has been chosen
   bool warm_history = false;  // d_eps0 enters the Anderson history instead of starting it

@@ -149,6 +149,11 @@ class Solver:
         results are bit-identical either way). Returns whether it is in use."""
         return bool(_lib.check(self._lib.lsb_set_tiled(self._h, 1 if on else 0), "lsb_set_tiled"))
 
+    def set_slab(self, on=True):
+        """Fused slab pass (inverse y + z + forward y per x-plane; the default where it
+        applies; results are bit-identical either way). Returns whether it is in use."""
+        return bool(_lib.check(self._lib.lsb_set_slab(self._h, 1 if on else 0), "lsb_set_slab"))
+
     def set_warm_history(self, on=True):
         """With on, a warm start (``epsilon0``) enters the Anderson history as the second
         iterate instead of starting the iteration (needs depth >= 1)."""

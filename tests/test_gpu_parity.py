@@ -502,6 +502,32 @@ def test_tiled_layout_matches_strided(ls, n, depth):
 
 
 @pytest.mark.parametrize("depth", [0, 3])
+@pytest.mark.parametrize("n", [(32, 16, 16), (64, 32, 32), (16, 48, 48), (64, 64, 64),
+                               (48, 96, 96), (128, 128, 128)])
+def test_slab_pass_matches_separate_passes(ls, n, depth):
+    """The fused slab pass (inverse y, z pass, forward y of every x-plane in one cluster
+    kernel) gives the fields of the separate y and z passes bit for bit (same arithmetic,
+    same order), including the initial stress and the converged iteration counts."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import Solver
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    eb = np.tile(EPS_BAR, (2, 1))
+    out = []
+    for slab in (True, False):
+        s = Solver(g, batch=2, depth=depth)
+        assert s.set_slab(slab) == slab
+        r = s.solve(lm, mu, eb, rtol=1e-6, atol=1e-20, maxiter=400)
+        out.append((r.epsilon.clone(), r.sigma.clone(), r.iters.copy(), r.mean_sigma.copy()))
+        s.close()
+    assert (out[0][2] == out[1][2]).all()
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    assert (out[0][3] == out[1][3]).all()
+
+
+@pytest.mark.parametrize("depth", [0, 3])
 def test_graph_replay_bit_identical(ls, depth):
     """Iterations replayed from a CUDA graph and launched kernel by kernel give the same
     bits (same kernels, same order)."""
