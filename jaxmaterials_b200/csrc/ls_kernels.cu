@@ -518,50 +518,58 @@ __global__ void finalize_kernel(int nblk, int phase, InstanceState* __restrict__
   s.iter += 1;
 }
 
+// Ring access of VW consecutive elements: float4 for VW = 4 (FP32 rings whose slot length
+// 6 nv is a multiple of 4, so that every slot starts 16-byte aligned), scalars otherwise.
+// Wide loads keep four times the bytes in flight per load, which the streaming kernels
+// below need at their register-limited occupancy.
+template <typename T, int VW>
+struct RingVec { using type = T; };
+template <>
+struct RingVec<float, 4> { using type = float4; };
+template <typename T>
+__device__ __forceinline__ T lane_of(const T& v, int) { return v; }
+__device__ __forceinline__ float lane_of(const float4& v, int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
 // Gram-row partials of the newest residual r_j (slot j of the ring) for every instance in
-// `phase`: partials[b][blk][q] = sum over block blk's voxels of sum_c w_c r_j r_q, with
-// Voigt weights w = (1,1,1,2,2,2), in FP64 (lippmann_schwinger.py:217-231). A streaming
-// kernel of its own: every ring value of a voxel is requested before the first product,
-// so each thread keeps 6 M1 loads in flight (M1 = depth + 1 slots, a template constant).
-template <typename T, int M1>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) anderson_gram_kernel(long long nv, int phase,
-                                                               const InstanceState* __restrict__ st,
-                                                               const T* __restrict__ r,
-                                                               double* __restrict__ partials) {
+// `phase`: partials[b][blk][q] = sum over block blk's ring elements (component c, voxel) of
+// w_c r_j r_q, with Voigt weights w = (1,1,1,2,2,2), in FP64 (lippmann_schwinger.py:217-231).
+// A streaming kernel of its own, walking the 6 nv elements of a slot as the combine does, VW
+// elements per load, every slot of an element requested before the first product (M1 =
+// depth + 1 slots, a template constant).
+template <typename T, int M1, int VW>
+__global__ void __launch_bounds__(256) anderson_gram_kernel(long long nv, int phase,
+                                                            const InstanceState* __restrict__ st,
+                                                            const T* __restrict__ r,
+                                                            double* __restrict__ partials) {
+  using V = typename RingVec<T, VW>::type;
   __shared__ double red[kMaxDepth + 1][32];
   const int b = blockIdx.y;
   const InstanceState& s = st[b];
   if (s.done || s.phase != phase) return;
   int slot, filled;
   anderson_slots<T>(s, M1 - 1, slot, filled);
-  const size_t ring = (size_t)6 * nv;
-  const T* rb = r + (size_t)b * M1 * ring;
+  const long long n6 = 6 * nv, nvec = n6 / VW;
+  const T* rb = r + (size_t)b * M1 * n6;
   double dots[M1];
 #pragma unroll
   for (int q = 0; q < M1; ++q) dots[q] = 0.0;
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv;
-       v += (long long)gridDim.x * blockDim.x) {
-    T rq[M1][6];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvec;
+       i += (long long)gridDim.x * blockDim.x) {
+    V rq[M1];
 #pragma unroll
     for (int q = 0; q < M1; ++q)
+      if (q < filled) rq[q] = reinterpret_cast<const V*>(rb + (size_t)q * n6)[i];
+    V x = rq[0];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) rq[q][c] = q < filled ? rb[q * ring + (size_t)c * nv + v] : (T)0;
-    double rn[6];
+    for (int q = 1; q < M1; ++q) x = q == slot ? rq[q] : x;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      T x = rq[0][c];
+    for (int k = 0; k < VW; ++k) {
+      const double wx = (i * VW + k < 3 * nv ? 1.0 : 2.0) * (double)lane_of(x, k);
 #pragma unroll
-      for (int q = 1; q < M1; ++q) x = q == slot ? rq[q][c] : x;
-      rn[c] = (c < 3 ? 1.0 : 2.0) * (double)x;
-    }
-#pragma unroll
-    for (int q = 0; q < M1; ++q) {
-      if (q < filled) {
-        double d = 0.0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) d += rn[c] * (double)rq[q][c];
-        dots[q] += d;
-      }
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) dots[q] += wx * (double)lane_of(rq[q], k);
     }
   }
   double pad[kMaxDepth + 1];
@@ -574,14 +582,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) anderson_gram_ker
 }
 
 // Anderson combine for every instance in `phase`: eps = sum_s alpha_s g_s over the filled
-// slots (lippmann_schwinger.py:228-231), accumulated in the field precision in slot order.
-template <typename T, int M1>
+// slots (lippmann_schwinger.py:228-231), accumulated in the field precision in slot order,
+// VW elements per load.
+template <typename T, int M1, int VW>
 __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int phase,
                                                                const InstanceState* __restrict__ st,
                                                                const T* __restrict__ g,
                                                                const double* __restrict__ alpha,
                                                                const T* __restrict__ inject,
                                                                T* __restrict__ eps) {
+  using V = typename RingVec<T, VW>::type;
   const int b = blockIdx.y;
   const InstanceState& s = st[b];
   if (s.done || s.phase != phase) return;
@@ -593,6 +603,7 @@ __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int
 #pragma unroll
   for (int q = 0; q < M1; ++q) a[q] = q < filled ? (T)al[q] : (T)0;
   T* eb = eps + (size_t)b * n6;
+  const long long nvec = n6 / VW;
   if (inject && s.iter == 1 && s.aa_base == 0) {
     // first update with a warm start in the history: the next iterate is the given field,
     // whose residual then enters the ring beside the cold start's
@@ -602,16 +613,30 @@ __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int
       eb[i] = ib[i];
     return;
   }
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n6;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvec;
        i += (long long)gridDim.x * blockDim.x) {
-    T gv[M1];
-#pragma unroll
-    for (int q = 0; q < M1; ++q) gv[q] = q < filled ? gb[q * n6 + i] : (T)0;
-    T e = 0;
+    V gv[M1];
 #pragma unroll
     for (int q = 0; q < M1; ++q)
-      if (q < filled) e += a[q] * gv[q];
-    eb[i] = e;
+      if (q < filled) gv[q] = reinterpret_cast<const V*>(gb + (size_t)q * n6)[i];
+    if constexpr (VW == 4 && sizeof(T) == 4) {
+      float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) {
+          e.x += a[q] * gv[q].x;
+          e.y += a[q] * gv[q].y;
+          e.z += a[q] * gv[q].z;
+          e.w += a[q] * gv[q].w;
+        }
+      reinterpret_cast<float4*>(eb)[i] = e;
+    } else {
+      T e = 0;
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) e += a[q] * gv[q];
+      eb[i] = e;
+    }
   }
 }
 
@@ -965,9 +990,18 @@ template <typename T>
 void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batch,
                           const InstanceState* st, const T* r, double* partials, cudaStream_t stream) {
   const dim3 grid(nblk, batch);
+  const bool vec = sizeof(T) == 4 && (6 * nv) % 4 == 0;
   switch (depth + 1) {
-#define LSB_GRAM(M) \
-    case M: anderson_gram_kernel<T, M><<<grid, 256, 0, stream>>>(nv, phase, st, r, partials); break;
+#define LSB_GRAM(M)                                                                              \
+    case M:                                                                                      \
+      if constexpr (sizeof(T) == 4) {                                                            \
+        if (vec) {                                                                               \
+          anderson_gram_kernel<T, M, 4><<<grid, 256, 0, stream>>>(nv, phase, st, r, partials); \
+          break;                                                                                 \
+        }                                                                                        \
+      }                                                                                          \
+      anderson_gram_kernel<T, M, 1><<<grid, 256, 0, stream>>>(nv, phase, st, r, partials);     \
+      break;
     LSB_GRAM(2) LSB_GRAM(3) LSB_GRAM(4) LSB_GRAM(5) LSB_GRAM(6) LSB_GRAM(7) LSB_GRAM(8) LSB_GRAM(9)
 #undef LSB_GRAM
     default: break;
@@ -980,9 +1014,18 @@ void launch_anderson_combine(long long nv, int depth, int phase, int batch, cons
                              const T* inject) {
   const long long n6 = 6 * nv;
   const dim3 grid((unsigned)std::min<long long>(2048, (n6 + 255) / 256), batch);
+  const bool vec = sizeof(T) == 4 && n6 % 4 == 0;
   switch (depth + 1) {
-#define LSB_COMB(M) \
-    case M: anderson_combine_kernel<T, M><<<grid, 256, 0, stream>>>(n6, phase, st, g, alpha, inject, eps); break;
+#define LSB_COMB(M)                                                                                        \
+    case M:                                                                                                \
+      if constexpr (sizeof(T) == 4) {                                                                      \
+        if (vec) {                                                                                         \
+          anderson_combine_kernel<T, M, 4><<<grid, 256, 0, stream>>>(n6, phase, st, g, alpha, inject, eps); \
+          break;                                                                                           \
+        }                                                                                                  \
+      }                                                                                                    \
+      anderson_combine_kernel<T, M, 1><<<grid, 256, 0, stream>>>(n6, phase, st, g, alpha, inject, eps);     \
+      break;
     LSB_COMB(2) LSB_COMB(3) LSB_COMB(4) LSB_COMB(5) LSB_COMB(6) LSB_COMB(7) LSB_COMB(8) LSB_COMB(9)
 #undef LSB_COMB
     default: break;

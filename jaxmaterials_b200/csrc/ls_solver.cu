@@ -498,11 +498,11 @@ struct StepTimer {
   }
 };
 
-// Blocks per instance of the Anderson Gram-row kernel (its partials fit the z-block-sized
-// buffer).
+// Blocks per instance of the Anderson Gram-row kernel (as many as the combine kernel, and
+// its partials fit the z-block-sized buffer).
 int gram_blocks(const lsb_solver* s) {
   return (int)std::max<long long>(
-      1, std::min<long long>({(long long)s->aa_zblocks, 592LL, (s->g.nv + 255) / 256}));
+      1, std::min<long long>({(long long)s->aa_zblocks, 2048LL, (6 * s->g.nv + 255) / 256}));
 }
 
 // One iteration of precision T: x pass, criterion and stop decision, inverse y pass, then

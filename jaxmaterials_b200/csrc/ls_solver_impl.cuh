@@ -28,7 +28,7 @@ struct lsb_solver {
   // the fused slab pass (inverse y + z + forward y per x-plane) replaces the y and z passes
   // of FP32 solves over the tiled layout with the isotropic law
   bool slab = false;
-  bool slab_allowed = true;
+  bool slab_allowed = false;  // measured slower than the separate passes (opt-in)
   cudaError_t launch_error = cudaSuccess;  // first failed cluster launch since the last check
   int xvariant = 0;      // x-pass tile variant of the fast passes (chosen by timing)
   bool xtuned = false;   // xvariant has been chosen

@@ -150,8 +150,9 @@ class Solver:
         return bool(_lib.check(self._lib.lsb_set_tiled(self._h, 1 if on else 0), "lsb_set_tiled"))
 
     def set_slab(self, on=True):
-        """Fused slab pass (inverse y + z + forward y per x-plane; the default where it
-        applies; results are bit-identical either way). Returns whether it is in use."""
+        """Fused slab pass (inverse y + z + forward y per x-plane; opt-in, measured slower
+        than the separate passes at 128^3; results are bit-identical either way). Returns
+        whether it is in use."""
         return bool(_lib.check(self._lib.lsb_set_slab(self._h, 1 if on else 0), "lsb_set_slab"))
 
     def set_warm_history(self, on=True):
