@@ -534,7 +534,8 @@ __device__ __forceinline__ float lane_of(const float4& v, int k) {
 
 // Gram-row partials of the newest residual r_j (slot j of the ring) for every instance in
 // `phase`: partials[b][blk][q] = sum over block blk's ring elements (component c, voxel) of
-// w_c r_j r_q, with Voigt weights w = (1,1,1,2,2,2), in FP64 (lippmann_schwinger.py:217-231).
+// w_c r_j r_q, with Voigt weights w = (1,1,1,2,2,2), accumulated in FP64 (FP32 rings: four
+// neighbouring products summed in FP32 first) (lippmann_schwinger.py:217-231).
 // A streaming kernel of its own, walking the 6 nv elements of a slot as the combine does, VW
 // elements per load, every slot of an element requested before the first product (M1 =
 // depth + 1 slots, a template constant).
@@ -564,12 +565,24 @@ __global__ void __launch_bounds__(256) anderson_gram_kernel(long long nv, int ph
     V x = rq[0];
 #pragma unroll
     for (int q = 1; q < M1; ++q) x = q == slot ? rq[q] : x;
-#pragma unroll
-    for (int k = 0; k < VW; ++k) {
-      const double wx = (i * VW + k < 3 * nv ? 1.0 : 2.0) * (double)lane_of(x, k);
+    if constexpr (VW == 4 && sizeof(T) == 4) {
+      // the group's four weighted products summed in FP32, the sum added in FP64 (the
+      // kernel is bound by its FP64 issue rate otherwise)
+      const long long e0 = i * 4;
+      const float4 wx = make_float4((e0 < 3 * nv ? 1.f : 2.f) * x.x, (e0 + 1 < 3 * nv ? 1.f : 2.f) * x.y,
+                                    (e0 + 2 < 3 * nv ? 1.f : 2.f) * x.z, (e0 + 3 < 3 * nv ? 1.f : 2.f) * x.w);
 #pragma unroll
       for (int q = 0; q < M1; ++q)
-        if (q < filled) dots[q] += wx * (double)lane_of(rq[q], k);
+        if (q < filled)
+          dots[q] += (double)(wx.x * rq[q].x + wx.y * rq[q].y + wx.z * rq[q].z + wx.w * rq[q].w);
+    } else {
+#pragma unroll
+      for (int k = 0; k < VW; ++k) {
+        const double wx = (i * VW + k < 3 * nv ? 1.0 : 2.0) * (double)lane_of(x, k);
+#pragma unroll
+        for (int q = 0; q < M1; ++q)
+          if (q < filled) dots[q] += wx * (double)lane_of(rq[q], k);
+      }
     }
   }
   double pad[kMaxDepth + 1];
