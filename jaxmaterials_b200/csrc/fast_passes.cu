@@ -605,13 +605,19 @@ __host__ __device__ constexpr int z_ld() {
 struct ZLayout {  // byte offsets inside the z pass's dynamic shared memory
   size_t zbuf, rst, est, lst, total;
 };
-template <int NZ>
+// MODE < 0: the mode is a run-time argument (every staging region); otherwise only the
+// regions that mode stages (spectrum rows for 1 and 3, strain rows for 1-3, lambda and mu
+// rows for 0-2), so that the other modes keep more blocks resident.
+template <int NZ, int MODE = -1>
 __host__ __device__ constexpr ZLayout z_layout() {
   constexpr int L = z_lines<NZ>(), NZH = NZ / 2 + 1;
+  constexpr bool r = MODE < 0 || MODE == 1 || MODE == 3;
+  constexpr bool e = MODE != 0;
+  constexpr bool l = MODE != 3;
   constexpr size_t zb = (size_t)3 * L * z_ld<NZ>() * 8;
-  constexpr size_t rs = (size_t)6 * L * NZH * 8;
-  constexpr size_t es = (size_t)6 * L * NZ * 4;
-  constexpr size_t ls = (size_t)2 * L * NZ * 4;
+  constexpr size_t rs = r ? (size_t)6 * L * NZH * 8 : 0;
+  constexpr size_t es = e ? (size_t)6 * L * NZ * 4 : 0;
+  constexpr size_t ls = l ? (size_t)2 * L * NZ * 4 : 0;
   return ZLayout{0, zb, zb + rs, zb + rs + es, zb + rs + es + ls};
 }
 
@@ -656,14 +662,16 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
 // staging buffers are filled by ordinary loads.
 // LAW: 0 isotropic (lambda, mu staged), 1 damage extension, 2 anisotropic stiffness (21
 // entries read per voxel from global memory; lambda and mu not staged).
-template <int NZ, int LAW>
+// MODE >= 0 fixes the mode at compile time (mode_arg is then ignored).
+template <int NZ, int LAW, int MODE>
 __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fast(
-    GridDesc g, int mode, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
+    GridDesc g, int mode_arg, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
     const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med,
     AndersonArgs<float> aa) {
   constexpr int P = Split<NZ>::P, L = z_lines<NZ>(), LD = z_ld<NZ>(), NZH = NZ / 2 + 1;
-  constexpr ZLayout LY = z_layout<NZ>();
+  constexpr ZLayout LY = z_layout<NZ, MODE>();
+  const int mode = MODE >= 0 ? MODE : mode_arg;
   extern __shared__ __align__(128) unsigned char zfraw[];
   float2* zbuf = reinterpret_cast<float2*>(zfraw + LY.zbuf);  // 3L lines of LD values
   float2* rst = reinterpret_cast<float2*>(zfraw + LY.rst);    // [6][L][NZH] spectrum rows
@@ -1254,8 +1262,8 @@ size_t tile_index(const GridDesc& g, int x, int ky, int kz) {
 template <int N>
 static size_t xtsmem() { return (size_t)6 * x_region<N, kTW, XTSplit<N>>() * sizeof(float2); }
 
-template <int N>
-static size_t zsmem() { return z_layout<N>().total; }
+template <int N, int MODE = -1>
+static size_t zsmem() { return z_layout<N, MODE>().total; }
 template <int N>
 static int z_blocks_for(const GridDesc& g) {
   return (int)(((long long)g.nx * g.ny + z_lines<N>() - 1) / z_lines<N>());
@@ -1268,9 +1276,12 @@ static size_t xsmem() {
 template <int N>
 static cudaError_t configure_n() {
   const int zs = (int)zsmem<N>();
-  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+  cudaError_t e = cudaFuncSetAttribute(zpass_fast<N, 1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 2, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, 0>());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, 1>());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, 2>());
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(zpass_fast<N, 0, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, 3>());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 1>());
   if (e == cudaSuccess) e = cudaFuncSetAttribute(xpass_fast<N, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<N, 0>());
@@ -1307,15 +1318,34 @@ static void zlaunch(const GridDesc& g, int mode, int batch, const float* lambda,
   dim3 grid((unsigned)z_blocks_for<N>(g), batch);
   // every chunk offset is a multiple of 16 bytes when the base pointers are
   const int bulk = aligned16(lambda) && aligned16(mu) && aligned16(eps) && aligned16(spec) ? 1 : 0;
-  if (g.cf32)
-    zpass_fast<N, 2><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
-                                                             eps_bar, eps0, st, med, aa);
-  else if (g.dmg32)
-    zpass_fast<N, 1><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
-                                                             eps_bar, eps0, st, med, aa);
-  else
-    zpass_fast<N, 0><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
-                                                             eps_bar, eps0, st, med, aa);
+  if (g.cf32) {
+    zpass_fast<N, 2, -1><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                 eps_bar, eps0, st, med, aa);
+    return;
+  }
+  if (g.dmg32) {
+    zpass_fast<N, 1, -1><<<grid, z_threads<N>(), zsmem<N>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                 eps_bar, eps0, st, med, aa);
+    return;
+  }
+  switch (mode) {
+    case 0:
+      zpass_fast<N, 0, 0><<<grid, z_threads<N>(), zsmem<N, 0>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                     eps_bar, eps0, st, med, aa);
+      break;
+    case 1:
+      zpass_fast<N, 0, 1><<<grid, z_threads<N>(), zsmem<N, 1>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                     eps_bar, eps0, st, med, aa);
+      break;
+    case 2:
+      zpass_fast<N, 0, 2><<<grid, z_threads<N>(), zsmem<N, 2>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                     eps_bar, eps0, st, med, aa);
+      break;
+    default:
+      zpass_fast<N, 0, 3><<<grid, z_threads<N>(), zsmem<N, 3>(), s>>>(g, mode, bulk, lambda, mu, eps, spec,
+                                                                     eps_bar, eps0, st, med, aa);
+      break;
+  }
 }
 
 void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, const float* mu,
