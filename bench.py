@@ -421,6 +421,7 @@ def step_roofline(solver, lm_d, mu_d, g, batch, depth, workload):
     step_bytes = sum(k["algorithmic_bytes"] for k in kernels)
     survey_b = 152.0 if depth == 0 else 200.0 + 72.0 * depth
     return {
+        "pass_config": solver.pass_config(),
         "bound": "hbm",
         "kernel": top["kernel"],
         "achieved": top["GBs"],

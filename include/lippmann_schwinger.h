@@ -126,6 +126,16 @@ int lsb_set_tiled(lsb_solver *solver, int on);
  * after the call, 0 if not. */
 int lsb_set_slab(lsb_solver *solver, int on);
 
+/* No reference counterpart. FP32 pass configuration of the solver: out (host int[4]) =
+ * tiled layout in use, x-pass tile variant of the strided layout, slab pass in use, and
+ * whether the configuration is settled (by the autotuner on the first FP32 solve or
+ * profile, or by the caller through lsb_tile_variant / lsb_set_tiled / lsb_set_slab).
+ * The autotuner times every candidate configuration on the solve's own iteration and
+ * keeps the fastest; its choices are cached per (device, grid, batch, Anderson depth,
+ * law) in the file named by the environment variable LSB_TUNE_CACHE (default
+ * $HOME/.cache/jaxmaterials_b200/tune.tsv; empty or "0": no file). */
+int lsb_pass_config(lsb_solver *solver, int *out);
+
 /* No reference counterpart. on != 0 (default): each phase of a solve captures one
  * iteration's launches into a CUDA graph on a stream of the solver's own (ordered after
  * the work already on the solver's stream, and that stream waits for it) and replays it;

@@ -43,6 +43,7 @@ SIGNATURES = {
     "lsb_tile_variant": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_set_tiled": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_set_slab": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "lsb_pass_config": (ctypes.c_int, [c_void_p, c_int_p]),
     "lsb_set_reference_e0": (ctypes.c_int, [c_void_p, ctypes.c_int, c_double_p]),
     "lsb_c_eff_batch": (ctypes.c_int, [ctypes.c_int, c_int_p, c_double_p,
                                        ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),

@@ -8,12 +8,18 @@
 //   MIXED  FP32 until the criterion stalls near the tolerance, then the stalled
 //          instances continue from their iterate with FP64 fields and FFTs (default);
 //   FP64   FP64 fields and FFTs from the start.
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -627,45 +633,162 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   }
 }
 
-// Chooses the faster x-pass tile variant of the fast FP32 passes by timing both (three
-// launches each after one warm-up, CUDA events on the solver's stream) on this solver's
-// buffers; the passes only write the spectrum, the partials and the zero mode, all of
-// which the solve recomputes before use. Runs once per solver.
-int tune_xpass(lsb_solver* s, int batch) {
-  if (!use_fast32(s)) return 0;  // the generic passes have no tile variants
-  s->xtuned = true;
-  if (s->tiled) return 0;        // one form of the x pass over the tiled layout
-  if (fast::x_tiles(s->g, 0) == fast::x_tiles(s->g, 1)) return 0;
+// ---- autotuner of the FP32 pass configuration
+//
+// Candidates for a grid of the compile-time-size passes: the tiled spectrum layout
+// between the y and x passes (when the solver holds its buffer), the fused slab pass
+// over it (ny == nz, isotropic law), and the strided x pass with either tile variant.
+// Each runs the solve's own iteration (Anderson when depth > 0) on this solver's buffers
+// from a fresh state: the initial pass, depth + 2 untimed iterations that fill the
+// Anderson rings, then kTuneReps timed iterations (CUDA events on the solver's stream,
+// tolerances 0 so that every pass does its full work). The fastest is kept; the choice is
+// remembered per (device, grid, batch, depth, law) for the process and in a cache file
+// (LSB_TUNE_CACHE, else $HOME/.cache/jaxmaterials_b200/tune.tsv; an empty value or "0"
+// disables the file), so that later processes skip the timing.
+struct TuneChoice {
+  int tiled, xvariant, slab;
+};
+constexpr int kTuneReps = 3;
+
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice>* g_tune = nullptr;
+
+std::string tune_path() {
+  const char* env = std::getenv("LSB_TUNE_CACHE");
+  if (env) return (env[0] == '\0' || std::string(env) == "0") ? std::string() : std::string(env);
+  const char* home = std::getenv("HOME");
+  if (!home || !home[0]) return std::string();
+  return std::string(home) + "/.cache/jaxmaterials_b200/tune.tsv";
+}
+
+void tune_load_locked() {
+  if (g_tune) return;
+  g_tune = new std::map<std::string, TuneChoice>();
+  const std::string path = tune_path();
+  if (path.empty()) return;
+  std::ifstream in(path);
+  std::string line;
+  while (std::getline(in, line)) {
+    std::istringstream ls(line);
+    std::string key;
+    TuneChoice c{};
+    if (std::getline(ls, key, '\t') && (ls >> c.tiled >> c.xvariant >> c.slab)) (*g_tune)[key] = c;
+  }
+}
+
+void tune_store_locked(const std::string& key, const TuneChoice& c, float ms) {
+  (*g_tune)[key] = c;
+  const std::string path = tune_path();
+  if (path.empty()) return;
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {
+    // create the directory chain (ignore failures: the choice then stays in memory only)
+    std::string dir = path.substr(0, slash);
+    for (size_t k = 1; k <= dir.size(); ++k)
+      if (k == dir.size() || dir[k] == '/') mkdir(dir.substr(0, k).c_str(), 0755);
+  }
+  std::ofstream out(path, std::ios::app);
+  if (out) out << key << '\t' << c.tiled << '\t' << c.xvariant << '\t' << c.slab << '\t' << ms << '\n';
+}
+
+std::string tune_key(const lsb_solver* s, int batch) {
+  cudaDeviceProp prop;
+  std::string dev = "device";
+  if (cudaGetDeviceProperties(&prop, s->device) == cudaSuccess)
+    dev = std::string(prop.name) + "/" + std::to_string(prop.multiProcessorCount);
+  const char* law = s->g.cf32 ? "aniso" : (s->g.dmg32 ? "damage" : "iso");
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|b%d|m%d|%s", dev.c_str(), s->g.nx, s->g.ny, s->g.nz,
+                batch, s->depth, law);
+  return buf;
+}
+
+void apply_choice(lsb_solver* s, const TuneChoice& c) {
+  s->tiled = c.tiled && s->d_tspec32 != nullptr && fast::tiled_supported(s->g);
+  s->slab = c.slab && s->tiled && fast::slab_supported(s->g);
+  s->xvariant = c.xvariant;
+  if (s->tiled) s->sh32.x_blocks_per_instance = fast::x_tiles_tiled(s->g);
+  else s->sh32.x_blocks_per_instance = fast::x_tiles(s->g, s->xvariant) * s->g.ny;
+}
+
+// Times kTuneReps iterations of the current configuration (see above); ms per iteration.
+int time_config(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu, float* d_eps,
+                int nstruct, float* ms_out) {
   cudaStream_t st = s->stream;
+  SolveParams sp = make_params(s, 0.0, 0.0, 0x3fffffff, LSB_RULE_CUDA);
+  sp.precision = kPrecFP32;
+  sp.stall_window = 0;
+  LaunchShape sh = s->sh32;
+  launch_reset_state(batch, 0, s->d_state, st);
+  launch_medium<float>(s->g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
+  const AndersonArgs<float> aa = anderson_args<float>(s, s->depth > 0);
+  if (use_slab(s)) {
+    pass_slab<float>(s, 0, batch, d_lambda, d_mu, d_eps, nullptr, aa);
+  } else {
+    pass_z<float>(s, 0, batch, d_lambda, d_mu, d_eps, s->d_spec32, nullptr, aa);
+    pass_y<float>(s, false, batch, s->d_spec32);
+  }
+  for (int i = 0; i < s->depth + 2; ++i)
+    enqueue_iteration<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, aa, sp, sh, 0, nullptr, nullptr);
   cudaEvent_t ev[2];
   LSB_CUDA(cudaEventCreate(&ev[0]));
   LSB_CUDA(cudaEventCreate(&ev[1]));
-  float best = 0.f;
-  int bestv = 0;
-  for (int v = 0; v < 2; ++v) {
-    fast::launch_xpass(s->g, v, batch, s->d_spec32, s->d_medium, s->d_state, s->d_partials, st);
-    cudaEventRecord(ev[0], st);
-    for (int r = 0; r < 3; ++r)
-      fast::launch_xpass(s->g, v, batch, s->d_spec32, s->d_medium, s->d_state, s->d_partials, st);
-    cudaEventRecord(ev[1], st);
-    cudaError_t e = cudaEventSynchronize(ev[1]);
-    float ms = 0.f;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
-    if (e != cudaSuccess) {
-      cudaEventDestroy(ev[0]);
-      cudaEventDestroy(ev[1]);
-      return fail(-2, "x-pass tuning: %s", cudaGetErrorString(e));
-    }
-    if (v == 0 || ms < best) {
-      best = ms;
-      bestv = v;
-    }
-  }
+  cudaEventRecord(ev[0], st);
+  for (int i = 0; i < kTuneReps; ++i)
+    enqueue_iteration<float>(s, batch, d_lambda, d_mu, d_eps, s->d_spec32, aa, sp, sh, 0, nullptr, nullptr);
+  cudaEventRecord(ev[1], st);
+  cudaError_t e = cudaEventSynchronize(ev[1]);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
-  s->launches += 8;
-  s->xvariant = bestv;
-  s->sh32.x_blocks_per_instance = fast::x_tiles(s->g, bestv) * s->g.ny;
+  if (e == cudaSuccess) e = take_launch_error(s);
+  if (e != cudaSuccess) return fail(-2, "pass tuning: %s", cudaGetErrorString(e));
+  s->launches += (long long)(s->depth + 2 + kTuneReps) * iteration_launches(s->depth > 0, use_slab(s)) + 4;
+  *ms_out = ms / kTuneReps;
+  return 0;
+}
+
+// Chooses the pass configuration of the fast FP32 passes (see above). Runs once per solver
+// unless the caller fixed the configuration (lsb_tile_variant, lsb_set_tiled, lsb_set_slab);
+// leaves the per-instance state to be reset by the solve.
+int tune_passes(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu, float* d_eps,
+                int nstruct) {
+  if (!use_fast32(s)) return 0;  // the generic passes have one configuration
+  s->xtuned = true;
+  const std::string key = tune_key(s, batch);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_load_locked();
+    auto f = g_tune->find(key);
+    if (f != g_tune->end()) {
+      apply_choice(s, f->second);
+      return 0;
+    }
+  }
+  std::vector<TuneChoice> cand;
+  if (s->d_tspec32 && fast::tiled_supported(s->g)) {
+    cand.push_back({1, 0, 0});
+    if (fast::slab_supported(s->g) && !s->g.cf32 && !s->g.dmg32) cand.push_back({1, 0, 1});
+  }
+  cand.push_back({0, 0, 0});
+  if (fast::x_tiles(s->g, 0) != fast::x_tiles(s->g, 1)) cand.push_back({0, 1, 0});
+  TuneChoice best = cand[0];
+  float best_ms = 0.f;
+  if (cand.size() > 1) {
+    for (size_t k = 0; k < cand.size(); ++k) {
+      apply_choice(s, cand[k]);
+      float ms = 0.f;
+      LSB_TRY(time_config(s, batch, d_lambda, d_mu, d_eps, nstruct, &ms));
+      if (k == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = cand[k];
+      }
+    }
+  }
+  apply_choice(s, best);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  tune_store_locked(key, best, best_ms);
   return 0;
 }
 
@@ -698,12 +821,12 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
   if (s->precision != kPrecFP32) LSB_TRY(ensure_fp64(s, nstruct));
 
   LSB_CUDA(cudaMemcpyAsync(s->d_epsbar, eps_bar, sizeof(double) * 6 * batch, cudaMemcpyHostToDevice, st));
+  if (!s->xtuned && !fp64_start) LSB_TRY(tune_passes(s, batch, d_lambda, d_mu, d_eps, nstruct));
   if (s->d_history)
     LSB_CUDA(cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, st));
   launch_reset_state(batch, fp64_start ? 1 : 0, s->d_state, st, s->use_e0ref ? s->d_e0ref : nullptr);
   launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
   s->launches += 3;
-  if (!s->xtuned && !fp64_start) LSB_TRY(tune_xpass(s, batch));
   bool any64 = fp64_start;
   if (!fp64_start) {
     // a warm start either starts the iteration or (warm_history) enters the Anderson
@@ -876,8 +999,18 @@ int lsb_tile_variant(lsb_solver* solver, int variant) {
   return solver->xvariant;
 }
 
+int lsb_pass_config(lsb_solver* solver, int* out) {
+  if (!solver || !out) return fail(-1, "null argument");
+  out[0] = solver->tiled ? 1 : 0;
+  out[1] = solver->xvariant;
+  out[2] = solver->slab ? 1 : 0;
+  out[3] = solver->xtuned ? 1 : 0;
+  return 0;
+}
+
 int lsb_set_slab(lsb_solver* solver, int on) {
   if (!solver) return fail(-1, "null solver");
+  solver->xtuned = true;  // the caller's choice: no autotuning
   solver->slab_allowed = on != 0;
   solver->slab = solver->slab_allowed && solver->tiled && fast::slab_supported(solver->g);
   return solver->slab ? 1 : 0;
@@ -886,6 +1019,7 @@ int lsb_set_slab(lsb_solver* solver, int on) {
 int lsb_set_tiled(lsb_solver* solver, int on) {
   if (!solver) return fail(-1, "null solver");
   lsb_solver* s = solver;
+  s->xtuned = true;  // the caller's choice: no autotuning
   const bool want = on != 0 && s->fast32 && fast::tiled_supported(s->g);
   if (want && !s->d_tspec32) {
     if (!s->owns_memory) return fail(-1, "this solver cannot allocate the tiled spectrum");
@@ -992,9 +1126,11 @@ int lsb_profile_step(lsb_solver* s, int batch, const float* d_lambda, const floa
   if (nstruct < 0) return nstruct;
   LSB_TRY(prepare_damage(s, nstruct));
   LSB_TRY(prepare_aniso(s, nstruct));
+  if (!s->xtuned) LSB_TRY(tune_passes(s, batch, d_lambda, d_mu, d_eps, nstruct));
+  sh = s->sh32;  // (the tuned configuration's x-pass blocks)
+  if (!use_fast32(s)) sh.x_blocks_per_instance = s->x_blocks_generic32;
   launch_reset_state(batch, 0, s->d_state, st);
   launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, st);
-  if (!s->xtuned) LSB_TRY(tune_xpass(s, batch));
   const AndersonArgs<float> aa = anderson_args<float>(s, s->depth > 0);
   if (use_slab(s)) {
     pass_slab<float>(s, 0, batch, d_lambda, d_mu, d_eps, nullptr, aa);

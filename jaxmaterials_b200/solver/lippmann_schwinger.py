@@ -149,6 +149,15 @@ class Solver:
         results are bit-identical either way). Returns whether it is in use."""
         return bool(_lib.check(self._lib.lsb_set_tiled(self._h, 1 if on else 0), "lsb_set_tiled"))
 
+    def pass_config(self):
+        """FP32 pass configuration: dict(tiled, xvariant, slab, settled); settled once the
+        autotuner ran (first FP32 solve) or the caller fixed it."""
+        out = np.zeros(4, dtype=np.int32)
+        _lib.check(self._lib.lsb_pass_config(self._h, out.ctypes.data_as(_lib.c_int_p)),
+                   "lsb_pass_config")
+        return {"tiled": bool(out[0]), "xvariant": int(out[1]), "slab": bool(out[2]),
+                "settled": bool(out[3])}
+
     def set_slab(self, on=True):
         """Fused slab pass (inverse y + z + forward y per x-plane; opt-in, measured slower
         than the separate passes at 128^3; results are bit-identical either way). Returns

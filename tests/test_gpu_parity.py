@@ -549,3 +549,39 @@ def test_graph_replay_bit_identical(ls, depth):
         s.close()
     assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
     assert (out[0][2] == out[1][2]).all() and (out[0][3] == out[1][3]).all()
+
+
+def test_autotuner_caches_its_choice(ls, tmp_path, monkeypatch):
+    """The first FP32 solve of a configuration times the candidate pass configurations and
+    records the fastest in the cache file (LSB_TUNE_CACHE); a second solver of the same
+    configuration takes the recorded choice; the fields equal those of every forced
+    configuration (tiled and strided layouts, slab pass on and off)."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import Solver
+
+    cache = tmp_path / "tune.tsv"
+    monkeypatch.setenv("LSB_TUNE_CACHE", str(cache))
+    n = (32, 32, 32)
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    eb = np.tile(EPS_BAR, (3, 1))
+    s = Solver(g, batch=3, depth=2)
+    assert not s.pass_config()["settled"]
+    r = s.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=10)
+    cfg = s.pass_config()
+    assert cfg["settled"]
+    lines = [l.split("\t") for l in cache.read_text().splitlines()]
+    assert any("32x32x32|b3|m2|iso" in l[0] for l in lines)
+    s2 = Solver(g, batch=3, depth=2)
+    s2.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=1)
+    assert s2.pass_config() == cfg
+    s2.close()
+    for tiled, slab in ((True, False), (True, True), (False, False)):
+        f = Solver(g, batch=3, depth=2)
+        f.set_tiled(tiled)
+        f.set_slab(slab)
+        rf = f.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=10)
+        assert torch.equal(rf.epsilon, r.epsilon)
+        f.close()
+    s.close()
