@@ -215,7 +215,21 @@ def batched_run(count, seed, depth):
     by_n = {}
     for g, it in zip(gs, iters):
         by_n.setdefault(g.nx, []).append(float(it.mean()))
+    # each grid size alone (same call, its structures only): where the time goes
+    per_size = {}
+    for n in sorted(by_n):
+        idx = [i for i, g in enumerate(gs) if g.nx == n]
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        _, it_n, _ = c_eff_batch([lms[i] for i in idx], [mus[i] for i in idx], [gs[i] for i in idx],
+                                 depth=depth, maxiter=5000)
+        torch.cuda.synchronize()
+        sec_n = time.perf_counter() - t1
+        per_size[str(n)] = {"structures": len(idx), "seconds": sec_n,
+                            "solves_per_s": 6 * len(idx) / sec_n,
+                            "voxel_iter_per_s": float((nv[idx][:, None] * it_n).sum()) / sec_n}
     return {
+        "per_size_alone": per_size,
         "seconds": sec,
         "solves": 6 * count,
         "value": 6 * count / sec,

@@ -131,8 +131,8 @@ int lsb_set_slab(lsb_solver *solver, int on);
  * whether the configuration is settled (by the autotuner on the first FP32 solve or
  * profile, or by the caller through lsb_tile_variant / lsb_set_tiled / lsb_set_slab).
  * The autotuner times every candidate configuration on the solve's own iteration and
- * keeps the fastest; its choices are cached per (device, grid, batch, Anderson depth,
- * law) in the file named by the environment variable LSB_TUNE_CACHE (default
+ * keeps the fastest; its choices are cached per (device, grid, Anderson depth, law) in
+ * the file named by the environment variable LSB_TUNE_CACHE (default
  * $HOME/.cache/jaxmaterials_b200/tune.tsv; empty or "0": no file). */
 int lsb_pass_config(lsb_solver *solver, int *out);
 

@@ -11,6 +11,9 @@
 // of the memory budget (share proportional to the bucket's voxels); the chunks of a
 // bucket are evened out so that the last one is not a small remainder.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -60,7 +63,7 @@ struct BucketResult {
 
 void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int precision,
                 double rtol, double atol, int maxiter, const float* const* lambda,
-                const float* const* mu, double* c_eff, int* iters, int* status,
+                const float* const* mu, double* c_eff, int* iters, int* status, int priority,
                 BucketResult* out) {
   auto fail_here = [&](int rc) {
     out->rc = rc;
@@ -75,7 +78,7 @@ void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int prec
   chunk = (n + nchunks - 1) / nchunks;
 
   cudaStream_t st = nullptr;
-  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority) != cudaSuccess) {
     out->rc = -2;
     out->error = "cudaStreamCreate failed";
     return;
@@ -99,6 +102,11 @@ void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int prec
   for (int j = 0; j < chunk; ++j)
     for (int k = 0; k < 6; ++k) eb[36 * j + 7 * k] = 1.0;
   std::vector<int> it(6 * chunk), stt(6 * chunk);
+  // LSB_BATCH_TRACE: one line per bucket on stderr (grid, structures, chunking, time, FP64
+  // continuations)
+  const bool trace = std::getenv("LSB_BATCH_TRACE") != nullptr;
+  const auto t_start = std::chrono::steady_clock::now();
+  long long switched = 0, updates = 0;
   for (int c0 = 0; c0 < n && out->rc == 0; c0 += chunk) {
     const int c = std::min(chunk, n - c0);
     for (int j = 0; j < c; ++j) {
@@ -115,12 +123,23 @@ void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int prec
       fail_here(rc);
       break;
     }
+    if (trace)
+      for (int k = 0; k < 6 * c; ++k) {
+        switched += s->h_state[k].switched;
+        updates += s->h_state[k].iter;
+      }
     for (int j = 0; j < c; ++j) {
       const int m = bk.members[c0 + j];
       std::memcpy(c_eff + 36 * (size_t)m, mean.data() + 36 * (size_t)j, sizeof(double) * 36);
       std::memcpy(iters + 6 * (size_t)m, it.data() + 6 * (size_t)j, sizeof(int) * 6);
       std::memcpy(status + 6 * (size_t)m, stt.data() + 6 * (size_t)j, sizeof(int) * 6);
     }
+  }
+  if (trace) {
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    std::fprintf(stderr, "lsb_c_eff_batch: grid %dx%dx%d structures %d chunk %d (%d chunks) %.3f s, "
+                 "%lld updates, %lld instances continued in FP64\n", bk.voxels[0], bk.voxels[1],
+                 bk.voxels[2], n, chunk, nchunks, sec, updates, switched);
   }
   cudaFree(d_lame);
   lsb_destroy(s);
@@ -179,6 +198,26 @@ extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* ext
   double total = 0.0;
   for (const Bucket& b : buckets) total += b.voxels_total;
 
+  // Stream priorities: the smaller a bucket's grid, the higher its priority, so that the
+  // short kernels of small grids are not queued behind the blocks of the large ones (each
+  // small-grid iteration is a chain of short dependent launches); the small buckets then
+  // finish early and the large ones keep the GPU.
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+    cudaGetLastError();
+    least = greatest = 0;
+  }
+  std::vector<double> sizes;
+  for (const Bucket& b : buckets) sizes.push_back((double)b.voxels[0] * b.voxels[1] * b.voxels[2]);
+  std::vector<double> sorted_sizes = sizes;
+  std::sort(sorted_sizes.begin(), sorted_sizes.end());
+  sorted_sizes.erase(std::unique(sorted_sizes.begin(), sorted_sizes.end()), sorted_sizes.end());
+  auto priority_of = [&](size_t b) {
+    // rank 0 (smallest grid) -> greatest priority (numerically lowest), clamped to the range
+    const int rank = (int)(std::lower_bound(sorted_sizes.begin(), sorted_sizes.end(), sizes[b]) -
+                           sorted_sizes.begin());
+    return std::min(least, greatest + rank);
+  };
   // Buckets whose share of the budget holds at least one structure run concurrently, one
   // host thread each; the others run afterwards one at a time with the whole budget.
   std::vector<BucketResult> res(buckets.size());
@@ -192,12 +231,12 @@ extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* ext
     }
     threads.emplace_back(run_bucket, std::cref(buckets[b]), device, share, depth, precision,
                          (double)rtol, (double)atol, maxiter, lambda, mu, c_eff, iters, status,
-                         &res[b]);
+                         priority_of(b), &res[b]);
   }
   for (auto& t : threads) t.join();
   for (size_t b : serial)
     run_bucket(buckets[b], device, budget, depth, precision, (double)rtol, (double)atol, maxiter,
-               lambda, mu, c_eff, iters, status, &res[b]);
+               lambda, mu, c_eff, iters, status, priority_of(b), &res[b]);
   for (size_t b = 0; b < buckets.size(); ++b)
     if (res[b].rc)
       return fail(res[b].rc, "bucket %dx%dx%d: %s", buckets[b].voxels[0], buckets[b].voxels[1],

@@ -443,7 +443,14 @@ struct GraphPhase {
   cudaGraphExec_t exec = nullptr;
   explicit GraphPhase(lsb_solver* solver) : s(solver), user(solver->stream) {
     if (!s->use_graphs) return;
-    if (!s->graph_stream && cudaStreamCreateWithFlags(&s->graph_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // (the graph stream takes the caller's stream priority)
+    int prio = 0;
+    if (cudaStreamGetPriority(user, &prio) != cudaSuccess) {
+      cudaGetLastError();
+      prio = 0;
+    }
+    if (!s->graph_stream &&
+        cudaStreamCreateWithPriority(&s->graph_stream, cudaStreamNonBlocking, prio) != cudaSuccess) {
       s->graph_stream = nullptr;
       cudaGetLastError();
       return;
@@ -642,7 +649,9 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
 // from a fresh state: the initial pass, depth + 2 untimed iterations that fill the
 // Anderson rings, then kTuneReps timed iterations (CUDA events on the solver's stream,
 // tolerances 0 so that every pass does its full work). The fastest is kept; the choice is
-// remembered per (device, grid, batch, depth, law) for the process and in a cache file
+// timed on the instances of at most one structure (at most six; the ranking of the
+// configurations does not depend on the batch) and remembered per (device, grid, depth, law)
+// for the process and in a cache file
 // (LSB_TUNE_CACHE, else $HOME/.cache/jaxmaterials_b200/tune.tsv; an empty value or "0"
 // disables the file), so that later processes skip the timing.
 struct TuneChoice {
@@ -691,15 +700,15 @@ void tune_store_locked(const std::string& key, const TuneChoice& c, float ms) {
   if (out) out << key << '\t' << c.tiled << '\t' << c.xvariant << '\t' << c.slab << '\t' << ms << '\n';
 }
 
-std::string tune_key(const lsb_solver* s, int batch) {
+std::string tune_key(const lsb_solver* s) {
   cudaDeviceProp prop;
   std::string dev = "device";
   if (cudaGetDeviceProperties(&prop, s->device) == cudaSuccess)
     dev = std::string(prop.name) + "/" + std::to_string(prop.multiProcessorCount);
   const char* law = s->g.cf32 ? "aniso" : (s->g.dmg32 ? "damage" : "iso");
   char buf[256];
-  std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|b%d|m%d|%s", dev.c_str(), s->g.nx, s->g.ny, s->g.nz,
-                batch, s->depth, law);
+  std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|m%d|%s", dev.c_str(), s->g.nx, s->g.ny, s->g.nz,
+                s->depth, law);
   return buf;
 }
 
@@ -756,7 +765,10 @@ int tune_passes(lsb_solver* s, int batch, const float* d_lambda, const float* d_
                 int nstruct) {
   if (!use_fast32(s)) return 0;  // the generic passes have one configuration
   s->xtuned = true;
-  const std::string key = tune_key(s, batch);
+  const std::string key = tune_key(s);
+  // one structure's instances (structures_of has set g.lame_group for the solve's batch)
+  const int tb = std::min(batch, std::min(s->g.lame_group, 6));
+  nstruct = 1;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     tune_load_locked();
@@ -779,7 +791,7 @@ int tune_passes(lsb_solver* s, int batch, const float* d_lambda, const float* d_
     for (size_t k = 0; k < cand.size(); ++k) {
       apply_choice(s, cand[k]);
       float ms = 0.f;
-      LSB_TRY(time_config(s, batch, d_lambda, d_mu, d_eps, nstruct, &ms));
+      LSB_TRY(time_config(s, tb, d_lambda, d_mu, d_eps, nstruct, &ms));
       if (k == 0 || ms < best_ms) {
         best_ms = ms;
         best = cand[k];

@@ -572,7 +572,7 @@ def test_autotuner_caches_its_choice(ls, tmp_path, monkeypatch):
     cfg = s.pass_config()
     assert cfg["settled"]
     lines = [l.split("\t") for l in cache.read_text().splitlines()]
-    assert any("32x32x32|b3|m2|iso" in l[0] for l in lines)
+    assert any("32x32x32|m2|iso" in l[0] for l in lines)
     s2 = Solver(g, batch=3, depth=2)
     s2.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=1)
     assert s2.pass_config() == cfg
