@@ -140,11 +140,16 @@ __host__ __device__ constexpr int y_min_blocks() {
 // TILED: the x-pass side of the transform is the tiled layout in `tspec` (see xpass_tiled):
 // the forward pass reads `spec` (cuFFT layout) and writes `tspec`, the inverse pass reads
 // `tspec` and writes `spec`. Otherwise both sides are `spec`, transformed in place.
-// (the tiled form keeps a second base pointer and index terms: three quarters of the
-// resident blocks, so that it does not spill)
+// (the tiled form keeps a second base pointer and index terms; LSB_YT_MINB_NUM / 4 of the
+// in-place form's resident blocks: 4/4 measured fastest at 128^3, 0.141 against 0.151 ms
+// at 3/4, despite a few bytes of spill)
+#ifndef LSB_YT_MINB_NUM
+#define LSB_YT_MINB_NUM 4
+#endif
 template <int NY, bool TILED>
 __global__ void __launch_bounds__(y_threads<NY>(),
-                                  TILED ? (3 * y_min_blocks<NY>() / 4 > 2 ? 3 * y_min_blocks<NY>() / 4 : 2)
+                                  TILED ? (LSB_YT_MINB_NUM * y_min_blocks<NY>() / 4 > 2
+                                               ? LSB_YT_MINB_NUM * y_min_blocks<NY>() / 4 : 2)
                                         : y_min_blocks<NY>()) ypass_fast(GridDesc g, int inverse,
                                                                float2* __restrict__ spec,
                                                                float2* __restrict__ tspec,
@@ -496,8 +501,12 @@ template <>
 struct XTSplit<48> { static constexpr int E = 8, P = 6; };
 template <int NX>
 __host__ __device__ constexpr int xt_threads() { return 6 * XTSplit<NX>::P * kTW; }
+// (three 384-thread blocks per SM: 0.193 against 0.208 ms with two at 128^3)
+#ifndef LSB_XT_MINB
+#define LSB_XT_MINB 3
+#endif
 template <int NX>
-__host__ __device__ constexpr int xt_min_blocks() { return xt_threads<NX>() <= 192 ? 4 : 2; }
+__host__ __device__ constexpr int xt_min_blocks() { return xt_threads<NX>() <= 192 ? 4 : LSB_XT_MINB; }
 
 // Block = one tile (full tile of ky, or a tail group of 8 ky) of one instance; thread
 // (c, p, t) with t fastest.
