@@ -142,6 +142,14 @@ int lsb_pass_config(lsb_solver *solver, int *out);
  * on = 0 launches the kernels one by one on the solver's stream. */
 int lsb_set_graphs(lsb_solver *solver, int on);
 
+/* No reference counterpart. on = 1 (default, with graphs on): each phase of a solve is one
+ * launch of a graph whose conditional WHILE node repeats the captured iteration until no
+ * instance of the phase is running (decided on the device after every iteration, capped
+ * at maxiter + 2 evaluations); the host waits once. on = 0: the host replays the iteration
+ * graph in growing chunks and reads the instance states after each chunk. Both give
+ * bit-identical results. */
+int lsb_set_device_loop(lsb_solver *solver, int on);
+
 /* No reference counterpart. Groups instances by microstructure: with
  * instances_per_field = k > 0, instance b of a solve reads the Lame fields of structure
  * b / k from d_lambda, d_mu laid out [batch / k][nv] (and gets that structure's own

@@ -435,10 +435,27 @@ void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
 // With `anderson` the update is Anderson mixing of depth s->depth (rings of precision T).
 // Moves a phase's work to the solver's graph stream (ordered after everything already on
 // the caller's stream) and back (the caller's stream waits for the phase); owns the graph.
+// End of one body execution of a phase's device-driven loop: counts the evaluations and
+// keeps the loop going while an instance of `phase` is still running and fewer than
+// max_evals evaluations have run (the hard cap that makes the loop terminate even if no
+// instance stops). One warp.
+__global__ void loop_check_kernel(cudaGraphConditionalHandle handle, const InstanceState* __restrict__ st,
+                                  int batch, int phase, int* count, int max_evals) {
+  int any = 0;
+  for (int b = threadIdx.x; b < batch; b += 32) any |= (!st[b].done && st[b].phase == phase) ? 1 : 0;
+  any = __any_sync(0xffffffffu, any);
+  if (threadIdx.x == 0) {
+    const int c = *count + 1;
+    *count = c;
+    cudaGraphSetConditional(handle, (any && c < max_evals) ? 1u : 0u);
+  }
+}
+
 struct GraphPhase {
   lsb_solver* s;
   cudaStream_t user;
   bool on = false;
+  bool loop = false;  // the graph is a device-driven WHILE loop over the iteration
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   explicit GraphPhase(lsb_solver* solver) : s(solver), user(solver->stream) {
@@ -486,6 +503,54 @@ struct GraphPhase {
       graph = nullptr;
       cudaGetLastError();
     }
+  }
+  // Builds a graph of one conditional WHILE node whose body is one enqueue() followed by
+  // loop_check_kernel, so that a single launch runs the phase to its end; on any failure
+  // nothing is kept (capture() or the host-polled loop remains).
+  template <typename F>
+  bool capture_loop(F&& enqueue, int batch, int phase, int max_evals) {
+    if (!on) return false;
+    if (!s->d_loop_count && cudaMalloc(&s->d_loop_count, sizeof(int)) != cudaSuccess) {
+      s->d_loop_count = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphConditionalHandle handle;
+    cudaGraphNode_t node;
+    cudaGraphNodeParams params = {};
+    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      params.type = cudaGraphNodeTypeConditional;
+      params.conditional.handle = handle;
+      params.conditional.type = cudaGraphCondTypeWhile;
+      params.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, g, nullptr, 0, &params) == cudaSuccess;
+    }
+    if (ok) {
+      cudaGraph_t body = params.conditional.phGraph_out[0];
+      ok = cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        enqueue();
+        loop_check_kernel<<<1, 32, 0, s->stream>>>(handle, s->d_state, batch, phase, s->d_loop_count,
+                                                   max_evals);
+        cudaGraph_t captured = nullptr;
+        ok = cudaStreamEndCapture(s->stream, &captured) == cudaSuccess;
+      }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+    if (!ok) {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (g) cudaGraphDestroy(g);
+      exec = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+    graph = g;
+    loop = true;
+    return true;
   }
   ~GraphPhase() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -613,9 +678,26 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
   auto iteration = [&]() {
     enqueue_iteration<T>(s, batch, lam, mu, eps, spec, aa, sp, sh, phase, inject, nullptr);
   };
+  const long long max_evals = (long long)sp.maxiter + 2;
+  // one launch runs the whole phase: a WHILE node over the iteration, stopped on the device
+  if (s->use_loop && gp.capture_loop(iteration, batch, phase, (int)max_evals)) {
+    LSB_CUDA(cudaMemsetAsync(s->d_loop_count, 0, sizeof(int), st));
+    LSB_CUDA(cudaGraphLaunch(gp.exec, st));
+    int evals = 0;
+    LSB_CUDA(cudaMemcpyAsync(s->h_state, s->d_state, sizeof(InstanceState) * batch,
+                             cudaMemcpyDeviceToHost, st));
+    LSB_CUDA(cudaMemcpyAsync(&evals, s->d_loop_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LSB_CUDA(cudaStreamSynchronize(st));
+    LSB_CUDA(take_launch_error(s));
+    s->launches += (iteration_launches(mix, slab) + 1) * evals;
+    for (int b = 0; b < batch; ++b)
+      if (!s->h_state[b].done && s->h_state[b].phase == phase)
+        return fail(-4, "internal: iteration loop stopped after %d evaluations with instance %d running",
+                    evals, b);
+    return 0;
+  }
   gp.capture(iteration);
   long long launched = 0;
-  const long long max_evals = (long long)sp.maxiter + 2;
   int chunk = 1;
   for (;;) {
     int n = (int)std::min<long long>(chunk, max_evals - launched);
@@ -1048,6 +1130,12 @@ int lsb_set_warm_history(lsb_solver* solver, int on) {
   if (!solver) return fail(-1, "null solver");
   if (on && solver->depth == 0) return fail(-1, "a warm start in the Anderson history needs depth >= 1");
   solver->warm_history = on != 0;
+  return 0;
+}
+
+int lsb_set_device_loop(lsb_solver* solver, int on) {
+  if (!solver) return fail(-1, "null solver");
+  solver->use_loop = on != 0;
   return 0;
 }
 

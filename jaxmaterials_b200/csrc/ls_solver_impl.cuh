@@ -41,6 +41,8 @@ struct lsb_solver {
   bool use_graphs = true;
   cudaStream_t graph_stream = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  int* d_loop_count = nullptr;   // evaluations of the device-driven iteration loop
+  bool use_loop = true;          // one WHILE-node graph launch per phase (else host-polled)
   // FP32 work buffers
   float* d_eps32 = nullptr;      // [batch][6][nv] (used when the caller passes no strain buffer)
   float2* d_spec32 = nullptr;    // [batch][6][nm]
@@ -111,7 +113,7 @@ struct lsb_solver {
                     d_epsbar, d_scratch, d_mean_scratch, d_mean, d_history, d_tw32, d_tw64,
                     d_tables, d_aa_g32, d_aa_r32, d_aa_g64, d_aa_r64, d_aa_partials, d_aa_mat,
                     d_aa_alpha, d_e0ref, d_dmg_conv, d_pf_w, d_pf_chi, d_pf_part, d_pf_state,
-                    d_cf_conv, d_c0, d_c0_part};
+                    d_cf_conv, d_c0, d_c0_part, d_loop_count};
     for (void* p : bufs) cudaFree(p);
     if (h_state) cudaFreeHost(h_state);
     if (h_pf_state) cudaFreeHost(h_pf_state);

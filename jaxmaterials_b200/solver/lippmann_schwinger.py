@@ -158,6 +158,11 @@ class Solver:
         return {"tiled": bool(out[0]), "xvariant": int(out[1]), "slab": bool(out[2]),
                 "settled": bool(out[3])}
 
+    def set_device_loop(self, on=True):
+        """Run each solve phase as one graph launch whose WHILE node stops on the device
+        (default), or replay the iteration graph from the host in polled chunks."""
+        _lib.check(self._lib.lsb_set_device_loop(self._h, 1 if on else 0), "lsb_set_device_loop")
+
     def set_slab(self, on=True):
         """Fused slab pass (inverse y + z + forward y per x-plane; opt-in, measured slower
         than the separate passes at 128^3; results are bit-identical either way). Returns

@@ -528,6 +528,35 @@ def test_slab_pass_matches_separate_passes(ls, n, depth):
 
 
 @pytest.mark.parametrize("depth", [0, 3])
+@pytest.mark.parametrize("n", [(32, 32, 16), (37, 47, 61)])
+def test_device_loop_matches_host_polling(ls, n, depth):
+    """One graph launch per phase with the stop decision on the device (conditional WHILE
+    node) gives the same bits and iteration counts as the host-polled graph replays; a
+    zero-iteration case (homogeneous medium) and a maxiter-bounded case stop as well."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import MAXITER, Solver
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    eb = np.tile(EPS_BAR, (2, 1))
+    out = []
+    for loop in (True, False):
+        s = Solver(g, batch=2, depth=depth)
+        s.set_device_loop(loop)
+        r = s.solve(lm, mu, eb, rtol=1e-6, atol=1e-20, maxiter=400)
+        rm = s.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=7)
+        assert (rm.iters == 7).all() and (rm.status == MAXITER).all()
+        rh = s.solve(np.ones(n, np.float32), np.ones(n, np.float32), eb, rtol=1e-20, atol=1e-4,
+                     maxiter=50)
+        assert (rh.iters == 0).all()
+        out.append((r.epsilon.clone(), r.iters.copy(), r.mean_sigma.copy(), rm.epsilon.clone()))
+        s.close()
+    assert torch.equal(out[0][0], out[1][0]) and (out[0][1] == out[1][1]).all()
+    assert (out[0][2] == out[1][2]).all() and torch.equal(out[0][3], out[1][3])
+
+
+@pytest.mark.parametrize("depth", [0, 3])
 def test_graph_replay_bit_identical(ls, depth):
     """Iterations replayed from a CUDA graph and launched kernel by kernel give the same
     bits (same kernels, same order)."""
