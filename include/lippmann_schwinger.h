@@ -110,7 +110,7 @@ int lsb_set_warm_history(lsb_solver *solver, int on);
 int lsb_tile_variant(lsb_solver *solver, int variant);
 
 /* No reference counterpart. Layout of the FP32 spectrum between the y and x passes:
- * on = 1 (the default where it applies: every extent in {16, 32, 48, 64, 96, 128}) keeps
+ * on = 1 (where it applies: every extent in {16, 32, 48, 64, 96, 128}, ny a power of two) keeps
  * it in contiguous x tiles of 8 kz columns in a second spectrum buffer, so that the x pass
  * reads one contiguous chunk per component and tile; on = 0 keeps the cuFFT layout
  * throughout and the strided x pass (lsb_tile_variant). Both give bit-identical results.

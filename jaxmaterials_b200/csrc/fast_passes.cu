@@ -146,11 +146,16 @@ __host__ __device__ constexpr int y_min_blocks() {
 #ifndef LSB_YT_MINB_NUM
 #define LSB_YT_MINB_NUM 4
 #endif
+template <int NY>
+__host__ __device__ constexpr int yt_min_blocks() {
+  // (other extents: half the in-place form's blocks; at 48 and 96, whose threads hold 16
+  // values, the full count spilled and made the pass 2-3x slower)
+  return NY == 128 ? LSB_YT_MINB_NUM * y_min_blocks<NY>() / 4
+                   : (y_min_blocks<NY>() / 2 > 2 ? y_min_blocks<NY>() / 2 : 2);
+}
 template <int NY, bool TILED>
-__global__ void __launch_bounds__(y_threads<NY>(),
-                                  TILED ? (LSB_YT_MINB_NUM * y_min_blocks<NY>() / 4 > 2
-                                               ? LSB_YT_MINB_NUM * y_min_blocks<NY>() / 4 : 2)
-                                        : y_min_blocks<NY>()) ypass_fast(GridDesc g, int inverse,
+__global__ void __launch_bounds__(y_threads<NY>(), TILED ? yt_min_blocks<NY>() : y_min_blocks<NY>())
+    ypass_fast(GridDesc g, int inverse,
                                                                float2* __restrict__ spec,
                                                                float2* __restrict__ tspec,
                                                                const InstanceState* __restrict__ st) {
@@ -1201,8 +1206,11 @@ int x_tiles(const GridDesc& g, int variant) {
   }
 }
 
+// (power-of-two ny only: at ny = 48 and 96 the tiled y pass measured 2-4x slower than the
+// in-place one, 0.50 against 0.11 ms at 48^3 x 96 instances)
 bool tiled_supported(const GridDesc& g) {
-  return supported(g) && g.nx <= 128 && g.ny % kTW == 0 && (g.nzh - 1) % kTW == 0;
+  const bool ypow2 = (g.ny & (g.ny - 1)) == 0;
+  return supported(g) && g.nx <= 128 && ypow2 && g.ny % kTW == 0 && (g.nzh - 1) % kTW == 0;
 }
 
 int x_tiles_tiled(const GridDesc& g) { return g.ny * ((g.nzh - 1) / kTW) + g.ny / kTW; }

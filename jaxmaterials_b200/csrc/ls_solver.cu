@@ -576,11 +576,12 @@ struct StepTimer {
   }
 };
 
-// Blocks per instance of the Anderson Gram-row kernel (as many as the combine kernel, and
-// its partials fit the z-block-sized buffer).
+// Blocks per instance of the Anderson Gram-row kernel: about four 16-byte element groups
+// per thread (fewer left the 64^3 Gram row dominated by its block reductions), at most 2048
+// and within the z-block-sized partials buffer.
 int gram_blocks(const lsb_solver* s) {
   return (int)std::max<long long>(
-      1, std::min<long long>({(long long)s->aa_zblocks, 2048LL, (6 * s->g.nv + 255) / 256}));
+      1, std::min<long long>({(long long)s->aa_zblocks, 2048LL, (6 * s->g.nv + 4095) / 4096}));
 }
 
 // One iteration of precision T: x pass, criterion and stop decision, inverse y pass, then
@@ -731,8 +732,7 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
 // from a fresh state: the initial pass, depth + 2 untimed iterations that fill the
 // Anderson rings, then kTuneReps timed iterations (CUDA events on the solver's stream,
 // tolerances 0 so that every pass does its full work). The fastest is kept; the choice is
-// timed on the instances of at most one structure (at most six; the ranking of the
-// configurations does not depend on the batch) and remembered per (device, grid, depth, law)
+// timed on at most 24 of the solve's instances and remembered per (device, grid, depth, law)
 // for the process and in a cache file
 // (LSB_TUNE_CACHE, else $HOME/.cache/jaxmaterials_b200/tune.tsv; an empty value or "0"
 // disables the file), so that later processes skip the timing.
@@ -848,9 +848,10 @@ int tune_passes(lsb_solver* s, int batch, const float* d_lambda, const float* d_
   if (!use_fast32(s)) return 0;  // the generic passes have one configuration
   s->xtuned = true;
   const std::string key = tune_key(s);
-  // one structure's instances (structures_of has set g.lame_group for the solve's batch)
-  const int tb = std::min(batch, std::min(s->g.lame_group, 6));
-  nstruct = 1;
+  // up to 24 instances (structures_of has set g.lame_group for the solve's batch): enough
+  // for the small grids' ranking to be that of their large batches
+  const int tb = std::min(batch, 24);
+  nstruct = (tb + s->g.lame_group - 1) / s->g.lame_group;
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     tune_load_locked();

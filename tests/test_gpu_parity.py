@@ -474,7 +474,7 @@ def test_x_tile_variants_agree(ls, n):
 
 
 @pytest.mark.parametrize("depth", [0, 3])
-@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 48), (32, 16, 96), (48, 32, 64), (96, 48, 16)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 48), (32, 16, 96), (48, 32, 64), (96, 64, 16)])
 def test_tiled_layout_matches_strided(ls, n, depth):
     """The tiled spectrum layout between the y and x passes gives the fields of the strided
     x pass: bit for bit where both passes split the x transform alike, and to FP32
@@ -502,8 +502,8 @@ def test_tiled_layout_matches_strided(ls, n, depth):
 
 
 @pytest.mark.parametrize("depth", [0, 3])
-@pytest.mark.parametrize("n", [(32, 16, 16), (64, 32, 32), (16, 48, 48), (64, 64, 64),
-                               (48, 96, 96), (128, 128, 128)])
+@pytest.mark.parametrize("n", [(32, 16, 16), (64, 32, 32), (48, 64, 64), (64, 64, 64),
+                               (128, 128, 128)])
 def test_slab_pass_matches_separate_passes(ls, n, depth):
     """The fused slab pass (inverse y, z pass, forward y of every x-plane in one cluster
     kernel) gives the fields of the separate y and z passes bit for bit (same arithmetic,
