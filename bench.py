@@ -54,6 +54,8 @@ def parse():
                    help="grid of the anisotropic C_eff leg (0: skip)")
     p.add_argument("--c2-256", type=int, default=1, dest="c2_256",
                    help="steps of the 256^3 config-2 leg (0: skip)")
+    p.add_argument("--learned", type=int, default=32,
+                   help="grid of the bounded learned warm-start leg (0: skip)")
     p.add_argument("--comparators", type=int, default=1,
                    help="time the cuFFT loop and the reference's CUDA library (0: skip)")
     # fixed-iteration runs for profilers (no JSON line): every pass of every iteration does
@@ -172,6 +174,68 @@ def aniso_run(n):
                            "cores": os.cpu_count(), "kind": "port",
                            "sample": f"3 anisotropic Anderson updates of one load at {m}^3 "
                                      "(oracle, FP32 fields, SciPy FFT on all cores)"}
+    return res
+
+
+def learned_run(n, train_count, test_count, epochs, depth):
+    """The learned warm start (config 5) at a bounded size, so that the line carries it:
+    `train_count` structures of the batched distribution at n^3 solved by the library
+    (training data), the spectral network trained on them by the library's kernels
+    (`epochs` epochs), then `test_count` held-out structures solved as batches cold,
+    warm-started (compatible part of the prediction, the same absolute stop), with the
+    scaled start and with the prediction in the Anderson history, and with the plain
+    iteration (depth 0, cold). The full configuration (4096 structures at 64^3, 20 epochs)
+    is `python -m jaxmaterials_b200.learned.warm_start`."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.learned import warm_start as W
+    from jaxmaterials_b200.learned.network import SpectralNet
+    from jaxmaterials_b200.solver import Solver
+
+    t0 = time.perf_counter()
+    ind = torch.as_tensor(W.indicators(W.structure_params(train_count, n, 11))).cuda()
+    targets, it = W.solve_dataset(ind, depth=depth)
+    torch.cuda.synchronize()
+    data_s = time.perf_counter() - t0
+    net = SpectralNet(seed=0)
+    t0 = time.perf_counter()
+    losses = W.train(net, ind, targets, epochs=epochs)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del targets, ind
+    torch.cuda.empty_cache()
+    test = torch.as_tensor(W.indicators(W.structure_params(test_count, n, 12))).cuda()
+    chunk = min(16, test_count)
+    res = W.summarise(W.evaluate(net, test, depth=depth, chunk=chunk), n)
+    # the plain iteration on the same held-out structures, same batches
+    g = GridSpec(n, n, n, float(n), float(n), float(n))
+    s = Solver(g, batch=6 * chunk, depth=0)
+    eye = np.eye(6, dtype=np.float32)
+    plain_s, plain_it = 0.0, []
+    for c0 in range(0, test_count, chunk):
+        c = min(chunk, test_count - c0)
+        lm, mu = W.lame_from_indicator(test[c0:c0 + c])
+        s.solve(lm, mu, np.tile(eye, (c, 1)), rtol=1e-6, maxiter=5000, want_sigma=False)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = s.solve(lm, mu, np.tile(eye, (c, 1)), rtol=1e-6, maxiter=5000, want_sigma=False)
+        torch.cuda.synchronize()
+        plain_s += time.perf_counter() - t0
+        plain_it.append(r.iters)
+    s.close()
+    plain = 6 * test_count / plain_s
+    best = max(("warm", res["warm_solves_per_s"]), ("scaled", res["scaled_solves_per_s"]),
+               ("history", res["history_solves_per_s"]), key=lambda kv: kv[1])
+    res.update({
+        "train_structures": train_count, "epochs": epochs, "data_s": data_s, "train_s": train_s,
+        "final_loss": losses[-1], "plain_iters_per_solve": float(np.concatenate(plain_it).mean()),
+        "plain_solves_per_s": plain,
+        "learned_batched_solves_per_s": best[1], "learned_mode": best[0],
+        "learned_batched_vs_plain": best[1] / plain,
+        "cold_anderson_batched_vs_plain": res["cold_solves_per_s"] / plain,
+        "timing": "wall clock per batch of 16 structures x 6 loads after the network's inference "
+                  "(included in the warm figures)",
+    })
     return res
 
 
@@ -880,6 +944,14 @@ def own_arm(args):
         except Exception as exc:  # reported in the line; the solver figures stand
             comparators = {"error": f"{type(exc).__name__}: {exc}"}
 
+    learned = None
+    if args.learned > 0 and world == 1:
+        torch.cuda.empty_cache()
+        try:
+            learned = learned_run(args.learned, 256, 64, 6, args.depth)
+        except Exception as exc:  # reported in the line; the solver figures stand
+            learned = {"error": f"{type(exc).__name__}: {exc}"}
+
     c2_256 = None
     if args.c2_256 > 0 and world == 1:
         torch.cuda.empty_cache()
@@ -913,6 +985,7 @@ def own_arm(args):
             "fp64_iteration_share": fp64_share,
             "plain": plain,
             "c2_256": c2_256,
+            "learned": learned,
             "comparators": comparators,
             "batched": batched,
             "generator": generator,
