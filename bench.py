@@ -83,6 +83,7 @@ def profile_case(args):
     lm, mu = fibres.lame_fields(st)
     g = GridSpec(n, n, n, float(n), float(n), float(n))
     s = Solver(g, batch=args.batch, depth=args.depth, precision=args.precision)
+    s.set_device_loop(False)  # profilers do not see kernels inside conditional graphs
     eb = np.eye(6, dtype=np.float32)[np.arange(args.batch) % 6]
     r = s.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=args.iters, want_sigma=False)
     torch.cuda.synchronize()

@@ -147,7 +147,9 @@ int lsb_set_graphs(lsb_solver *solver, int on);
  * instance of the phase is running (decided on the device after every iteration, capped
  * at maxiter + 2 evaluations); the host waits once. on = 0: the host replays the iteration
  * graph in growing chunks and reads the instance states after each chunk. Both give
- * bit-identical results. */
+ * bit-identical results. The environment variable LSB_DEVICE_LOOP=0 sets the default of
+ * new solvers to 0 (kernel profilers do not see the kernels of graphs that hold
+ * conditional nodes). */
 int lsb_set_device_loop(lsb_solver *solver, int on);
 
 /* No reference counterpart. Groups instances by microstructure: with

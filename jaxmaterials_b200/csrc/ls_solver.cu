@@ -286,6 +286,9 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
   auto* s = new lsb_solver();
   s->batch_cap = batch;
   s->depth = depth;
+  // LSB_DEVICE_LOOP=0: host-polled graph replays instead of the conditional-node loop
+  // (profilers cannot see the kernels of graphs that hold conditional nodes)
+  if (const char* env = std::getenv("LSB_DEVICE_LOOP")) s->use_loop = std::string(env) != "0";
   cudaGetDevice(&s->device);
   int rc = plan_grid(s, voxels, extents);
   if (rc) {
