@@ -934,10 +934,13 @@ __device__ __forceinline__ void slab_ydft(float2* cols, int kw, bool inverse, co
   const int tid = threadIdx.x, nt = blockDim.x;
   const int per_round = nt / P;
   const int ncols = 6 * kw;
-  const int p = tid % P, qq = tid / P;
+  // columns across the lanes, as in ypass_fast: the lanes of a warp touch neighbouring
+  // columns of one slot, so neither step has bank conflicts (p across the lanes put every
+  // step-B read of a warp in one bank)
+  const int qq = tid % per_round, p = tid / per_round;
   for (int base = 0; base < ncols; base += per_round) {
     const int q = base + qq;
-    const bool on = qq < per_round && q < ncols;
+    const bool on = p < P && q < ncols;
     float2* col = cols + (on ? ((size_t)(q / kw) * NY * kSlabKW + (q % kw)) : 0);
     float2 v[E];
     if (on) {
@@ -1010,6 +1013,22 @@ __global__ void __launch_bounds__(slab_threads<NZ>(), 1) slab_fast(
   const size_t tail0 = (size_t)NY * NF * nx * kTW;
   constexpr bool kInverse = MODE == 1 || MODE == 3;
   constexpr bool kForward = MODE != 3;
+  // phase B reads this rank's rows of the strain (and lambda, mu): contiguous ROWS x NZ
+  // chunks, prefetched into L2 now so that those loads do not wait on DRAM after phase A
+  // (bulk prefetches need 16-byte aligned addresses: skipped for unaligned caller buffers)
+  const bool aligned = ((reinterpret_cast<uintptr_t>(eb) | reinterpret_cast<uintptr_t>(lambda) |
+                         reinterpret_cast<uintptr_t>(mu)) & 15) == 0;
+  if (tid == 0 && aligned && (MODE == 1 || MODE == 2 || MODE == 3)) {
+    const size_t row0 = ((size_t)x * NY + (size_t)rank * ROWS) * NZ;
+    const unsigned bytes = ROWS * NZ * 4;
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(eb + (size_t)c * nv + row0), "r"(bytes) : "memory");
+    if (MODE != 3) {
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(lambda + (size_t)(b / g.lame_group) * nv + row0), "r"(bytes) : "memory");
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(mu + (size_t)(b / g.lame_group) * nv + row0), "r"(bytes) : "memory");
+    }
+  }
 
   // ---- phase A: the rank's columns (tile `rank`, and the Nyquist column on the last rank)
   if constexpr (kInverse) {
