@@ -289,14 +289,58 @@ __device__ __forceinline__ void x_forward(float2* tr, float2* v, int p, int t, c
   __syncthreads();
 }
 
-// Per mode of the block's tile (all six components in the regions of buf): the FP64
-// Hermitian-weighted |xi~ . sigma_hat|^2 (returned, this thread's share), the FP64 zero
-// mode, and r_hat = -Gamma^0 sigma_hat written back conjugated for the inverse transform.
-// col_ky / col_kz map a column index to its (ky, kz); colf holds the columns' ky and kz
-// wave-vector factors.
+// Wave-vector factors of a block's columns and rows, in shared memory:
+// tilde(xi)_d = (2 n_d / L_d) * sin/cos products (fourier.py:9-58), tabulated in FP64 and
+// kept as FP32 for the isotropic Gamma^0 (whose operator is applied in FP32), as FP64 as
+// well for the anisotropic one (its per-mode acoustic inverse is FP64).
+template <int NX, int T, bool ANI>
+struct XWave {
+  float f[3][T];
+  float sx[NX], cx[NX];
+  double df[3][ANI ? T : 1];
+  double dsx[ANI ? NX : 1], dcx[ANI ? NX : 1];
+  // threads tid < T fill the column factors, all threads the row tables
+  template <typename CY, typename CZ>
+  __device__ __forceinline__ void fill(const GridDesc& g, CY col_ky, CZ col_kz) {
+    const int tid = threadIdx.x;
+    if (tid < T) {
+      const int kzz = col_kz(tid) < g.nzh ? col_kz(tid) : 0;
+      const int kyy = col_ky(tid);
+      const double c0 = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
+      const double c1 = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
+      const double c2 = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
+      f[0][tid] = (float)c0;
+      f[1][tid] = (float)c1;
+      f[2][tid] = (float)c2;
+      if constexpr (ANI) {
+        df[0][tid] = c0;
+        df[1][tid] = c1;
+        df[2][tid] = c2;
+      }
+    }
+    for (int i = tid; i < NX; i += blockDim.x) {
+      sx[i] = (float)g.sx[i];
+      cx[i] = (float)g.cx[i];
+      if constexpr (ANI) {
+        dsx[i] = g.sx[i];
+        dcx[i] = g.cx[i];
+      }
+    }
+  }
+};
+
+// Per mode of the block's tile (all six components in the regions of buf): the
+// Hermitian-weighted |xi~ . sigma_hat|^2 (FP32 per mode, summed in FP64; returned, this
+// thread's share), the FP64 zero mode, and r_hat = -Gamma^0 sigma_hat written back
+// conjugated for the inverse transform. col_ky / col_kz map a column index to its (ky, kz).
+// The isotropic form computes the wave vector and its norm in FP32 from the FP64 tables:
+// the operator it feeds is FP32, and the FP32 |xi|^2 differs from the FP64 one by
+// rounding (relative 1e-7; a component that underflows FP32 is below 1e-7 of another one
+// or the mode is below the guard either way), so the guard |xi|^2 < 1e-24 takes the same
+// modes in both except within that rounding of the threshold.
 template <int NX, int T, int REG, bool ANI, typename CY, typename CZ>
-__device__ __forceinline__ double x_modes(float2* buf, const double (*colf)[T], const double* ssx,
-                                          const double* scx, const GridDesc& g, const Medium& md,
+__device__ __forceinline__ double x_modes(float2* buf, const XWave<NX, T, ANI>& wv,
+                                          const GridDesc& g, const Medium& md,
                                           InstanceState* st, int b, CY col_ky, CZ col_kz) {
   const int tid = threadIdx.x;
   const int nzh = g.nzh;
@@ -309,18 +353,15 @@ __device__ __forceinline__ double x_modes(float2* buf, const double (*colf)[T], 
     float2 s[6];
 #pragma unroll
     for (int cc = 0; cc < 6; ++cc) s[cc] = buf[(size_t)cc * REG + kx * T + tt];
-    const double sxk = ssx[kx], cxk = scx[kx];
-    const double x0 = sxk * colf[0][tt];
-    const double x1 = cxk * colf[1][tt];
-    const double x2 = cxk * colf[2][tt];
+    const float f0 = wv.sx[kx] * wv.f[0][tt];
+    const float f1 = wv.cx[kx] * wv.f[1][tt];
+    const float f2 = wv.cx[kx] * wv.f[2][tt];
     {
-      const float f0 = (float)x0, f1 = (float)x1, f2 = (float)x2;
       float2 d0 = make_float2(f0 * s[0].x + f1 * s[3].x + f2 * s[4].x, f0 * s[0].y + f1 * s[3].y + f2 * s[4].y);
       float2 d1 = make_float2(f0 * s[3].x + f1 * s[1].x + f2 * s[5].x, f0 * s[3].y + f1 * s[1].y + f2 * s[5].y);
       float2 d2 = make_float2(f0 * s[4].x + f1 * s[5].x + f2 * s[2].x, f0 * s[4].y + f1 * s[5].y + f2 * s[2].y);
-      double m2 = (double)d0.x * d0.x + (double)d0.y * d0.y + (double)d1.x * d1.x +
-                  (double)d1.y * d1.y + (double)d2.x * d2.x + (double)d2.y * d2.y;
-      acc += ((kzz == 0 || 2 * kzz == g.nz) ? 1.0 : 2.0) * m2;
+      const float m2 = d0.x * d0.x + d0.y * d0.y + d1.x * d1.x + d1.y * d1.y + d2.x * d2.x + d2.y * d2.y;
+      acc += ((kzz == 0 || 2 * kzz == g.nz) ? 1.0 : 2.0) * (double)m2;
     }
     if (kx == 0 && col_ky(tt) == 0 && kzz == 0) {
 #pragma unroll
@@ -329,10 +370,13 @@ __device__ __forceinline__ double x_modes(float2* buf, const double (*colf)[T], 
         st[b].sig0[2 * cc + 1] = (double)s[cc].y;
       }
     }
-    // normalised wave vector: |xi| < 1e-12 (|xi|^2 < 1e-24) is replaced by 1 (fourier.py:84)
-    const double n2 = x0 * x0 + x1 * x1 + x2 * x2;
-    const double inv = n2 < 1.0e-24 ? 1.0 : rsqrt(n2);
     if constexpr (ANI) {
+      // normalised wave vector: |xi| < 1e-12 (|xi|^2 < 1e-24) is replaced by 1 (fourier.py:84)
+      const double x0 = wv.dsx[kx] * wv.df[0][tt];
+      const double x1 = wv.dcx[kx] * wv.df[1][tt];
+      const double x2 = wv.dcx[kx] * wv.df[2][tt];
+      const double n2 = x0 * x0 + x1 * x1 + x2 * x2;
+      const double inv = n2 < 1.0e-24 ? 1.0 : rsqrt(n2);
       // r = -Gamma^0 tau through the inverse acoustic matrix (FP64 per mode); modes without a
       // direction get r = 0
       const double zd[3] = {x0 * inv, x1 * inv, x2 * inv};
@@ -359,7 +403,10 @@ __device__ __forceinline__ double x_modes(float2* buf, const double (*colf)[T], 
       for (int cc = 0; cc < 6; ++cc) buf[(size_t)cc * REG + kx * T + tt] = make_float2(o[0][cc], -o[1][cc]);
       continue;
     }
-    const float z0 = (float)(x0 * inv), z1 = (float)(x1 * inv), z2 = (float)(x2 * inv);
+    // normalised wave vector: |xi| < 1e-12 (|xi|^2 < 1e-24) is replaced by 1 (fourier.py:84)
+    const float n2 = f0 * f0 + f1 * f1 + f2 * f2;
+    const float inv = n2 < 1.0e-24f ? 1.f : rsqrtf(n2);
+    const float z0 = f0 * inv, z1 = f1 * inv, z2 = f2 * inv;
     const float z00 = z0 * z0, z11 = z1 * z1, z22 = z2 * z2;
     const float z01 = z0 * z1, z02 = z0 * z2, z12 = z1 * z2;
     float r[2][6];
@@ -440,11 +487,10 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
   extern __shared__ __align__(16) unsigned char xfraw[];
   float2* buf = reinterpret_cast<float2*>(xfraw);  // 6 regions of REG values
   __shared__ double red[32];
-  __shared__ double colf[3][T];  // per-column wave-vector factors
   // shared-memory copies of the x twiddles and wave-vector tables (read per element / mode;
   // from shared memory the x pass is 6% faster at 128^3 than from the L1/global path)
-  __shared__ float2 stw[NX];           // exp(-2 pi i k / NX)
-  __shared__ double ssx[NX], scx[NX];  // sin, cos(pi kx / NX)
+  __shared__ float2 stw[NX];  // exp(-2 pi i k / NX)
+  __shared__ XWave<NX, T, ANI> wv;
   const int b = blockIdx.z;
   if (!active32(st[b])) return;
   const int tid = threadIdx.x;
@@ -468,29 +514,16 @@ __global__ void __launch_bounds__(6 * XSplit<NX>::P * x_cols_v<NX, V>(), x_min_b
   const float2* tw = g.px.tw;
   float2* tr = buf + (size_t)c * REG;   // this component's region
 
-  if (tid < T) {
-    // tilde(xi)_d = (2 n_d / L_d) * sin/cos products (fourier.py:9-58); the ky and kz
-    // factors of this block's columns, FP64
-    const int kzz = col_kz(tid) < nzh ? col_kz(tid) : 0;
-    const int kyy = col_ky(tid);
-    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
-    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
-    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
-  }
+  wv.fill(g, col_ky, col_kz);
 
   // forward: load, step A, transpose
   float2 v[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = valid ? gcol[(size_t)(p + P * e) * xstride] : make_float2(0.f, 0.f);
-  for (int i = tid; i < NX; i += blockDim.x) {
-    stw[i] = tw[i];
-    ssx[i] = g.sx[i];
-    scx[i] = g.cx[i];
-  }
+  for (int i = tid; i < NX; i += blockDim.x) stw[i] = tw[i];
   __syncthreads();
   x_forward<NX, T>(tr, v, p, t, stw);
-  const double acc = x_modes<NX, T, REG, ANI>(buf, colf, ssx, scx, g, med[b / g.lame_group], st, b,
-                                              col_ky, col_kz);
+  const double acc = x_modes<NX, T, REG, ANI>(buf, wv, g, med[b / g.lame_group], st, b, col_ky, col_kz);
   x_inverse<NX, T, XSplit<NX>>(tr, p, t, stw, [&](int k, float2 w) {
     if (valid) gcol[(size_t)k * xstride] = w;
   });
@@ -525,9 +558,8 @@ __global__ void __launch_bounds__(xt_threads<NX>(), xt_min_blocks<NX>()) xpass_t
   extern __shared__ __align__(128) unsigned char xtraw[];
   float2* buf = reinterpret_cast<float2*>(xtraw);  // 6 regions of REG values
   __shared__ double red[32];
-  __shared__ double colf[3][T];
   __shared__ float2 stw[NX];
-  __shared__ double ssx[NX], scx[NX];
+  __shared__ XWave<NX, T, ANI> wv;
   __shared__ __align__(8) unsigned long long mbar_word;
   const int b = blockIdx.y;
   if (!active32(st[b])) return;
@@ -554,17 +586,8 @@ __global__ void __launch_bounds__(xt_threads<NX>(), xt_min_blocks<NX>()) xpass_t
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(6 * bytes) : "memory");
     for (int cc = 0; cc < 6; ++cc) bulk_g2s(buf + (size_t)cc * REG, sb + (size_t)cc * g.nm + chunk, bytes, mbar);
   }
-  if (tid < T) {
-    const int kzz = col_kz(tid), kyy = col_ky(tid);
-    colf[0][tid] = (2.0 * g.nx / g.Lx) * g.cy[kyy] * g.cz[kzz];
-    colf[1][tid] = (2.0 * g.ny / g.Ly) * g.sy[kyy] * g.cz[kzz];
-    colf[2][tid] = (2.0 * g.nz / g.Lz) * g.cy[kyy] * g.sz[kzz];
-  }
-  for (int i = tid; i < NX; i += blockDim.x) {
-    stw[i] = g.px.tw[i];
-    ssx[i] = g.sx[i];
-    scx[i] = g.cx[i];
-  }
+  wv.fill(g, col_ky, col_kz);
+  for (int i = tid; i < NX; i += blockDim.x) stw[i] = g.px.tw[i];
   if (!mbar_wait(mbar)) {
     // the copies did not land in time: report, leave the instance stopped, and wait once
     // more (bounded) before the shared memory is released
@@ -582,8 +605,7 @@ __global__ void __launch_bounds__(xt_threads<NX>(), xt_min_blocks<NX>()) xpass_t
   for (int e = 0; e < E; ++e) v[e] = tr[(p + P * e) * T + t];
   __syncthreads();
   x_forward<NX, T, SP>(tr, v, p, t, stw);
-  const double acc = x_modes<NX, T, REG, ANI>(buf, colf, ssx, scx, g, med[b / g.lame_group], st, b,
-                                              col_ky, col_kz);
+  const double acc = x_modes<NX, T, REG, ANI>(buf, wv, g, med[b / g.lame_group], st, b, col_ky, col_kz);
   float2* gout = sb + (size_t)c * g.nm + chunk;
   x_inverse<NX, T, SP>(tr, p, t, stw, [&](int k, float2 w) { gout[(size_t)k * T + t] = w; });
   x_block_sum(acc, red, partials + (size_t)b * gridDim.x + tile);

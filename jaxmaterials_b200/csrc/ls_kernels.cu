@@ -659,67 +659,116 @@ __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int
 // relabelling of the ring), A v = 1 is solved over the filled slots in FP64 by Gaussian
 // elimination with partial pivoting, alpha = v / sum(v). A singular or non-finite solve
 // falls back to the plain update alpha = e_slot.
-__global__ void anderson_solve_kernel(int nzblk, int depth, int phase, const InstanceState* __restrict__ st,
-                                      const double* __restrict__ partials, double* __restrict__ amat,
-                                      double* __restrict__ alpha) {
-  __shared__ double dot[kMaxDepth + 1];
+// The Gram row's block partials (nzblk rows of M1 values) are summed by the whole block,
+// each thread over a few rows with independent loads, then across warps; A is staged in
+// shared memory. The elimination runs on one thread over an M1 x M1 system held in
+// registers (compile-time M1): rows and columns past `filled` are an identity block with a
+// zero right-hand side, which leaves the filled block's arithmetic, pivots and solution
+// as they are and gives v = 0 on the padding.
+constexpr int kSolveThreads = 256;
+template <int M1>
+__global__ void __launch_bounds__(kSolveThreads) anderson_solve_kernel(
+    int nzblk, int phase, const InstanceState* __restrict__ st,
+    const double* __restrict__ partials, double* __restrict__ amat, double* __restrict__ alpha) {
+  __shared__ double red[kSolveThreads / 32][M1];
+  __shared__ double sA[M1 * M1];
   const int b = blockIdx.x;
   const InstanceState& s = st[b];
   if (s.done || s.phase != phase) return;
-  const int M1 = depth + 1;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int slot, filled;
-  anderson_slots<double>(s, depth, slot, filled);
-  if (warp < filled) {
-    double a = 0.0;
-    for (int i = lane; i < nzblk; i += 32) a += partials[((size_t)b * nzblk + i) * M1 + warp];
+  anderson_slots<double>(s, M1 - 1, slot, filled);
+  double* A = amat + (size_t)b * M1 * M1;
+  if (tid < M1 * M1) sA[tid] = A[tid];
+  double a[M1];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) dot[warp] = a;
+  for (int q = 0; q < M1; ++q) a[q] = 0.0;
+  const double* pb = partials + (size_t)b * nzblk * M1;
+#pragma unroll 4
+  for (int i = tid; i < nzblk; i += kSolveThreads) {
+#pragma unroll
+    for (int q = 0; q < M1; ++q)
+      if (q < filled) a[q] += pb[(size_t)i * M1 + q];
+  }
+#pragma unroll
+  for (int q = 0; q < M1; ++q) {
+    if (q >= filled) break;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a[q] += __shfl_xor_sync(0xffffffffu, a[q], o);
+    if (lane == 0) red[warp][q] = a[q];
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
-  double* A = amat + (size_t)b * M1 * M1;
-  for (int q = 0; q < filled; ++q) {
-    A[slot * M1 + q] = dot[q];
-    A[q * M1 + slot] = dot[q];
+  if (tid < filled) {
+    double t = 0.0;
+    for (int w = 0; w < kSolveThreads / 32; ++w) t += red[w][tid];
+    sA[slot * M1 + tid] = t;
+    sA[tid * M1 + slot] = t;
+    A[slot * M1 + tid] = t;
+    A[tid * M1 + slot] = t;
   }
-  double m[kMaxDepth + 1][kMaxDepth + 2];
-  for (int i = 0; i < filled; ++i) {
-    for (int j = 0; j < filled; ++j) m[i][j] = A[i * M1 + j];
-    m[i][filled] = 1.0;
+  __syncthreads();
+  if (tid != 0) return;
+  double m[M1][M1 + 1];
+#pragma unroll
+  for (int i = 0; i < M1; ++i) {
+#pragma unroll
+    for (int j = 0; j < M1; ++j)
+      m[i][j] = (i < filled && j < filled) ? sA[i * M1 + j] : (i == j ? 1.0 : 0.0);
+    m[i][M1] = i < filled ? 1.0 : 0.0;
   }
+  // (constant trip counts with guards, so that every index is a compile-time constant and
+  // m stays in registers)
   bool ok = true;
-  for (int c = 0; c < filled && ok; ++c) {
+#pragma unroll
+  for (int c = 0; c < M1; ++c) {
     int piv = c;
-    for (int i = c + 1; i < filled; ++i)
-      if (fabs(m[i][c]) > fabs(m[piv][c])) piv = i;
-    if (!(fabs(m[piv][c]) > 0.0)) { ok = false; break; }
-    if (piv != c)
-      for (int j = c; j <= filled; ++j) { double t = m[c][j]; m[c][j] = m[piv][j]; m[piv][j] = t; }
-    for (int i = c + 1; i < filled; ++i) {
-      const double f = m[i][c] / m[c][c];
-      for (int j = c; j <= filled; ++j) m[i][j] -= f * m[c][j];
-    }
+    double pv = fabs(m[c][c]);
+#pragma unroll
+    for (int i = 0; i < M1; ++i)
+      if (i > c) {
+        const double av = fabs(m[i][c]);
+        if (av > pv) { pv = av; piv = i; }
+      }
+    // (a zero pivot ends the solve; the remaining columns' arithmetic is discarded)
+    if (!(pv > 0.0)) ok = false;
+#pragma unroll
+    for (int i = 0; i < M1; ++i)
+      if (i > c) {
+        const bool sw = piv == i;
+#pragma unroll
+        for (int j = 0; j <= M1; ++j)
+          if (j >= c) {
+            const double x = m[c][j], y = m[i][j];
+            m[c][j] = sw ? y : x;
+            m[i][j] = sw ? x : y;
+          }
+      }
+#pragma unroll
+    for (int i = 0; i < M1; ++i)
+      if (i > c) {
+        const double f = m[i][c] / m[c][c];
+#pragma unroll
+        for (int j = 0; j <= M1; ++j)
+          if (j >= c) m[i][j] -= f * m[c][j];
+      }
   }
-  double v[kMaxDepth + 1];
+  double v[M1];
   double sum = 0.0;
   if (ok) {
-    for (int i = filled - 1; i >= 0; --i) {
-      double t = m[i][filled];
-      for (int j = i + 1; j < filled; ++j) t -= m[i][j] * v[j];
+#pragma unroll
+    for (int i = M1 - 1; i >= 0; --i) {
+      double t = m[i][M1];
+#pragma unroll
+      for (int j = 0; j < M1; ++j)
+        if (j > i) t -= m[i][j] * v[j];
       v[i] = t / m[i][i];
       sum += v[i];
     }
     ok = isfinite(sum) && sum != 0.0;
   }
   double* al = alpha + (size_t)b * M1;
-  for (int q = 0; q < M1; ++q) al[q] = 0.0;
-  if (ok) {
-    for (int q = 0; q < filled; ++q) al[q] = v[q] / sum;
-  } else {
-    al[slot] = 1.0;
-  }
+#pragma unroll
+  for (int q = 0; q < M1; ++q) al[q] = ok ? (q < filled ? v[q] / sum : 0.0) : (q == slot ? 1.0 : 0.0);
 }
 
 __global__ void reset_state_kernel(int batch, int phase, const double* e0_ref, InstanceState* st) {
@@ -995,8 +1044,16 @@ void launch_zpass(const GridDesc& g, const LaunchShape& s, int mode, int batch, 
 
 void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
                            const double* partials, double* amat, double* alpha, cudaStream_t stream) {
-  anderson_solve_kernel<<<batch, 32 * (depth + 1), 0, stream>>>(nzblk, depth, phase, st, partials,
-                                                                 amat, alpha);
+  switch (depth + 1) {
+#define LSB_SOLVE(M)                                                                          \
+    case M:                                                                                   \
+      anderson_solve_kernel<M><<<batch, kSolveThreads, 0, stream>>>(nzblk, phase, st, partials, \
+                                                                    amat, alpha);              \
+      break;
+    LSB_SOLVE(2) LSB_SOLVE(3) LSB_SOLVE(4) LSB_SOLVE(5) LSB_SOLVE(6) LSB_SOLVE(7) LSB_SOLVE(8) LSB_SOLVE(9)
+#undef LSB_SOLVE
+    default: break;
+  }
 }
 
 template <typename T>
