@@ -453,8 +453,9 @@ def cpu_sample(lm, mu, g, depth, budget_s, threads):
 def kernel_bytes(name, nv, nm, batch, depth):
     """Algorithmic bytes of one launch of the named kernel over `batch` instances of one
     structure (FP32 fields: real field 6 Nv 4 B, half spectrum 6 Nm 8 B, Lame pair 2 Nv 4 B;
-    every Anderson ring slot filled)."""
+    residual ring slots in FP16, 6 Nv 2 B; every Anderson ring slot filled)."""
     real, spec, lame = 6 * nv * 4, 6 * nm * 8, 2 * nv * 4
+    res = 6 * nv * 2
     m1 = depth + 1
     table = {
         "x pass": batch * 2 * spec,                          # spectrum read + write
@@ -462,14 +463,14 @@ def kernel_bytes(name, nv, nm, batch, depth):
         "y pass inverse": batch * 2 * spec,
         "y pass forward": batch * 2 * spec,
         "z pass update": batch * (2 * spec + 2 * real) + lame,  # spectrum r/w, eps r/w
-        "z pass residual rings": batch * (spec + real + 2 * real),  # spectrum, eps in; r, g out
-        "anderson gram": batch * m1 * real,                  # every r slot
+        "z pass residual rings": batch * (spec + real + res + real),  # spectrum, eps in; r, g out
+        "anderson gram": batch * m1 * res,                   # every r slot
         "anderson solve": 0,
         "anderson combine": batch * (m1 * real + real),      # every g slot in, eps out
         "z pass stress": batch * (real + spec) + lame,        # eps in, spectrum out
         # fused slab pass: the z pass's bytes (the y transforms stay on chip)
         "slab update": batch * (2 * spec + 2 * real) + lame,
-        "slab residual rings": batch * (spec + real + 2 * real),
+        "slab residual rings": batch * (spec + real + res + real),
         "slab stress": batch * (real + spec) + lame,
     }
     if name not in table:

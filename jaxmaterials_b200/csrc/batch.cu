@@ -43,9 +43,10 @@ size_t bytes_per_structure(const int v[3], int depth, int precision, int maxiter
   const size_t nv = (size_t)v[0] * v[1] * v[2];
   const size_t nm = (size_t)v[0] * v[1] * (v[2] / 2 + 1);
   const size_t partials = 8 * ((size_t)v[1] * (v[2] / 2 + 1) +
-                               (depth > 0 ? (size_t)v[0] * v[1] * (depth + 1) : 0));
+                               (depth > 0 ? (size_t)v[0] * v[1] * (depth + 2) : 0));
   const size_t history = 8 * ((size_t)maxiter + 8);
-  const size_t inst32 = 24 * nv + 48 * nm + (depth > 0 ? 2 * (size_t)(depth + 1) * 24 * nv : 0) +
+  // rings: g in FP32 and r in FP16, m+1 slots of 6 nv each
+  const size_t inst32 = 24 * nv + 48 * nm + (depth > 0 ? (size_t)(depth + 1) * 36 * nv : 0) +
                         6 * 1024 * 8 + partials + history;
   size_t inst64 = 0;
   if (precision != LSB_PREC_FP32) {

@@ -799,9 +799,12 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
     const int M1 = aa.depth + 1;
     const size_t ring = (size_t)6 * g.nv;
     const int slot = (st[b].iter - 1 - st[b].aa_base) % M1;
-    float* rb = aa.r + (size_t)b * M1 * ring;
+    __half* rb = aa.r + (size_t)b * M1 * ring;
     float* gb = aa.g + (size_t)b * M1 * ring;
     const float inv_nv = (float)(1.0 / (double)g.nv);
+    const int kexp = ring_exponent(st[b].ring_max, eps_bar + 6 * b);
+    const float rscale = ldexpf(1.f, kexp);
+    if (blockIdx.x == 0 && tid == 0) st[b].ring_exp[slot] = kexp;
     for (int idx = tid; idx < L * NZ; idx += nt) {
       const int l = idx / NZ, n = idx % NZ;
       const size_t vx = (size_t)(l0 + l) * NZ + n;
@@ -815,7 +818,7 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
         const size_t o = (size_t)c * g.nv + vx;
-        rb[slot * ring + o] = r[c];
+        rb[slot * ring + o] = ring_store(r[c], rscale);
         gb[slot * ring + o] = est[c * L * NZ + idx] + r[c];
       }
     }
@@ -1096,12 +1099,17 @@ __global__ void __launch_bounds__(slab_threads<NZ>(), 1) slab_fast(
   const float* lam = lambda + (size_t)(b / g.lame_group) * nv;
   const float* muf = mu + (size_t)(b / g.lame_group) * nv;
   int slot = 0;
-  float *rb = nullptr, *gb = nullptr;
+  __half* rb = nullptr;
+  float* gb = nullptr;
+  float rscale = 1.f;
   if constexpr (MODE == 3) {
     const int M1 = aa.depth + 1;
     slot = (st[b].iter - 1 - st[b].aa_base) % M1;
     rb = aa.r + (size_t)b * M1 * 6 * nv + (size_t)slot * 6 * nv;
     gb = aa.g + (size_t)b * M1 * 6 * nv + (size_t)slot * 6 * nv;
+    const int kexp = ring_exponent(st[b].ring_max, eps_bar + 6 * b);
+    rscale = ldexpf(1.f, kexp);
+    if (rank == 0 && x == 0 && tid == 0) st[b].ring_exp[slot] = kexp;
   }
   // owner rank and local column of half-spectrum column k
   auto owner = [&](int k) { return k < NF * kTW ? k / kTW : CS - 1; };
@@ -1135,8 +1143,8 @@ __global__ void __launch_bounds__(slab_threads<NZ>(), 1) slab_fast(
           const float2 w = zbuf[(size_t)(pr * R + l) * LD + n];
           const float r0 = w.x * inv_nv, r1 = -w.y * inv_nv;
           const size_t o0 = (size_t)(2 * pr) * nv + vx, o1 = (size_t)(2 * pr + 1) * nv + vx;
-          rb[o0] = r0;
-          rb[o1] = r1;
+          rb[o0] = ring_store(r0, rscale);
+          rb[o1] = ring_store(r1, rscale);
           gb[o0] = eb[o0] + r0;
           gb[o1] = eb[o1] + r1;
         }

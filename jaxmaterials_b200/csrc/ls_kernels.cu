@@ -122,9 +122,15 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
     anderson_slots<T>(st[b], aa.depth, slot, filled);
     const int M1 = aa.depth + 1;
     const size_t ring = (size_t)6 * g.nv;   // one slot
-    T* rb = aa.r + (size_t)b * M1 * ring;
+    typename ResRing<T>::type* rb = aa.r + (size_t)b * M1 * ring;
     T* gb = aa.g + (size_t)b * M1 * ring;
     const T inv_nv = (T)(1.0 / (double)g.nv);
+    float rscale = 1.f;  // FP16 residual ring: the slot's power-of-two scale
+    if constexpr (sizeof(T) == 4) {
+      const int k = ring_exponent(st[b].ring_max, eps_bar + 6 * b);
+      rscale = ldexpf(1.f, k);
+      if (blockIdx.x == 0 && tid == 0) st[b].ring_exp[slot] = k;
+    }
     for (int idx = tid; idx < L * nz; idx += nt) {
       int l = idx / nz, n = idx - l * nz;
       long long line = l0 + l;
@@ -140,7 +146,10 @@ __global__ void __launch_bounds__(kMaxThreads) zpass_kernel(GridDesc g, int mode
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
         const size_t o = (size_t)c * g.nv + v;
-        rb[slot * ring + o] = r[c];
+        if constexpr (sizeof(T) == 4)
+          rb[slot * ring + o] = ring_store(r[c], rscale);
+        else
+          rb[slot * ring + o] = r[c];
         gb[slot * ring + o] = eb[o] + r[c];
       }
     }
@@ -534,64 +543,120 @@ __device__ __forceinline__ float lane_of(const float4& v, int k) {
 
 // Gram-row partials of the newest residual r_j (slot j of the ring) for every instance in
 // `phase`: partials[b][blk][q] = sum over block blk's ring elements (component c, voxel) of
-// w_c r_j r_q, with Voigt weights w = (1,1,1,2,2,2), accumulated in FP64 (FP32 rings: four
-// neighbouring products summed in FP32 first) (lippmann_schwinger.py:217-231).
+// w_c r_j r_q, with Voigt weights w = (1,1,1,2,2,2), accumulated in FP64
+// (lippmann_schwinger.py:217-231); partials[b][blk][M1] = the block's max |r_j|.
+// FP32 phase: the ring holds FP16 values r_q 2^k_q; eight neighbouring weighted products are
+// summed in FP32, the sum added in FP64 (the kernel is bound by its FP64 issue rate
+// otherwise), and the block's sums are scaled back by 2^-(k_j + k_q) (exact). The rounding
+// of the stored residuals is independent from element to element, so it averages out of
+// the sums: relative to the FP32 ring the Gram entries change by about 2^-11 / sqrt(n).
 // A streaming kernel of its own, walking the 6 nv elements of a slot as the combine does, VW
-// elements per load, every slot of an element requested before the first product (M1 =
-// depth + 1 slots, a template constant).
+// elements per load (16 bytes of FP16 for VW = 8), every slot of an element requested
+// before the first product (M1 = depth + 1 slots, a template constant).
+__device__ __forceinline__ void unpack8(const uint4& u, float* f) {
+  const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 t = __half22float2(*reinterpret_cast<const __half2*>(&w[k]));
+    f[2 * k] = t.x;
+    f[2 * k + 1] = t.y;
+  }
+}
+
 template <typename T, int M1, int VW>
 __global__ void __launch_bounds__(256) anderson_gram_kernel(long long nv, int phase,
                                                             const InstanceState* __restrict__ st,
-                                                            const T* __restrict__ r,
+                                                            const typename ResRing<T>::type* __restrict__ r,
                                                             double* __restrict__ partials) {
-  using V = typename RingVec<T, VW>::type;
+  using R = typename ResRing<T>::type;
   __shared__ double red[kMaxDepth + 1][32];
+  __shared__ float redm[32];
   const int b = blockIdx.y;
   const InstanceState& s = st[b];
   if (s.done || s.phase != phase) return;
   int slot, filled;
   anderson_slots<T>(s, M1 - 1, slot, filled);
-  const long long n6 = 6 * nv, nvec = n6 / VW;
-  const T* rb = r + (size_t)b * M1 * n6;
+  const long long n6 = 6 * nv, nvec = n6 / VW, n3 = 3 * nv;
+  const R* rb = r + (size_t)b * M1 * n6;
   double dots[M1];
 #pragma unroll
   for (int q = 0; q < M1; ++q) dots[q] = 0.0;
+  float amax = 0.f;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvec;
        i += (long long)gridDim.x * blockDim.x) {
-    V rq[M1];
-#pragma unroll
-    for (int q = 0; q < M1; ++q)
-      if (q < filled) rq[q] = reinterpret_cast<const V*>(rb + (size_t)q * n6)[i];
-    V x = rq[0];
-#pragma unroll
-    for (int q = 1; q < M1; ++q) x = q == slot ? rq[q] : x;
-    if constexpr (VW == 4 && sizeof(T) == 4) {
-      // the group's four weighted products summed in FP32, the sum added in FP64 (the
-      // kernel is bound by its FP64 issue rate otherwise)
-      const long long e0 = i * 4;
-      const float4 wx = make_float4((e0 < 3 * nv ? 1.f : 2.f) * x.x, (e0 + 1 < 3 * nv ? 1.f : 2.f) * x.y,
-                                    (e0 + 2 < 3 * nv ? 1.f : 2.f) * x.z, (e0 + 3 < 3 * nv ? 1.f : 2.f) * x.w);
+    if constexpr (sizeof(T) == 4 && VW == 8) {
+      uint4 rq[M1];
 #pragma unroll
       for (int q = 0; q < M1; ++q)
-        if (q < filled)
-          dots[q] += (double)(wx.x * rq[q].x + wx.y * rq[q].y + wx.z * rq[q].z + wx.w * rq[q].w);
-    } else {
+        if (q < filled) rq[q] = reinterpret_cast<const uint4*>(rb + (size_t)q * n6)[i];
+      uint4 xu = rq[0];
 #pragma unroll
-      for (int k = 0; k < VW; ++k) {
-        const double wx = (i * VW + k < 3 * nv ? 1.0 : 2.0) * (double)lane_of(x, k);
+      for (int q = 1; q < M1; ++q) xu = q == slot ? rq[q] : xu;
+      float wx[8];
+      unpack8(xu, wx);
+      const long long e0 = i * 8;
 #pragma unroll
-        for (int q = 0; q < M1; ++q)
-          if (q < filled) dots[q] += wx * (double)lane_of(rq[q], k);
+      for (int k = 0; k < 8; ++k) {
+        amax = fmaxf(amax, fabsf(wx[k]));
+        if (e0 + k >= n3) wx[k] *= 2.f;
       }
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) {
+          float f[8];
+          unpack8(rq[q], f);
+          float sum = 0.f;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) sum = fmaf(wx[k], f[k], sum);
+          dots[q] += (double)sum;
+        }
+    } else if constexpr (sizeof(T) == 4) {
+      float rq[M1];
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) rq[q] = __half2float(rb[(size_t)q * n6 + i]);
+      float x = rq[0];
+#pragma unroll
+      for (int q = 1; q < M1; ++q) x = q == slot ? rq[q] : x;
+      amax = fmaxf(amax, fabsf(x));
+      const float wx = (i < n3 ? 1.f : 2.f) * x;
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) dots[q] += (double)(wx * rq[q]);
+    } else {
+      T rq[M1];
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) rq[q] = rb[(size_t)q * n6 + i];
+      T x = rq[0];
+#pragma unroll
+      for (int q = 1; q < M1; ++q) x = q == slot ? rq[q] : x;
+      const double wx = (i < n3 ? 1.0 : 2.0) * (double)x;
+#pragma unroll
+      for (int q = 0; q < M1; ++q)
+        if (q < filled) dots[q] += wx * (double)rq[q];
     }
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0) redm[threadIdx.x >> 5] = amax;
   double pad[kMaxDepth + 1];
 #pragma unroll
   for (int q = 0; q <= kMaxDepth; ++q) pad[q] = q < M1 ? dots[q < M1 ? q : 0] : 0.0;
   double out[kMaxDepth + 1];
-  block_sum_slots(pad, filled, red, out);
-  if ((int)threadIdx.x < filled)
-    partials[((size_t)b * gridDim.x + blockIdx.x) * M1 + threadIdx.x] = out[threadIdx.x];
+  block_sum_slots(pad, filled, red, out);  // (its barrier also orders redm)
+  double* pb = partials + ((size_t)b * gridDim.x + blockIdx.x) * (M1 + 1);
+  const int t = threadIdx.x;
+  if (t < filled) {
+    double v = out[t];
+    if constexpr (sizeof(T) == 4) v = ldexp(v, -(s.ring_exp[slot] + s.ring_exp[t]));
+    pb[t] = v;
+  }
+  if (t == 0) {
+    float m = 0.f;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) m = fmaxf(m, redm[w]);
+    pb[M1] = sizeof(T) == 4 ? ldexp((double)m, -s.ring_exp[slot]) : 0.0;
+  }
 }
 
 // Anderson combine for every instance in `phase`: eps = sum_s alpha_s g_s over the filled
@@ -659,21 +724,22 @@ __global__ void __launch_bounds__(256) anderson_combine_kernel(long long n6, int
 // relabelling of the ring), A v = 1 is solved over the filled slots in FP64 by Gaussian
 // elimination with partial pivoting, alpha = v / sum(v). A singular or non-finite solve
 // falls back to the plain update alpha = e_slot.
-// The Gram row's block partials (nzblk rows of M1 values) are summed by the whole block,
-// each thread over a few rows with independent loads, then across warps; A is staged in
-// shared memory. The elimination runs on one thread over an M1 x M1 system held in
+// The Gram row's block partials (nzblk rows of M1 values and the block's max |r_j|) are
+// summed by the whole block, each thread over a few rows with independent loads, then
+// across warps; the max of the newest residual goes to the instance state, for the scale of
+// the next FP16 slot. A is staged in shared memory. The elimination runs on one thread over an M1 x M1 system held in
 // registers (compile-time M1): rows and columns past `filled` are an identity block with a
 // zero right-hand side, which leaves the filled block's arithmetic, pivots and solution
 // as they are and gives v = 0 on the padding.
 constexpr int kSolveThreads = 256;
 template <int M1>
 __global__ void __launch_bounds__(kSolveThreads) anderson_solve_kernel(
-    int nzblk, int phase, const InstanceState* __restrict__ st,
+    int nzblk, int phase, InstanceState* __restrict__ st,
     const double* __restrict__ partials, double* __restrict__ amat, double* __restrict__ alpha) {
-  __shared__ double red[kSolveThreads / 32][M1];
+  __shared__ double red[kSolveThreads / 32][M1 + 1];
   __shared__ double sA[M1 * M1];
   const int b = blockIdx.x;
-  const InstanceState& s = st[b];
+  InstanceState& s = st[b];
   if (s.done || s.phase != phase) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int slot, filled;
@@ -683,12 +749,14 @@ __global__ void __launch_bounds__(kSolveThreads) anderson_solve_kernel(
   double a[M1];
 #pragma unroll
   for (int q = 0; q < M1; ++q) a[q] = 0.0;
-  const double* pb = partials + (size_t)b * nzblk * M1;
+  double mx = 0.0;
+  const double* pb = partials + (size_t)b * nzblk * (M1 + 1);
 #pragma unroll 4
   for (int i = tid; i < nzblk; i += kSolveThreads) {
 #pragma unroll
     for (int q = 0; q < M1; ++q)
-      if (q < filled) a[q] += pb[(size_t)i * M1 + q];
+      if (q < filled) a[q] += pb[(size_t)i * (M1 + 1) + q];
+    mx = fmax(mx, pb[(size_t)i * (M1 + 1) + M1]);
   }
 #pragma unroll
   for (int q = 0; q < M1; ++q) {
@@ -697,7 +765,15 @@ __global__ void __launch_bounds__(kSolveThreads) anderson_solve_kernel(
     for (int o = 16; o > 0; o >>= 1) a[q] += __shfl_xor_sync(0xffffffffu, a[q], o);
     if (lane == 0) red[warp][q] = a[q];
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) red[warp][M1] = mx;
   __syncthreads();
+  if (tid == M1) {
+    double m = 0.0;
+    for (int w = 0; w < kSolveThreads / 32; ++w) m = fmax(m, red[w][M1]);
+    if (phase == 0) s.ring_max = (float)m;
+  }
   if (tid < filled) {
     double t = 0.0;
     for (int w = 0; w < kSolveThreads / 32; ++w) t += red[w][tid];
@@ -1042,7 +1118,7 @@ void launch_zpass(const GridDesc& g, const LaunchShape& s, int mode, int batch, 
       g, mode, s.lines_per_block, lambda, mu, eps, spec, eps_bar, eps0, st, med, aa);
 }
 
-void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
+void launch_anderson_solve(int nzblk, int depth, int phase, int batch, InstanceState* st,
                            const double* partials, double* amat, double* alpha, cudaStream_t stream) {
   switch (depth + 1) {
 #define LSB_SOLVE(M)                                                                          \
@@ -1058,15 +1134,16 @@ void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const Ins
 
 template <typename T>
 void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batch,
-                          const InstanceState* st, const T* r, double* partials, cudaStream_t stream) {
+                          const InstanceState* st, const typename ResRing<T>::type* r,
+                          double* partials, cudaStream_t stream) {
   const dim3 grid(nblk, batch);
-  const bool vec = sizeof(T) == 4 && (6 * nv) % 4 == 0;
+  const bool vec = sizeof(T) == 4 && (6 * nv) % 8 == 0;
   switch (depth + 1) {
 #define LSB_GRAM(M)                                                                              \
     case M:                                                                                      \
       if constexpr (sizeof(T) == 4) {                                                            \
         if (vec) {                                                                               \
-          anderson_gram_kernel<T, M, 4><<<grid, 256, 0, stream>>>(nv, phase, st, r, partials); \
+          anderson_gram_kernel<T, M, 8><<<grid, 256, 0, stream>>>(nv, phase, st, r, partials); \
           break;                                                                                 \
         }                                                                                        \
       }                                                                                          \
@@ -1175,7 +1252,7 @@ void launch_stress(const GridDesc& g, int phase, int batch, const InstanceState*
                                 const Medium*, InstanceState*, double*, cudaStream_t);          \
   template void launch_medium<T>(long long, int, const T*, const T*, double*, Medium*, cudaStream_t); \
   template void launch_anderson_gram<T>(long long, int, int, int, int, const InstanceState*,    \
-                                        const T*, double*, cudaStream_t);                       \
+                                        const typename ResRing<T>::type*, double*, cudaStream_t); \
   template void launch_anderson_combine<T>(long long, int, int, int, const InstanceState*,      \
                                            const T*, const double*, T*, cudaStream_t, const T*);
 LSB_INST(float)

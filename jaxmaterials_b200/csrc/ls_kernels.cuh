@@ -34,19 +34,22 @@ template <typename T>
 void launch_zpass(const GridDesc& g, const LaunchShape& ls, int mode, int batch, const T* lambda,
                   const T* mu, T* eps, cplx<T>* spec, const double* eps_bar, const T* eps0,
                   InstanceState* st, const Medium* med, const AndersonArgs<T>& aa, cudaStream_t s);
-// Gram-row partials [batch][nblk][depth+1] of the newest residual of every instance in
-// `phase` (r: the residual ring [batch][depth+1][6][nv]).
+// Gram-row partials [batch][nblk][depth+2] of the newest residual of every instance in
+// `phase` (depth+1 products and the block's max |r|; r: the residual ring
+// [batch][depth+1][6][nv], FP16 with per-slot scales in the FP32 phase).
 template <typename T>
 void launch_anderson_gram(long long nv, int nblk, int depth, int phase, int batch,
-                          const InstanceState* st, const T* r, double* partials, cudaStream_t s);
+                          const InstanceState* st, const typename ResRing<T>::type* r,
+                          double* partials, cudaStream_t s);
 // eps = sum_s alpha_s g_s for every instance in `phase` (g: [batch][depth+1][6][nv]);
 // with `inject` ([batch][6][nv]) the first update of a solve sets eps = inject instead.
 template <typename T>
 void launch_anderson_combine(long long nv, int depth, int phase, int batch, const InstanceState* st,
                              const T* g, const double* alpha, T* eps, cudaStream_t s,
                              const T* inject = nullptr);
-// Anderson coefficients of every instance in `phase` from the Gram-row partials.
-void launch_anderson_solve(int nzblk, int depth, int phase, int batch, const InstanceState* st,
+// Anderson coefficients of every instance in `phase` from the Gram-row partials (and, in
+// the FP32 phase, the newest residual's max |r| into the instance state).
+void launch_anderson_solve(int nzblk, int depth, int phase, int batch, InstanceState* st,
                            const double* partials, double* amat, double* alpha, cudaStream_t s);
 template <typename T>
 void launch_ypass(const GridDesc& g, const LaunchShape& ls, bool inverse, int batch, cplx<T>* spec,

@@ -330,8 +330,8 @@ int create_impl(lsb_solver** out, const int voxels[3], const double extents[3], 
     s->aa_zblocks = std::max(std::max(s->sh32.z_blocks, s->sh64.z_blocks),
                              s->fast32 ? fast::z_blocks(g) : 0);
     ok = alloc((void**)&s->d_aa_g32, sizeof(float) * B * M1 * 6 * g.nv) &&
-         alloc((void**)&s->d_aa_r32, sizeof(float) * B * M1 * 6 * g.nv) &&
-         alloc((void**)&s->d_aa_partials, sizeof(double) * B * s->aa_zblocks * M1) &&
+         alloc((void**)&s->d_aa_r32, sizeof(__half) * B * M1 * 6 * g.nv) &&
+         alloc((void**)&s->d_aa_partials, sizeof(double) * B * s->aa_zblocks * (M1 + 1)) &&
          alloc((void**)&s->d_aa_mat, sizeof(double) * B * M1 * M1) &&
          alloc((void**)&s->d_aa_alpha, sizeof(double) * B * M1);
     if (!ok) {

@@ -54,10 +54,10 @@ struct lsb_solver {
   int lame64_structs = 0;        // structures d_lame64 holds
   // Anderson acceleration (depth > 0): rings of g = eps + r and r, Gram matrices, coefficients
   float* d_aa_g32 = nullptr;     // [batch][m+1][6][nv]
-  float* d_aa_r32 = nullptr;
+  __half* d_aa_r32 = nullptr;    // FP16, per-slot power-of-two scales (InstanceState)
   double* d_aa_g64 = nullptr;    // FP64 rings, allocated for FP64 runs
   double* d_aa_r64 = nullptr;
-  double* d_aa_partials = nullptr;  // [batch][z blocks][m+1]
+  double* d_aa_partials = nullptr;  // [batch][z blocks][m+2]: Gram-row sums, block max abs r
   double* d_aa_mat = nullptr;    // [batch][m+1][m+1]
   double* d_aa_alpha = nullptr;  // [batch][m+1]
   int aa_zblocks = 0;

@@ -11,6 +11,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace lsb {
@@ -147,11 +148,25 @@ struct InstanceState {
   // zero frequency at the level of the stress fluctuation; the zero mode is restored in
   // FP64 (sig0), and Gamma^0 and xi vanish there, so nothing else depends on it.
   double shift[6];
+  // FP32 phase, Anderson residual ring in FP16: slot q holds r_q * 2^ring_exp[q]; ring_max
+  // is max |r| of the newest residual (from the Gram row), from which the next slot's
+  // exponent is chosen.
+  float ring_max;
+  int ring_exp[9];
 };
 
 enum Precision : int { kPrecFP32 = 0, kPrecMixed = 1, kPrecFP64 = 2 };
 
 constexpr int kMaxDepth = 8;  // largest Anderson depth m (ring of m+1 slots)
+static_assert(sizeof(InstanceState::ring_exp) / sizeof(int) == kMaxDepth + 1, "one exponent per slot");
+
+// Element type of the residual ring: the residuals enter only the Gram row (the mixing
+// coefficients), never the iterate, so the FP32 phase stores them in FP16, scaled per slot
+// by a power of two; the FP64 phase keeps doubles.
+template <typename T>
+struct ResRing { using type = T; };
+template <>
+struct ResRing<float> { using type = __half; };
 
 // Anderson acceleration state of one batch (lippmann_schwinger.py:217-231). For update j
 // of an instance (j = iter - 1 - aa_base), slot j mod (m+1) of the rings receives
@@ -159,12 +174,34 @@ constexpr int kMaxDepth = 8;  // largest Anderson depth m (ring of m+1 slots)
 // iterate is eps = sum_s alpha_s g_s over the filled slots.
 template <typename T>
 struct AndersonArgs {
-  int depth;             // m (0: plain iteration)
-  T* g;                  // [batch][m+1][6][nv]
-  T* r;                  // [batch][m+1][6][nv]
-  double* partials;      // [batch][z blocks][m+1] Gram-row partials
-  const double* alpha;   // [batch][m+1] mixing coefficients of the current update
+  int depth;                        // m (0: plain iteration)
+  T* g;                             // [batch][m+1][6][nv]
+  typename ResRing<T>::type* r;     // [batch][m+1][6][nv]
+  double* partials;                 // [batch][z blocks][m+1] Gram-row partials
+  const double* alpha;              // [batch][m+1] mixing coefficients of the current update
 };
+
+// Scale exponent of the FP16 residual slot written by the current update: the newest
+// residual's max |r| (or, for the first slot of a history, 8 max |eps_bar|) is mapped below
+// 2^10, so a residual may grow 64-fold between updates before FP16's 65504 is reached, and
+// elements down to 2^-24 of that max keep full FP16 precision.
+__host__ __device__ __forceinline__ int ring_exponent(float ring_max, const double* eps_bar6) {
+  float m = ring_max;
+  if (!(m > 0.f) || !(m < 3.0e38f)) {
+    double e = 0.0;
+    for (int c = 0; c < 6; ++c) e = fmax(e, fabs(eps_bar6[c]));
+    m = (float)(8.0 * (e > 0.0 && e < 1e30 ? e : 1.0));
+  }
+  int ex;
+  frexpf(m, &ex);  // m < 2^ex
+  int k = 10 - ex;
+  return k < -60 ? -60 : (k > 60 ? 60 : k);
+}
+
+// r * 2^k rounded to FP16, saturated at +-65504 (k in [-60, 60]).
+__device__ __forceinline__ __half ring_store(float r, float scale) {
+  return __float2half_rn(fminf(fmaxf(r * scale, -65504.f), 65504.f));
+}
 
 struct SolveParams {
   double rtol, atol;
