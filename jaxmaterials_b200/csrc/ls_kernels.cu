@@ -564,7 +564,7 @@ __device__ __forceinline__ void unpack8(const uint4& u, float* f) {
 }
 
 template <typename T, int M1, int VW>
-__global__ void __launch_bounds__(256) anderson_gram_kernel(long long nv, int phase,
+__global__ void __launch_bounds__(256, M1 <= 6 ? 4 : 3) anderson_gram_kernel(long long nv, int phase,
                                                             const InstanceState* __restrict__ st,
                                                             const typename ResRing<T>::type* __restrict__ r,
                                                             double* __restrict__ partials) {
