@@ -2,14 +2,17 @@
 // unit load cases each -- the dataset loop of src/jaxmaterials/data/data.py:178-186 run
 // as batched solves on one GPU.
 //
-// Schedule. Structures are grouped into buckets of equal grid (voxels and extents). Each
-// bucket runs on its own host thread and CUDA stream, so the small-grid buckets fill the
-// GPU while a large-grid bucket's thread polls its convergence state. Inside a bucket
-// one solver holds `chunk` structures x 6 load cases; instance b reads the Lame fields
-// of structure b / 6 and its own reference medium, and retires at its own convergence
-// (kernels skip retired instances). The chunk is the largest that fits the bucket's share
-// of the memory budget (share proportional to the bucket's voxels); the chunks of a
-// bucket are evened out so that the last one is not a small remainder.
+// Schedule. Structures are grouped into buckets of equal grid (voxels and extents). Inside
+// a bucket one solver holds `chunk` structures x 6 load cases; instance b reads the Lame
+// fields of structure b / 6 and its own reference medium, and retires at its own
+// convergence (kernels skip retired instances). The chunk is the largest that fits the
+// bucket's share of the memory budget (share proportional to the bucket's voxels); the
+// chunks of a bucket are evened out so that the last one is not a small remainder.
+// Default: the whole dataset is ONE CUDA graph launch (run_dataset_graph): each bucket a
+// chain of its chunks' solves, whose iteration loops are conditional WHILE nodes stopped on
+// the device, the buckets independent branches with priorities by grid size; the host
+// waits once. Fallback (and LSB_BATCH_GRAPH=0): each bucket on its own host thread and
+// stream, one graph launch per chunk and phase.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -17,6 +20,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -147,6 +151,237 @@ void run_bucket(const Bucket& bk, int device, size_t budget, int depth, int prec
   cudaStreamDestroy(st);
 }
 
+// ---- one graph for the whole dataset
+//
+// Every bucket gets its solver at once (chunk sized to the bucket's share of the budget,
+// as above) and its structures' Lame fields are copied to the device up front; the solves
+// of all chunks are then appended to ONE CUDA graph -- each bucket a chain of its chunks'
+// solves (append_solve_f32: device-opened and device-stopped WHILE loops over the
+// iterations, FP32 then the FP64 continuation), the buckets independent branches whose
+// kernel nodes carry the bucket's priority (smallest grid highest) -- which is
+// instantiated and launched once. The host waits once, for the whole dataset. Returns
+// kNoGraph (and leaves nothing behind) when this schedule does not apply: a bucket whose
+// share cannot hold one structure, the Lame fields above a third of the budget, or a graph
+// call that failed; the caller then runs the threaded schedule.
+constexpr int kNoGraph = 1;
+
+struct GraphBucket {
+  lsb_solver* s = nullptr;
+  cudaStream_t st = nullptr;
+  float* d_lame = nullptr;  // [2][members][nv]: lambda of every member, then mu
+  int chunk = 0;
+  double* h_mean = nullptr;          // [6 members][6] in the pinned result buffer
+  InstanceState* h_state = nullptr;  // [6 members]
+};
+
+void set_priority(cudaGraph_t g, int prio) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return;
+  cudaLaunchAttributeValue v = {};
+  v.priority = prio;
+  for (cudaGraphNode_t nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+      cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributePriority, &v);
+  }
+}
+
+int run_dataset_graph(const std::vector<Bucket>& buckets, int device, size_t budget, int depth,
+                      int precision, double rtol, double atol, int maxiter,
+                      const float* const* lambda, const float* const* mu,
+                      const std::vector<int>& priority, double* c_eff, int* iters, int* status,
+                      bool trace) {
+  double total = 0.0, lame_bytes = 0.0;
+  for (const Bucket& b : buckets) {
+    total += b.voxels_total;
+    lame_bytes += 8.0 * b.voxels_total;
+  }
+  if (lame_bytes > (double)budget / 3.0) return kNoGraph;
+  const size_t rest = budget - (size_t)lame_bytes;
+  std::vector<GraphBucket> gb(buckets.size());
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap = nullptr, body = nullptr, run = nullptr;
+  unsigned char* h_res = nullptr;  // pinned: every structure's means and states
+  int rc = 0;
+  std::vector<std::pair<const char*, double>> times;  // (step, seconds) for the trace
+  auto tick = [&](const char* what) {
+    static thread_local auto last = std::chrono::steady_clock::now();
+    const auto now = std::chrono::steady_clock::now();
+    if (what) times.emplace_back(what, std::chrono::duration<double>(now - last).count());
+    last = now;
+  };
+  tick(nullptr);
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    tick("graph release");
+    for (GraphBucket& b : gb) {
+      cudaFree(b.d_lame);
+      if (b.s) lsb_destroy(b.s);
+      if (b.st) cudaStreamDestroy(b.st);
+    }
+    tick("solvers release");
+    if (h_res) cudaFreeHost(h_res);
+    if (cap) cudaStreamDestroy(cap);
+    if (body) cudaStreamDestroy(body);
+    if (run) cudaStreamDestroy(run);
+    cudaGetLastError();
+  };
+  size_t nmembers = 0;
+  for (const Bucket& b : buckets) nmembers += b.members.size();
+  if (cudaMallocHost(&h_res, (sizeof(double) * 36 + sizeof(InstanceState) * 6) * nmembers) != cudaSuccess) {
+    cudaGetLastError();
+    return kNoGraph;
+  }
+  {
+    size_t off = 0;
+    for (size_t k = 0; k < buckets.size(); ++k) {
+      gb[k].h_mean = reinterpret_cast<double*>(h_res) + 36 * off;
+      off += buckets[k].members.size();
+    }
+    off = 0;
+    InstanceState* hs = reinterpret_cast<InstanceState*>(h_res + sizeof(double) * 36 * nmembers);
+    for (size_t k = 0; k < buckets.size(); ++k) {
+      gb[k].h_state = hs + 6 * off;
+      off += buckets[k].members.size();
+    }
+  }
+  // solvers, Lame fields on the device and tuned passes, one host thread per bucket (the
+  // buckets' uploads from pageable memory and allocations proceed in parallel)
+  for (size_t k = 0; k < buckets.size(); ++k) {
+    const Bucket& bk = buckets[k];
+    const size_t per = bytes_per_structure(bk.voxels, depth, precision, maxiter);
+    const size_t share = (size_t)((double)rest * bk.voxels_total / total);
+    if (share < per) {
+      cleanup();
+      return kNoGraph;
+    }
+    const int n = (int)bk.members.size();
+    const int chunk = (int)std::min<size_t>(share / per, (size_t)n);
+    const int nchunks = (n + chunk - 1) / chunk;
+    gb[k].chunk = (n + nchunks - 1) / nchunks;
+  }
+  std::vector<int> setup_rc(buckets.size(), 0);
+  std::vector<std::string> setup_err(buckets.size());
+  auto set_up = [&](size_t k) {
+    cudaSetDevice(device);
+    const Bucket& bk = buckets[k];
+    GraphBucket& b = gb[k];
+    const long long nv = (long long)bk.voxels[0] * bk.voxels[1] * bk.voxels[2];
+    const int n = (int)bk.members.size();
+    if (cudaStreamCreateWithPriority(&b.st, cudaStreamNonBlocking, priority[k]) != cudaSuccess ||
+        cudaMalloc(&b.d_lame, sizeof(float) * 2 * (size_t)n * nv) != cudaSuccess) {
+      cudaGetLastError();
+      setup_rc[k] = kNoGraph;
+      return;
+    }
+    for (int j = 0; j < n; ++j) {
+      const int m = bk.members[j];
+      cudaMemcpyAsync(b.d_lame + (size_t)j * nv, lambda[m], sizeof(float) * nv, cudaMemcpyHostToDevice, b.st);
+      cudaMemcpyAsync(b.d_lame + (size_t)(n + j) * nv, mu[m], sizeof(float) * nv, cudaMemcpyHostToDevice, b.st);
+    }
+    int r = lsb_create(&b.s, bk.voxels, bk.extents, 6 * b.chunk, depth);
+    if (r == 0) {
+      b.s->stream = b.st;
+      b.s->precision = precision;
+      b.s->lame_group = 6;
+      r = prepare_graph_solve(b.s, 6 * b.chunk, b.d_lame, b.d_lame + (size_t)n * nv, maxiter);
+    }
+    if (r) {
+      setup_rc[k] = r;
+      setup_err[k] = lsb_last_error();
+    }
+  };
+  {
+    std::vector<std::thread> th;
+    for (size_t k = 0; k < buckets.size(); ++k) th.emplace_back(set_up, k);
+    for (auto& t : th) t.join();
+  }
+  for (size_t k = 0; k < buckets.size() && rc == 0; ++k)
+    if (setup_rc[k]) {
+      rc = setup_rc[k] == kNoGraph ? kNoGraph
+                                   : fail(setup_rc[k], "bucket %dx%dx%d: %s", buckets[k].voxels[0],
+                                          buckets[k].voxels[1], buckets[k].voxels[2], setup_err[k].c_str());
+    }
+  tick("solvers, fields, tuning");
+  if (rc == 0 &&
+      (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaStreamCreateWithFlags(&run, cudaStreamNonBlocking) != cudaSuccess || cudaGraphCreate(&graph, 0) != cudaSuccess))
+    rc = kNoGraph;
+  // one branch per bucket: its chunks' solves in sequence
+  std::set<cudaGraphNode_t> seen;  // root nodes of the buckets already appended
+  for (size_t k = 0; k < buckets.size() && rc == 0; ++k) {
+    const Bucket& bk = buckets[k];
+    GraphBucket& b = gb[k];
+    const long long nv = (long long)bk.voxels[0] * bk.voxels[1] * bk.voxels[2];
+    const int n = (int)bk.members.size();
+    std::vector<cudaGraphNode_t> deps, last;
+    std::vector<cudaGraph_t> bodies;
+    for (int c0 = 0; c0 < n && rc == 0; c0 += b.chunk) {
+      const int c = std::min(b.chunk, n - c0);
+      rc = append_solve_f32(b.s, graph, deps, cap, body, 6 * c, b.d_lame + (size_t)c0 * nv,
+                            b.d_lame + (size_t)(n + c0) * nv, rtol, atol, maxiter, b.h_mean + 36 * (size_t)c0,
+                            b.h_state + 6 * (size_t)c0, &last, &bodies);
+      deps = last;
+    }
+    if (rc) break;
+    // this bucket's kernel nodes (the ones added since the previous bucket, and the loop
+    // bodies) get its priority
+    size_t n_now = 0;
+    cudaGraphGetNodes(graph, nullptr, &n_now);
+    std::vector<cudaGraphNode_t> all(n_now);
+    cudaGraphGetNodes(graph, all.data(), &n_now);
+    cudaLaunchAttributeValue v = {};
+    v.priority = priority[k];
+    for (size_t i = 0; i < n_now; ++i) {
+      if (!seen.insert(all[i]).second) continue;
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(all[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+        cudaGraphKernelNodeSetAttribute(all[i], cudaLaunchAttributePriority, &v);
+    }
+    for (cudaGraph_t bg : bodies) set_priority(bg, priority[k]);
+  }
+  tick("graph build");
+  if (rc == 0 && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc = kNoGraph;
+  tick("instantiate");
+  if (rc == 0) {
+    cudaError_t e = cudaGraphLaunch(exec, run);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(run);
+    if (e != cudaSuccess) rc = fail(-2, "dataset graph: %s", cudaGetErrorString(e));
+  }
+  tick("run");
+  if (rc == 0) {
+    for (size_t k = 0; k < buckets.size(); ++k) {
+      const Bucket& bk = buckets[k];
+      const GraphBucket& b = gb[k];
+      for (size_t j = 0; j < bk.members.size(); ++j) {
+        const int m = bk.members[j];
+        std::memcpy(c_eff + 36 * (size_t)m, b.h_mean + 36 * j, sizeof(double) * 36);
+        for (int q = 0; q < 6; ++q) {
+          iters[6 * (size_t)m + q] = b.h_state[6 * j + q].iter;
+          status[6 * (size_t)m + q] = b.h_state[6 * j + q].status;
+        }
+      }
+    }
+  }
+  cleanup();
+  tick("release");
+  if (trace && rc == 0) {
+    std::fprintf(stderr, "lsb_c_eff_batch: one graph over %zu buckets:", buckets.size());
+    for (auto& t : times) std::fprintf(stderr, " %s %.3f s,", t.first, t.second);
+    std::fprintf(stderr, "\n");
+    for (size_t k = 0; k < buckets.size(); ++k)
+      std::fprintf(stderr, "  grid %dx%dx%d structures %zu chunk %d priority %d\n", buckets[k].voxels[0],
+                   buckets[k].voxels[1], buckets[k].voxels[2], buckets[k].members.size(), gb[k].chunk,
+                   priority[k]);
+  }
+  return rc;
+}
+
 }  // namespace
 
 extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* extents,
@@ -219,6 +454,16 @@ extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* ext
                            sorted_sizes.begin());
     return std::min(least, greatest + rank);
   };
+  // One graph for the whole dataset (LSB_BATCH_GRAPH=0: the threaded schedule below).
+  const char* gmode = std::getenv("LSB_BATCH_GRAPH");
+  if (!(gmode && gmode[0] == '0' && gmode[1] == 0)) {
+    std::vector<int> prio(buckets.size());
+    for (size_t b = 0; b < buckets.size(); ++b) prio[b] = priority_of(b);
+    const int grc = run_dataset_graph(buckets, device, budget, depth, precision, (double)rtol, (double)atol,
+                                      maxiter, lambda, mu, prio, c_eff, iters, status,
+                                      std::getenv("LSB_BATCH_TRACE") != nullptr);
+    if (grc != kNoGraph) return grc;
+  }
   // Buckets whose share of the budget holds at least one structure run concurrently, one
   // host thread each; the others run afterwards one at a time with the whole budget.
   std::vector<BucketResult> res(buckets.size());

@@ -436,6 +436,20 @@ void pass_x(lsb_solver* s, int batch, cplx<T>* spec) {
 // Runs the loop of precision T for every instance in its phase until none is left there.
 // init_mode: 0 (eps from eps_bar / eps0) or 2 (continue from eps in place).
 // With `anderson` the update is Anderson mixing of depth s->depth (rings of precision T).
+// Start of a phase's device-driven loop inside a larger graph: resets the evaluation count
+// and opens the loop only if an instance of `phase` is running (the loop's default is
+// closed). One warp.
+__global__ void loop_arm_kernel(cudaGraphConditionalHandle handle, const InstanceState* __restrict__ st,
+                                int batch, int phase, int* count) {
+  int any = 0;
+  for (int b = threadIdx.x; b < batch; b += 32) any |= (!st[b].done && st[b].phase == phase) ? 1 : 0;
+  any = __any_sync(0xffffffffu, any);
+  if (threadIdx.x == 0) {
+    *count = 0;
+    cudaGraphSetConditional(handle, any ? 1u : 0u);
+  }
+}
+
 // Moves a phase's work to the solver's graph stream (ordered after everything already on
 // the caller's stream) and back (the caller's stream waits for the phase); owns the graph.
 // End of one body execution of a phase's device-driven loop: counts the evaluations and
@@ -972,6 +986,142 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
     if (residual) residual[b] = s->h_state[b].e;
   }
   s->last_batch = batch;
+  return 0;
+}
+
+// Appends the device work of one FP32-start solve of `batch` instances (the sequence of
+// solve_f32: reset, media, initial pass, the FP32 loop, the FP64 continuation of stalled
+// instances, the means of the stresses) to `graph`, after the nodes in `deps`; both loops
+// are conditional WHILE nodes opened and stopped on the device. The mean stresses and the
+// instance states are copied into the pinned h_mean ([batch][6]) and h_state ([batch]) at
+// the end. *last receives the terminal nodes, *bodies (if given) the loops' body graphs.
+// The caller has prepared the solver
+// (prepare_graph_solve) and owns the two capture streams. Returns 0 or a negative code
+// (the graph is then unusable).
+int append_solve_f32(lsb_solver* s, cudaGraph_t graph, const std::vector<cudaGraphNode_t>& deps,
+                     cudaStream_t cap, cudaStream_t body_st, int batch, const float* d_lambda,
+                     const float* d_mu, double rtol, double atol, int maxiter, double* h_mean,
+                     InstanceState* h_state, std::vector<cudaGraphNode_t>* last,
+                     std::vector<cudaGraph_t>* bodies) {
+  const GridDesc& g = s->g;
+  const int nstruct = structures_of(s, batch);
+  if (nstruct < 0) return nstruct;
+  if (!s->d_loop_count) LSB_CUDA(cudaMalloc(&s->d_loop_count, sizeof(int)));
+  const SolveParams sp = make_params(s, rtol, atol, maxiter, LSB_RULE_CUDA);
+  const int max_evals = maxiter + 2;
+  cudaStream_t saved = s->stream;
+  s->stream = cap;
+  LSB_CUDA(cudaStreamBeginCaptureToGraph(cap, graph, deps.empty() ? nullptr : deps.data(), nullptr,
+                                         deps.size(), cudaStreamCaptureModeThreadLocal));
+  // one conditional WHILE node at the capture's current position, opened by
+  // loop_arm_kernel; its body (one iteration and loop_check_kernel) captured on body_st
+  auto add_loop = [&](auto iteration, int phase) -> bool {
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+    loop_arm_kernel<<<1, 32, 0, cap>>>(h, s->d_state, batch, phase, s->d_loop_count);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* cur = nullptr;
+    size_t ncur = 0;
+    if (cudaStreamGetCaptureInfo(cap, &cs, nullptr, nullptr, &cur, &ncur) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusActive)
+      return false;
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = h;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    std::vector<cudaGraphNode_t> cdeps(cur, cur + ncur);
+    if (cudaGraphAddNode(&node, graph, cdeps.data(), cdeps.size(), &params) != cudaSuccess) return false;
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    if (bodies) bodies->push_back(body);
+    if (cudaStreamBeginCaptureToGraph(body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+      return false;
+    s->stream = body_st;
+    iteration();
+    loop_check_kernel<<<1, 32, 0, body_st>>>(h, s->d_state, batch, phase, s->d_loop_count, max_evals);
+    s->stream = cap;
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(body_st, &captured) != cudaSuccess) return false;
+    return cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+  };
+  bool ok = true;
+  if (s->d_history) cudaMemsetAsync(s->d_history, 0, sizeof(double) * (size_t)batch * s->history_len, cap);
+  launch_reset_state(batch, 0, s->d_state, cap, nullptr);
+  launch_medium<float>(g.nv, nstruct, d_lambda, d_mu, s->d_scratch, s->d_medium, cap);
+  {
+    LaunchShape sh = s->sh32;
+    if (!use_fast32(s)) sh.x_blocks_per_instance = s->x_blocks_generic32;
+    const AndersonArgs<float> aa = anderson_args<float>(s, s->depth > 0);
+    float* eps = s->d_eps32;
+    if (use_slab(s)) {
+      pass_slab<float>(s, 0, batch, d_lambda, d_mu, eps, nullptr, aa);
+    } else {
+      pass_z<float>(s, 0, batch, d_lambda, d_mu, eps, s->d_spec32, nullptr, aa);
+      pass_y<float>(s, false, batch, s->d_spec32);
+    }
+    ok = add_loop([&]() { enqueue_iteration<float>(s, batch, d_lambda, d_mu, eps, s->d_spec32, aa, sp, sh, 0,
+                                                  nullptr, nullptr); }, 0);
+  }
+  if (ok && s->precision == kPrecMixed) {
+    // continuation of the instances that stalled in FP32 (every kernel below skips the
+    // others; with none, the FP64 loop does not open)
+    const long long n6 = 6 * g.nv;
+    const long long nl = (long long)nstruct * g.nv;
+    launch_convert<float, double>(nl, d_lambda, s->d_lame64, cap);
+    launch_convert<float, double>(nl, d_mu, s->d_lame64 + nl, cap);
+    launch_convert_fields<float, double>(n6, batch, 1, s->d_state, s->d_eps32, s->d_eps64, cap);
+    const double* lam64 = s->d_lame64;
+    const double* mu64 = s->d_lame64 + nl;
+    LaunchShape sh = s->sh64;
+    const AndersonArgs<double> aa = anderson_args<double>(s, false);
+    pass_z<double>(s, 2, batch, lam64, mu64, s->d_eps64, s->d_spec64, nullptr, aa);
+    pass_y<double>(s, false, batch, s->d_spec64);
+    ok = add_loop([&]() { enqueue_iteration<double>(s, batch, lam64, mu64, s->d_eps64, s->d_spec64, aa, sp,
+                                                   sh, 1, nullptr, nullptr); }, 1);
+    if (ok) {
+      launch_convert_fields<double, float>(n6, batch, 0, s->d_state, s->d_eps64, s->d_eps32, cap);
+      launch_stress<double, float>(g, 1, batch, s->d_state, lam64, mu64, s->d_eps64, nullptr,
+                                   s->d_mean_scratch, s->d_mean, cap);
+    }
+  }
+  if (ok) {
+    launch_stress<float, float>(g, 0, batch, s->d_state, d_lambda, d_mu, s->d_eps32, nullptr,
+                                s->d_mean_scratch, s->d_mean, cap);
+    cudaMemcpyAsync(h_mean, s->d_mean, sizeof(double) * 6 * batch, cudaMemcpyDeviceToHost, cap);
+    cudaMemcpyAsync(h_state, s->d_state, sizeof(InstanceState) * batch, cudaMemcpyDeviceToHost, cap);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* cur = nullptr;
+    size_t ncur = 0;
+    ok = cudaStreamGetCaptureInfo(cap, &cs, nullptr, nullptr, &cur, &ncur) == cudaSuccess &&
+         cs == cudaStreamCaptureStatusActive;
+    if (ok) last->assign(cur, cur + ncur);
+  }
+  cudaGraph_t captured = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(cap, &captured);
+  s->stream = saved;
+  if (!ok || e != cudaSuccess) {
+    const cudaError_t le = cudaGetLastError();
+    return fail(-2, "building the dataset graph failed (%s)",
+                cudaGetErrorString(e != cudaSuccess ? e : le));
+  }
+  return 0;
+}
+
+// Prepares a solver for append_solve_f32: unit loads (six per structure) in d_epsbar, the
+// criterion history, the FP64 buffers of the mixed-precision continuation, and the pass
+// configuration (autotuned on the fields at d_lambda / d_mu, the first structures').
+int prepare_graph_solve(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu, int maxiter) {
+  const int nstruct = structures_of(s, batch);
+  if (nstruct < 0) return nstruct;
+  LSB_TRY(ensure_history(s, maxiter + 8));
+  if (s->precision != kPrecFP32) LSB_TRY(ensure_fp64(s, nstruct));
+  std::vector<double> eb(6 * (size_t)batch, 0.0);
+  for (int b = 0; b < batch; ++b) eb[6 * b + b % 6] = 1.0;
+  LSB_CUDA(cudaMemcpy(s->d_epsbar, eb.data(), sizeof(double) * eb.size(), cudaMemcpyHostToDevice));
+  if (!s->xtuned) LSB_TRY(tune_passes(s, batch, d_lambda, d_mu, s->d_eps32, nstruct));
+  LSB_CUDA(cudaStreamSynchronize(s->stream));
   return 0;
 }
 

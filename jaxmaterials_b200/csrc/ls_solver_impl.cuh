@@ -152,5 +152,13 @@ int solve_f32(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu
               double* mean_sigma, double rtol, double atol, int maxiter, int rule, int* iters,
               int* status, double* residual);
 
+// Dataset graphs (batch.cu): see ls_solver.cu.
+int prepare_graph_solve(lsb_solver* s, int batch, const float* d_lambda, const float* d_mu, int maxiter);
+int append_solve_f32(lsb_solver* s, cudaGraph_t graph, const std::vector<cudaGraphNode_t>& deps,
+                     cudaStream_t cap, cudaStream_t body_st, int batch, const float* d_lambda,
+                     const float* d_mu, double rtol, double atol, int maxiter, double* h_mean,
+                     InstanceState* h_state, std::vector<cudaGraphNode_t>* last,
+                     std::vector<cudaGraph_t>* bodies);
+
 }  // namespace detail
 }  // namespace lsb

@@ -103,6 +103,28 @@ def test_c_eff_batch_memory_chunks():
     np.testing.assert_array_equal(full[1], tight[1])
 
 
+def test_c_eff_batch_graph_equals_threads(monkeypatch):
+    """The whole dataset as one CUDA graph (the default schedule: every bucket a chain of
+    its chunks' solves, each loop a device-stopped WHILE node) gives the threaded
+    schedule's C_eff, iterations and status bit for bit, also for instances continued in
+    FP64 after an FP32 stall (rtol 2e-7 lies below the FP32 floor at these sizes)."""
+    from jaxmaterials_b200.solver import c_eff_batch
+
+    structs = fibre_set([16, 32, 24, 16, 32, 48], seed=3)
+    lms, mus, gs = zip(*structs)
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("LSB_BATCH_GRAPH", mode)
+        for rtol in (1e-6, 2e-7):
+            out[mode, rtol] = c_eff_batch(lms, mus, list(gs), rtol=rtol, maxiter=3000, depth=5)
+    for rtol in (1e-6, 2e-7):
+        g, t = out["1", rtol], out["0", rtol]
+        np.testing.assert_array_equal(g[0], t[0])
+        np.testing.assert_array_equal(g[1], t[1])
+        np.testing.assert_array_equal(g[2], t[2])
+        assert (g[2] == 1).all()
+
+
 def test_c_eff_batch_rejects_bad_input():
     from jaxmaterials_b200 import GridSpec
     from jaxmaterials_b200._lib import LibraryError
