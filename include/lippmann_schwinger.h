@@ -226,7 +226,9 @@ int lsb_c_eff(const float *lambda, const float *mu, const int voxels[3],
  * voxels[3*i..3*i+2], extents[3*i..3*i+2] and host Lame fields lambda[i], mu[i]
  * (float[nv_i]); grids may differ between structures. Structures of equal grid run
  * together (instance b of a launch reads structure b / 6, each with its own reference
- * medium and its own convergence), different grids concurrently on separate streams.
+ * medium and its own convergence), different grids concurrently: the whole dataset is one
+ * CUDA graph launch (one branch per grid; environment LSB_BATCH_GRAPH=0, or a budget too
+ * small for it, selects one host thread and stream per grid instead; same results).
  * depth: Anderson depth; precision: LSB_PREC_*; memory_gb: device memory the call may
  * use (<= 0: 70% of the free memory). Outputs: c_eff host double[nstruct*36],
  * iters and status host int[nstruct*6]. */
