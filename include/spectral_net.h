@@ -20,7 +20,9 @@ extern "C" {
 
 /* y = act(W x + bias + add); pre (optional) receives the pre-activation.
  * act: 0 identity, 1 GELU (erf form). Channel pairs (cin, cout): (2,32), (32,32),
- * (32,36), (2,4), (4,4), (4,6). add and bias may be NULL. */
+ * (32,36), (2,4), (4,4), (4,6). add and bias may be NULL. The pairs with cin = 32 run on
+ * the tensor cores when nv is a multiple of 16 (x rounded to bf16 for the products, FP32
+ * accumulation); the others, and any nv, on FP32 FMA kernels. */
 int lsn_pointwise_forward(int batch, int cin, int cout, long long nv, const float *x,
                           const void *w_bf16, const float *bias, const float *add, float *pre,
                           float *y, int act, void *stream);
@@ -44,6 +46,21 @@ int lsn_spectral_forward(int batch, int cin, int cout, const int n[3], const int
 int lsn_spectral_backward(int batch, int cin, int cout, const int n[3], const int modes[3],
                           const void *xh, const void *w_bf16, const void *dyh, void *dxh,
                           float *dw, void *stream);
+
+/* Truncated transforms between `fields` real fields f [fields][nx][ny][nz] float and their
+ * retained modes X [fields][mx][my][mz] complex64 (the dense mode layout above, i.e.
+ * lsn_spectral_forward/backward with n = (mx, my, 2 (mz - 1))):
+ *   forward:  X[m] = scale w(kz) sum_v f[v] exp(-2 pi i k.v / n)
+ *   inverse:  f[v] = scale Re sum_m w(kz) X[m] exp(+2 pi i k.v / n)
+ * with w(kz) = w_int for 0 < kz < nz/2, else 1. forward(1, 1) is numpy's rfftn at the
+ * retained modes, inverse(1/(nx ny nz), 2) numpy's irfftn of the zero-padded half spectrum;
+ * as real-linear maps forward(1, 1) and inverse(1, 1) are each other's transposes, and so
+ * are inverse(s, w) and forward(s, w), which gives the backward passes. work: device
+ * complex64 [fields][nx][my][mz]. fields <= 65535, ny nz <= 16384. */
+int lsn_truncated_forward(int fields, const int n[3], const int modes[3], const float *f,
+                          void *work, void *out, float scale, float w_int, void *stream);
+int lsn_truncated_inverse(int fields, const int n[3], const int modes[3], const void *x,
+                          void *work, float *f, float scale, float w_int, void *stream);
 
 /* Adam step `step` (>= 1, bias-corrected) on n float parameters. */
 int lsn_adam(long long n, float *param, const float *grad, float *m, float *v, float lr,

@@ -87,6 +87,10 @@ SIGNATURES = {
     "lsn_spectral_backward": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p,
                                              c_int_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                              c_void_p, c_void_p]),
+    "lsn_truncated_forward": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_void_p, c_void_p,
+                                             c_void_p, ctypes.c_float, ctypes.c_float, c_void_p]),
+    "lsn_truncated_inverse": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_void_p, c_void_p,
+                                             c_void_p, ctypes.c_float, ctypes.c_float, c_void_p]),
     "lsn_adam": (ctypes.c_int, [ctypes.c_longlong, c_void_p, c_void_p, c_void_p, c_void_p,
                                 ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                 ctypes.c_int, c_void_p]),

@@ -8,9 +8,12 @@ Architecture, for a grid of nv voxels:
     out = W_proj h_L + b_proj                                       36 channels
 R_l mixes channels per retained Fourier mode (modes[0] x modes[1] x modes[2]: the lowest
 |kx|, |ky| and kz >= 0); out[6 k + c] is component c of the strain fluctuation for the
-unit load e_k. Weights are BF16 in the kernels (FP32 master copies here), activations and
-accumulation FP32. Every weighted operation, forward and backward, runs in the kernels of
-include/spectral_net.h; the 3-D transforms between them are torch.fft (cuFFT).
+unit load e_k. Weights are BF16 in the kernels (FP32 master copies here), accumulation
+FP32; the 32-channel pointwise layers run on the tensor cores with their activations
+rounded to BF16. Every operation of the network, forward and backward, runs in the kernels
+of include/spectral_net.h: the pointwise layers, the per-mode mixing and the truncated
+transforms between the fields and their retained modes (direct sums over those modes
+instead of full 3-D FFTs).
 """
 
 import ctypes
@@ -121,24 +124,52 @@ def _functions():
                            "lsn_spectral_backward")
             return dxh, dw, None, None
 
-    return Pointwise, Spectral
+    def _trunc(kind, f_or_x, n, modes, scale, w_int, out):
+        bc = out.shape[0] * out.shape[1]
+        work = torch.empty((bc, n[0], modes[1], modes[2]), device=out.device, dtype=torch.complex64)
+        nn = (ctypes.c_int * 3)(*n)
+        mm = (ctypes.c_int * 3)(*modes)
+        fn = lib.lsn_truncated_forward if kind == "fwd" else lib.lsn_truncated_inverse
+        _lib.check_net(fn(bc, nn, mm, _ptr(f_or_x), _ptr(work), _ptr(out), float(scale), float(w_int),
+                          _stream(out)), "lsn_truncated_" + kind)
+        return out
 
+    class TruncatedForward(torch.autograd.Function):
+        """h [B, C, nx, ny, nz] -> its retained modes [B, C, mx, my, mz] (numpy rfftn
+        restricted to them); backward: the transposed map (truncated inverse, no weights)."""
 
-def inverse_half_spectrum(yh, n):
-    """Real field of a half spectrum [..., nx, ny, nz/2+1] that need not be Hermitian in
-    its kz = 0 and kz = nz/2 planes: inverse DFT over x and y, then the C2R transform along
-    z with the imaginary parts of those two planes dropped, i.e. the real part of the
-    planes' contribution (numpy.fft.irfftn semantics, well defined for any input)."""
-    import torch
+        @staticmethod
+        def forward(ctx, h, n, modes):
+            h = h.contiguous()
+            out = torch.empty(tuple(h.shape[:2]) + tuple(modes), device=h.device, dtype=torch.complex64)
+            ctx.n, ctx.modes = n, modes
+            return _trunc("fwd", h, n, modes, 1.0, 1.0, out)
 
-    z = torch.fft.ifftn(yh, dim=(-3, -2))
-    nzh = z.shape[-1]
-    keep = torch.ones(nzh, device=z.device, dtype=z.real.dtype)
-    keep[0] = 0.0
-    if n[2] % 2 == 0:
-        keep[nzh - 1] = 0.0
-    z = torch.complex(z.real, z.imag * keep)
-    return torch.fft.irfft(z, n=n[2], dim=-1)
+        @staticmethod
+        def backward(ctx, dx):
+            dx = dx.contiguous()
+            dh = torch.empty(tuple(dx.shape[:2]) + tuple(ctx.n), device=dx.device, dtype=torch.float32)
+            return _trunc("inv", dx, ctx.n, ctx.modes, 1.0, 1.0, dh), None, None
+
+    class TruncatedInverse(torch.autograd.Function):
+        """Retained modes [B, C, mx, my, mz] -> real field (numpy irfftn of the zero-padded
+        half spectrum); backward: the transposed map (truncated forward, same weights)."""
+
+        @staticmethod
+        def forward(ctx, y, n, modes):
+            y = y.contiguous()
+            out = torch.empty(tuple(y.shape[:2]) + tuple(n), device=y.device, dtype=torch.float32)
+            ctx.n, ctx.modes = n, modes
+            return _trunc("inv", y, n, modes, 1.0 / (n[0] * n[1] * n[2]), 2.0, out)
+
+        @staticmethod
+        def backward(ctx, ds):
+            ds = ds.contiguous()
+            dy = torch.empty(tuple(ds.shape[:2]) + tuple(ctx.modes), device=ds.device, dtype=torch.complex64)
+            n = ctx.n
+            return _trunc("fwd", ds, n, ctx.modes, 1.0 / (n[0] * n[1] * n[2]), 2.0, dy), None, None
+
+    return Pointwise, Spectral, TruncatedForward, TruncatedInverse
 
 
 _FN = None
@@ -191,14 +222,17 @@ class SpectralNet:
         """a: [B, 2, nx, ny, nz] float32 CUDA tensor -> [B, out_channels, nx, ny, nz]."""
         import torch
 
-        pointwise, spectral = functions()
+        pointwise, spectral, tfwd, tinv = functions()
         p = self.params
         n = tuple(int(s) for s in a.shape[2:])
+        # the mixing kernels read and write the dense retained-mode layout, which is the
+        # half-spectrum layout of a (mx, my, 2 (mz - 1)) grid
+        dense = (self.modes[0], self.modes[1], 2 * (self.modes[2] - 1))
         h = pointwise.apply(a, p["lift_w"], p["lift_b"], None, 0)
         for l in range(self.layers):
-            xh = torch.fft.rfftn(h, dim=(-3, -2, -1))
-            yh = spectral.apply(xh, p[f"spec{l}"], n, self.modes)
-            s = inverse_half_spectrum(yh, n)
+            xm = tfwd.apply(h, n, self.modes)
+            ym = spectral.apply(xm, p[f"spec{l}"], dense, self.modes)
+            s = tinv.apply(ym, n, self.modes)
             h = pointwise.apply(h, p[f"w{l}"], p[f"b{l}"], s, 1)
         return pointwise.apply(h, p["proj_w"], p["proj_b"], None, 0)
 

@@ -70,3 +70,20 @@ def fd_gradient(params, a, layers, modes, loss_weights, name, index, h=1e-3):
     p[name][index] = base - h
     lm = float(np.sum(loss_weights * forward(p, a, layers, modes)))
     return (lp - lm) / (2.0 * h)
+
+
+def inverse_half_spectrum(yh, n):
+    """(torch) Real field of a half spectrum [..., nx, ny, nz/2+1] that need not be Hermitian in
+    its kz = 0 and kz = nz/2 planes: inverse DFT over x and y, then the C2R transform along
+    z with the imaginary parts of those two planes dropped, i.e. the real part of the
+    planes' contribution (numpy.fft.irfftn semantics, well defined for any input)."""
+    import torch
+
+    z = torch.fft.ifftn(yh, dim=(-3, -2))
+    nzh = z.shape[-1]
+    keep = torch.ones(nzh, device=z.device, dtype=z.real.dtype)
+    keep[0] = 0.0
+    if n[2] % 2 == 0:
+        keep[nzh - 1] = 0.0
+    z = torch.complex(z.real, z.imag * keep)
+    return torch.fft.irfft(z, n=n[2], dim=-1)

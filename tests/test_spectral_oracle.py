@@ -1,5 +1,5 @@
-"""CPU checks of the warm-start network's oracle and of the inverse transform the product
-uses between the spectral kernels (no GPU)."""
+"""CPU checks of the warm-start network's oracle, including the torch restatement of the
+inverse transform that the GPU tests' torch reference uses (no GPU)."""
 
 import numpy as np
 
@@ -8,14 +8,13 @@ from oracle import spectral_net_oracle as SO
 
 def test_inverse_half_spectrum_is_numpy_irfftn():
     import torch
-    from jaxmaterials_b200.learned.network import inverse_half_spectrum
 
     rng = np.random.default_rng(0)
     for n in [(8, 6, 10), (7, 9, 5)]:
         shape = (2, 3, n[0], n[1], n[2] // 2 + 1)
         yh = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
         ref = np.fft.irfftn(yh, s=n, axes=(-3, -2, -1))
-        got = inverse_half_spectrum(torch.as_tensor(yh), n).numpy()
+        got = SO.inverse_half_spectrum(torch.as_tensor(yh), n).numpy()
         assert np.abs(got - ref).max() < 1e-12
 
 
