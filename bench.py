@@ -62,6 +62,9 @@ def parse():
     # its full work (tolerances 0), on the seeded n^3 benchmark composite
     p.add_argument("--profile-case", action="store_true",
                    help="run --iters iterations of --batch load cases at --n^3 and exit")
+    p.add_argument("--profile-net", type=int, default=0, metavar="N",
+                   help="per-kernel device times of one training step of the warm-start "
+                        "network at N^3 (batch --batch) and exit")
     p.add_argument("--n", type=int, default=128)
     p.add_argument("--batch", type=int, default=2)
     p.add_argument("--iters", type=int, default=3)
@@ -90,6 +93,45 @@ def profile_case(args):
     print(f"n={n} batch={args.batch} depth={args.depth} iters={list(r.iters)} "
           f"launches={s.kernel_launches()}")
     s.close()
+
+
+def profile_net(args):
+    """Device time of every kernel of one training step of the warm-start network
+    (forward, MSE loss, backward, Adam) on random inputs of its shape at n^3, batch
+    `--batch`: torch.profiler (CUPTI) over three steps after three warm-up steps."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from jaxmaterials_b200.learned.network import Adam, SpectralNet
+
+    n, bsz = args.profile_net, args.batch
+    g = torch.Generator(device="cuda").manual_seed(0)
+    net = SpectralNet(seed=0)
+    opt = Adam(net.params.values(), lr=1e-3)
+    lm = torch.rand((bsz, n, n, n), device="cuda", generator=g) * 17 + 2.5
+    mu = torch.rand((bsz, n, n, n), device="cuda", generator=g) * 28 + 1.1
+    tgt = torch.randn((bsz, 36, n, n, n), device="cuda", generator=g) * 0.1
+
+    def step():
+        out = net(SpectralNet.encode(lm, mu))
+        loss = torch.mean((out - tgt) ** 2)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    print(f"n={n} batch={bsz} ms per step {(time.perf_counter() - t) / 3 * 1e3:.2f}")
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+    print(prof.key_averages().table(sort_by="cuda_time_total", row_limit=25, max_name_column_width=60))
 
 
 def generator_run(count, seed):
@@ -1022,6 +1064,9 @@ def own_arm(args):
 
 def main():
     args = parse()
+    if args.profile_net:
+        profile_net(args)
+        return
     if args.profile_case:
         profile_case(args)
     elif args.impl == "reference":
