@@ -328,7 +328,12 @@ int run_dataset_graph(const std::vector<Bucket>& buckets, int device, size_t bud
                             b.h_state + 6 * (size_t)c0, &last, &bodies);
       deps = last;
     }
-    if (rc) break;
+    if (rc) {
+      // a graph that cannot be built leaves the dataset to the threaded schedule
+      if (trace) std::fprintf(stderr, "lsb_c_eff_batch: graph build failed (%s)\n", lsb_last_error());
+      rc = kNoGraph;
+      break;
+    }
     // this bucket's kernel nodes (the ones added since the previous bucket, and the loop
     // bodies) get its priority
     size_t n_now = 0;

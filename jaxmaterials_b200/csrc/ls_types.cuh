@@ -198,9 +198,11 @@ __host__ __device__ __forceinline__ int ring_exponent(float ring_max, const doub
   return k < -60 ? -60 : (k > 60 ? 60 : k);
 }
 
-// r * 2^k rounded to FP16, saturated at +-65504 (k in [-60, 60]).
+// r * 2^k rounded to FP16, saturated at +-65504 (k in [-60, 60]); a NaN stays NaN, so that
+// the Gram solve sees it and falls back to the plain update.
 __device__ __forceinline__ __half ring_store(float r, float scale) {
-  return __float2half_rn(fminf(fmaxf(r * scale, -65504.f), 65504.f));
+  const float t = r * scale;
+  return __float2half_rn(t != t ? t : fminf(fmaxf(t, -65504.f), 65504.f));
 }
 
 struct SolveParams {
