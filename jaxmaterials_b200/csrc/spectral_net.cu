@@ -567,6 +567,49 @@ __device__ __forceinline__ void base_table(float2* base, int n) {
   }
 }
 
+// Tensor-core stage of the inverse (y, z) part: real products on mma.sync m16n8k8 TF32 with the
+// three-term split a b = a_hi b_hi + a_hi b_lo + a_lo b_hi (hi = a rounded to TF32,
+// lo = the rest rounded to TF32), which keeps the FP32 accuracy of the direct sums.
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+  const float r = x - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// D[m][n] = sum_k A[m][k] B[k][n] over one 16 x 8 output tile at (m0, n0) (A row-major with
+// row stride lda, B row-major [k][n] with row stride ldb, K a multiple of 8); the warp's
+// fragment of D is returned in d (rows m0 + g, m0 + g + 8; columns n0 + 2t, n0 + 2t + 1).
+__device__ __forceinline__ void tile_product_tf32(const float* A, int lda, const float* B, int ldb, int K,
+                                                  int m0, int n0, float (&d)[4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  d[0] = d[1] = d[2] = d[3] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += 8) {
+    unsigned ah[4], al[4], bh0, bl0, bh1, bl1;
+    split_tf32(A[(m0 + g) * lda + k0 + t], ah[0], al[0]);
+    split_tf32(A[(m0 + g + 8) * lda + k0 + t], ah[1], al[1]);
+    split_tf32(A[(m0 + g) * lda + k0 + t + 4], ah[2], al[2]);
+    split_tf32(A[(m0 + g + 8) * lda + k0 + t + 4], ah[3], al[3]);
+    split_tf32(B[(k0 + t) * ldb + n0 + g], bh0, bl0);
+    split_tf32(B[(k0 + t + 4) * ldb + n0 + g], bh1, bl1);
+    mma_tf32(d, al, bh0, bh1);
+    mma_tf32(d, ah, bl0, bl1);
+    mma_tf32(d, ah, bh0, bh1);
+  }
+}
+
+// Row stride (floats) of a shared-memory matrix with n columns read as B fragments (lanes
+// (t, g) at rows t, columns g): rows four or eight banks apart, so the 32 lanes are distinct.
+__host__ __device__ __forceinline__ int frag_ld(int n) { return n % 16 == 8 ? n : n + 8; }
+__host__ __device__ __forceinline__ int pad8(int n) { return (n + 7) / 8 * 8; }
+
 // fwd, (y, z) part: P[bc][x][iy][iz] = sum_{y,z} f[bc][x][y][z] e^{-i(ky y + iz z)}.
 // Stage 1: thread (y, group) accumulates the iz of its group over z (plane rows padded by
 // one float so that the lanes, consecutive y, hit distinct banks; the twiddle row of an iz
@@ -698,21 +741,40 @@ __global__ void __launch_bounds__(256) trunc_inv_x(long long total, int nx, int 
 // inv, (y, z) part: f[bc][x][y][z] = Re sum_{iy,iz} Q[bc][x][iy][iz] e^{+i(ky y + iz z)}.
 // Stage 1: thread (y, iz) over iy. Stage 2: thread (y, z), z fastest, over iz (the row of
 // stage 1 is the same for the warp's lanes, the twiddles of an iz consecutive).
-__global__ void __launch_bounds__(kTrThreads) trunc_inv_yz(int nx, int ny, int nz, int my, int mz,
+__global__ void __launch_bounds__(kTrThreads) trunc_inv_yz(int nx, int ny, int nz, int my, int mz, int tc,
                                                            const float2* __restrict__ q,
                                                            float* __restrict__ f) {
   extern __shared__ __align__(16) unsigned char trraw[];
+  // tc: stage 2 on the tensor cores (ny % 16 == 0, nz % 8 == 0) as the product of rt
+  // [ny][2 mz] (re, im interleaved, zero-padded to a multiple of 8 columns) with bi
+  // [2 mz][nz] (rows cos, -sin of 2 pi iz z / nz)
+  const int kp = pad8(2 * mz), mzr = tc ? kp / 2 + 2 : mz;  // rt row: mzr complex values
+  const int ldb = frag_ld(nz);
   float2* tz = reinterpret_cast<float2*>(trraw);  // [mz][nz]
   float2* ty = tz + mz * nz;                      // [my][ny]
   float2* qs = ty + my * ny;                      // [my][mz]
-  float2* rt = qs + my * mz;                      // [ny][mz]
-  float2* base = rt + ny * mz;                    // [max(ny, nz)]
+  float2* rt = qs + my * mz;                      // [ny][mzr]
+  float2* base = rt + ny * mzr;                   // [max(ny, nz)]
+  float* bi = reinterpret_cast<float*>(base + (ny > nz ? ny : nz));  // [kp][ldb] (tc)
   const size_t bc = blockIdx.y;
   base_table(base, nz);
   __syncthreads();
   for (int i = threadIdx.x; i < mz * nz; i += blockDim.x) {
     const int iz = i / nz, z = i - iz * nz;
     tz[i] = base[(int)((long long)iz * z % nz)];
+  }
+  if (tc) {
+    for (int i = threadIdx.x; i < kp * ldb; i += blockDim.x) {
+      const int k = i / ldb, z = i - k * ldb, iz = k >> 1;
+      float v = 0.f;
+      if (k < 2 * mz && z < nz) {
+        const float2 w = base[(int)((long long)iz * z % nz)];
+        v = (k & 1) ? -w.y : w.x;
+      }
+      bi[i] = v;
+    }
+    // the padding columns of rt stay zero
+    for (int i = threadIdx.x; i < ny * mzr; i += blockDim.x) rt[i] = make_float2(0.f, 0.f);
   }
   __syncthreads();
   base_table(base, ny);
@@ -735,21 +797,36 @@ __global__ void __launch_bounds__(kTrThreads) trunc_inv_yz(int nx, int ny, int n
       re = fmaf(a.x, t.x, fmaf(-a.y, t.y, re));
       im = fmaf(a.y, t.x, fmaf(a.x, t.y, im));
     }
-    rt[o] = make_float2(re, im);
+    rt[y * mzr + iz] = make_float2(re, im);
   }
   __syncthreads();
   float* dst = f + (bc * nx + x) * (size_t)ny * nz;
+  if (tc) {
+    const int nt = nz / 8, tiles = ny / 16 * nt;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int tile = threadIdx.x >> 5; tile < tiles; tile += blockDim.x >> 5) {
+      const int m0 = tile / nt * 16, n0 = tile % nt * 8;
+      float d[4];
+      tile_product_tf32(reinterpret_cast<const float*>(rt), 2 * mzr, bi, ldb, kp, m0, n0, d);
+      *reinterpret_cast<float2*>(dst + (size_t)(m0 + g) * nz + n0 + 2 * t) = make_float2(d[0], d[1]);
+      *reinterpret_cast<float2*>(dst + (size_t)(m0 + g + 8) * nz + n0 + 2 * t) = make_float2(d[2], d[3]);
+    }
+    continue;
+  }
   for (int o = threadIdx.x; o < ny * nz; o += blockDim.x) {
     const int y = o / nz, z = o - y * nz;
     float v = 0.f;
     for (int iz = 0; iz < mz; ++iz) {
-      const float2 a = rt[y * mz + iz], t = tz[iz * nz + z];  // Re(a t)
+      const float2 a = rt[y * mzr + iz], t = tz[iz * nz + z];  // Re(a t)
       v = fmaf(a.x, t.x, fmaf(-a.y, t.y, v));
     }
     dst[o] = v;
   }
   }
 }
+
+// The (y, z) parts use the tensor-core stages when the plane tiles into 16 x 8 fragments.
+int tc_planes(int ny, int nz) { return ny % 16 == 0 && nz % 8 == 0 ? 1 : 0; }
 
 int trunc_check(long long bc, const int n[3], const int modes[3]) {
   if (bc < 1 || bc > 65535) return fail(-1, "truncated transform: fields outside [1, 65535]");
@@ -850,8 +927,11 @@ int lsn_truncated_inverse(int fields, const int n[3], const int modes[3], const 
   if (!n || !modes || !y || !work || !f) return fail(-1, "lsn_truncated_inverse: null argument");
   if (int rc = trunc_check(fields, n, modes)) return rc;
   const int nx = n[0], ny = n[1], nz = n[2], mx = modes[0], my = modes[1], mz = modes[2];
-  const size_t smem = sizeof(float2) * ((size_t)mz * nz + (size_t)my * ny + (size_t)my * mz + (size_t)ny * mz +
-                                        (ny > nz ? ny : nz));
+  const int tc = tc_planes(ny, nz);
+  const int mzr = tc ? pad8(2 * mz) / 2 + 2 : mz;
+  const size_t smem = sizeof(float2) * ((size_t)mz * nz + (size_t)my * ny + (size_t)my * mz + (size_t)ny * mzr +
+                                        (ny > nz ? ny : nz)) +
+                      (tc ? sizeof(float) * (size_t)pad8(2 * mz) * frag_ld(nz) : 0);
   static bool big = false;
   if (!big) {
     cudaFuncSetAttribute(trunc_fwd_yz, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
@@ -862,7 +942,7 @@ int lsn_truncated_inverse(int fields, const int n[3], const int modes[3], const 
   const long long total = (long long)fields * nx * my * mz;
   trunc_inv_x<<<(unsigned)((total + 255) / 256), 256, sizeof(float2) * nx, s>>>(
       total, nx, nz, mx, my, mz, scale, w_int, (const float2*)y, (float2*)work);
-  trunc_inv_yz<<<dim3(std::min(nx, kTrPlaneBlocks), fields), kTrThreads, smem, s>>>(nx, ny, nz, my, mz,
+  trunc_inv_yz<<<dim3(std::min(nx, kTrPlaneBlocks), fields), kTrThreads, smem, s>>>(nx, ny, nz, my, mz, tc,
                                                                                    (const float2*)work, f);
   return 0;
 }
