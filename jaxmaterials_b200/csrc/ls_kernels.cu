@@ -772,7 +772,10 @@ __global__ void __launch_bounds__(kSolveThreads) anderson_solve_kernel(
   if (tid == M1) {
     double m = 0.0;
     for (int w = 0; w < kSolveThreads / 32; ++w) m = fmax(m, red[w][M1]);
-    if (phase == 0) s.ring_max = (float)m;
+    // (a residual whose stored values all underflowed FP16 at this slot's scale reports
+    // the underflow threshold instead of 0, so that the next slot's scale rises by 2^34
+    // rather than falling back to the first slot's guess)
+    if (phase == 0) s.ring_max = m > 0.0 ? (float)m : ldexpf(1.f, -25 - s.ring_exp[slot]);
   }
   if (tid < filled) {
     double t = 0.0;

@@ -209,6 +209,29 @@ def test_linearity_and_batch(ls):
     s.close()
 
 
+@pytest.mark.parametrize("n", [(32, 32, 32), (37, 47, 61)])
+def test_anderson_scale_invariance(ls, n):
+    """Power-of-two scalings of eps_bar (2^-40, 2^30) scale every FP32 and FP64 operation of
+    the solve exactly, so the fields scale exactly and the iteration counts are unchanged
+    with Anderson depth 5: the FP16 residual ring chooses its per-slot scales from the data
+    (first slot from eps_bar, later slots from the previous residual's max), so the
+    residuals neither underflow nor overflow FP16 at either end."""
+    import torch
+    from jaxmaterials_b200 import GridSpec
+
+    g = GridSpec(*n, *EXT)
+    lm, mu = reference_material(n)
+    s = ls.Solver(g, batch=1, depth=5)
+    ref = s.solve(lm, mu, EPS_BAR, rtol=1e-6, atol=0.0, maxiter=400)
+    assert ref.status[0] == ls.CONVERGED
+    for e in (-40, 30):
+        f = np.float32(2.0 ** e)
+        r = s.solve(lm, mu, EPS_BAR * f, rtol=1e-6, atol=0.0, maxiter=400)
+        assert r.iters[0] == ref.iters[0]
+        assert torch.equal(r.epsilon[0], ref.epsilon[0] * float(f))
+    s.close()
+
+
 def _reference_cuda():
     path = os.path.join(ROOT, "oracle", "_ref", "liblippmannschwinger.so")
     if not os.path.exists(path):
