@@ -161,7 +161,11 @@ __global__ void __launch_bounds__(y_threads<NY>(), TILED ? yt_min_blocks<NY>() :
                                                                const InstanceState* __restrict__ st) {
   constexpr int E = YSplit<NY>::E, P = YSplit<NY>::P, NJ = (E + P - 1) / P;
   constexpr int YT = y_cols<NY>();
-  __shared__ float2 buf[NY * YT];
+  // rows k1 of the transposed layout padded to RS = 8 (mod 16) values, so that the two rows
+  // a half-warp reads in step B (lanes: YT columns t of consecutive k1) fall in disjoint
+  // bank halves (unpadded, P YT = 128 at 128 put them in the same banks)
+  constexpr int RS = P * YT + (8 - (P * YT) % 16 + 16) % 16;
+  __shared__ float2 buf[E * RS];
   const int bc = blockIdx.z;
   if (!active32(st[bc / 6])) return;
   const int t = threadIdx.x % YT, p = threadIdx.x / YT;
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(y_threads<NY>(), TILED ? yt_min_blocks<NY>() :
   }
   step_a<NY, E>(v, p, tw);
 #pragma unroll
-  for (int k1 = 0; k1 < E; ++k1) buf[(k1 * P + p) * YT + t] = v[k1];
+  for (int k1 = 0; k1 < E; ++k1) buf[k1 * RS + p * YT + t] = v[k1];
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < NJ; ++j) {
@@ -210,7 +214,7 @@ __global__ void __launch_bounds__(y_threads<NY>(), TILED ? yt_min_blocks<NY>() :
     if (k1 >= E) break;
     float2 w[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) w[q] = buf[(k1 * P + q) * YT + t];
+    for (int q = 0; q < P; ++q) w[q] = buf[k1 * RS + q * YT + t];
     Bfly<P>::run(w);
     if (valid) {
 #pragma unroll
