@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--profile-net", type=int, default=0, metavar="N",
                    help="per-kernel device times of one training step of the warm-start "
                         "network at N^3 (batch --batch) and exit")
+    p.add_argument("--layout", default="tuned", choices=["tuned", "tiled", "strided"],
+                   help="--profile-case: spectrum layout between the y and x passes "
+                        "(default: the autotuner's choice)")
     p.add_argument("--n", type=int, default=128)
     p.add_argument("--batch", type=int, default=2)
     p.add_argument("--iters", type=int, default=3)
@@ -87,6 +90,9 @@ def profile_case(args):
     g = GridSpec(n, n, n, float(n), float(n), float(n))
     s = Solver(g, batch=args.batch, depth=args.depth, precision=args.precision)
     s.set_device_loop(False)  # profilers do not see kernels inside conditional graphs
+    if args.layout != "tuned":
+        s.set_tiled(args.layout == "tiled")
+        s.tile_variant(0)
     eb = np.eye(6, dtype=np.float32)[np.arange(args.batch) % 6]
     r = s.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=args.iters, want_sigma=False)
     torch.cuda.synchronize()
