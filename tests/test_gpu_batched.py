@@ -125,6 +125,31 @@ def test_c_eff_batch_graph_equals_threads(monkeypatch):
         assert (g[2] == 1).all()
 
 
+def test_c_eff_batch_graph_buckets_by_extents(monkeypatch):
+    """Equal voxel counts with different extents are different buckets (their wave vectors
+    differ); single-structure buckets and a one-structure dataset take the graph path too:
+    the same results as the threaded schedule and as the single-structure path."""
+    from jaxmaterials_b200 import GridSpec
+    from jaxmaterials_b200.solver import c_eff, c_eff_batch
+
+    structs = fibre_set([16, 16, 24], seed=21)
+    lms, mus, gs = zip(*structs)
+    gs = [gs[0], GridSpec(16, 16, 16, 16.0, 24.0, 8.0), gs[2]]
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("LSB_BATCH_GRAPH", mode)
+        out[mode] = c_eff_batch(lms, mus, gs, rtol=1e-6, maxiter=3000, depth=5)
+        one = c_eff_batch(lms[:1], mus[:1], gs[:1], rtol=1e-6, maxiter=3000, depth=5)
+        np.testing.assert_array_equal(one[0][0], out[mode][0][0])
+    for k in range(3):
+        np.testing.assert_array_equal(out["1"][k], out["0"][k])
+    for i in range(3):
+        c1, it1, _ = c_eff(lms[i], mus[i], gs[i], rtol=1e-6, maxiter=3000, depth=5)
+        np.testing.assert_array_equal(out["1"][0][i], c1)
+        np.testing.assert_array_equal(out["1"][1][i], it1)
+    assert not np.allclose(out["1"][0][0], out["1"][0][1])  # the extents matter
+
+
 def test_c_eff_batch_rejects_bad_input():
     from jaxmaterials_b200 import GridSpec
     from jaxmaterials_b200._lib import LibraryError
