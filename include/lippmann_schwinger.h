@@ -109,6 +109,13 @@ int lsb_set_warm_history(lsb_solver *solver, int on);
  * 0 or 1 fixes it, -1 only queries. Returns the variant in use (0 before tuning). */
 int lsb_tile_variant(lsb_solver *solver, int variant);
 
+/* No reference counterpart. Variant of the FP32 y pass: kz columns per block (0: 8 at
+ * extent 128 and 16 elsewhere, 1: the other of 8 and 16; the results are the same). By
+ * default the solver's autotuner times both with each x-pass configuration on its first
+ * FP32 solve. variant = 0 or 1 fixes it (and the other choices), -1 only queries. Returns
+ * the variant in use. */
+int lsb_y_variant(lsb_solver *solver, int variant);
+
 /* No reference counterpart. Layout of the FP32 spectrum between the y and x passes:
  * on = 1 (where it applies: every extent in {16, 32, 48, 64, 96, 128}, ny a power of two) keeps
  * it in contiguous x tiles of 8 kz columns in a second spectrum buffer, so that the x pass

@@ -40,6 +40,7 @@ SIGNATURES = {
     "lsb_set_lame_group": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_set_graphs": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_set_device_loop": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "lsb_y_variant": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_set_warm_history": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_tile_variant": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "lsb_set_tiled": (ctypes.c_int, [c_void_p, ctypes.c_int]),

@@ -117,10 +117,12 @@ __host__ __device__ __forceinline__ size_t tile_offset(int nx, int ny, int nf, i
 #define LSB_Y_COLS 16
 #endif
 constexpr int kYT = LSB_Y_COLS;
-// kz columns per y-pass block for extent N (128, with 16 threads per column: 8 columns,
-// eight resident blocks per SM; measured -3% against 16 columns, 32 columns +14%)
-template <int N>
-__host__ __device__ constexpr int y_cols() { return N == 128 ? 8 : kYT; }
+// kz columns per y-pass block for extent N and variant YV: variant 0 is 8 at 128 (16
+// threads per column, eight resident blocks per SM; measured -3% against 16 columns, 32
+// columns +14%) and kYT elsewhere; variant 1 the other of 8 and 16. The autotuner times
+// both (the results are the same: a column's transform does not depend on YT).
+template <int N, int YV = 0>
+__host__ __device__ constexpr int y_cols() { return (N == 128) != (YV == 1) ? 8 : kYT; }
 
 // Split of the y transform (may differ from the x/z split): 128 = 8 x 16 puts 16 threads
 // on a column and halves the values each thread holds (measured -13% at 128^3 against
@@ -129,12 +131,12 @@ template <int N>
 struct YSplit { static constexpr int E = Split<N>::E, P = Split<N>::P; };
 template <>
 struct YSplit<128> { static constexpr int E = 8, P = 16; };
-template <int N>
-__host__ __device__ constexpr int y_threads() { return y_cols<N>() * YSplit<N>::P; }
-template <int N>
+template <int N, int YV = 0>
+__host__ __device__ constexpr int y_threads() { return y_cols<N, YV>() * YSplit<N>::P; }
+template <int N, int YV = 0>
 __host__ __device__ constexpr int y_min_blocks() {
   // (256: three blocks, so that its 16 values per thread fit without spilling)
-  return N == 256 ? 3 : 1024 / (32 * ((y_threads<N>() + 31) / 32));
+  return N == 256 ? 3 : 1024 / (32 * ((y_threads<N, YV>() + 31) / 32));
 }
 
 // TILED: the x-pass side of the transform is the tiled layout in `tspec` (see xpass_tiled):
@@ -146,21 +148,21 @@ __host__ __device__ constexpr int y_min_blocks() {
 #ifndef LSB_YT_MINB_NUM
 #define LSB_YT_MINB_NUM 4
 #endif
-template <int NY>
+template <int NY, int YV = 0>
 __host__ __device__ constexpr int yt_min_blocks() {
   // (other extents: half the in-place form's blocks; at 48 and 96, whose threads hold 16
   // values, the full count spilled and made the pass 2-3x slower)
-  return NY == 128 ? LSB_YT_MINB_NUM * y_min_blocks<NY>() / 4
-                   : (y_min_blocks<NY>() / 2 > 2 ? y_min_blocks<NY>() / 2 : 2);
+  return NY == 128 ? LSB_YT_MINB_NUM * y_min_blocks<NY, YV>() / 4
+                   : (y_min_blocks<NY, YV>() / 2 > 2 ? y_min_blocks<NY, YV>() / 2 : 2);
 }
-template <int NY, bool TILED>
-__global__ void __launch_bounds__(y_threads<NY>(), TILED ? yt_min_blocks<NY>() : y_min_blocks<NY>())
+template <int NY, bool TILED, int YV>
+__global__ void __launch_bounds__(y_threads<NY, YV>(), TILED ? yt_min_blocks<NY, YV>() : y_min_blocks<NY, YV>())
     ypass_fast(GridDesc g, int inverse,
                                                                float2* __restrict__ spec,
                                                                float2* __restrict__ tspec,
                                                                const InstanceState* __restrict__ st) {
   constexpr int E = YSplit<NY>::E, P = YSplit<NY>::P, NJ = (E + P - 1) / P;
-  constexpr int YT = y_cols<NY>();
+  constexpr int YT = y_cols<NY, YV>();
   // rows k1 of the transposed layout padded to RS = 8 (mod 16) values, so that the two rows
   // a half-warp reads in step B (lanes: YT columns t of consecutive k1) fall in disjoint
   // bank halves (unpadded, P YT = 128 at 128 put them in the same banks)
@@ -1447,29 +1449,36 @@ int z_blocks(const GridDesc& g) {
   }
 }
 
-template <int N>
-static void ylaunch(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
-                    const InstanceState* st, cudaStream_t s) {
+template <int N, int YV>
+static void ylaunch_v(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+                      const InstanceState* st, cudaStream_t s) {
   // with a one-column tail, full tiles + one tail tile (see ypass_fast)
-  constexpr int YT = y_cols<N>();
+  constexpr int YT = y_cols<N, YV>();
   dim3 grid(g.nzh % YT == 1 ? g.nzh / YT + 1 : (g.nzh + YT - 1) / YT, g.nx, 6 * batch);
   if (tspec)
-    ypass_fast<N, true><<<dim3(grid.y, grid.x, grid.z), y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec,
-                                                                                tspec, st);
+    ypass_fast<N, true, YV><<<dim3(grid.y, grid.x, grid.z), y_threads<N, YV>(), 0, s>>>(
+        g, inverse ? 1 : 0, spec, tspec, st);
   else
-    ypass_fast<N, false><<<grid, y_threads<N>(), 0, s>>>(g, inverse ? 1 : 0, spec, spec, st);
+    ypass_fast<N, false, YV><<<grid, y_threads<N, YV>(), 0, s>>>(g, inverse ? 1 : 0, spec, spec, st);
 }
 
-void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+template <int N>
+static void ylaunch(int variant, const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+                    const InstanceState* st, cudaStream_t s) {
+  if (variant) ylaunch_v<N, 1>(g, inverse, batch, spec, tspec, st, s);
+  else ylaunch_v<N, 0>(g, inverse, batch, spec, tspec, st, s);
+}
+
+void launch_ypass(const GridDesc& g, int variant, bool inverse, int batch, float2* spec, float2* tspec,
                   const InstanceState* st, cudaStream_t s) {
   switch (g.ny) {
-    case 16: ylaunch<16>(g, inverse, batch, spec, tspec, st, s); break;
-    case 32: ylaunch<32>(g, inverse, batch, spec, tspec, st, s); break;
-    case 48: ylaunch<48>(g, inverse, batch, spec, tspec, st, s); break;
-    case 96: ylaunch<96>(g, inverse, batch, spec, tspec, st, s); break;
-    case 64: ylaunch<64>(g, inverse, batch, spec, tspec, st, s); break;
-    case 128: ylaunch<128>(g, inverse, batch, spec, tspec, st, s); break;
-    default: ylaunch<256>(g, inverse, batch, spec, tspec, st, s); break;
+    case 16: ylaunch<16>(variant, g, inverse, batch, spec, tspec, st, s); break;
+    case 32: ylaunch<32>(variant, g, inverse, batch, spec, tspec, st, s); break;
+    case 48: ylaunch<48>(variant, g, inverse, batch, spec, tspec, st, s); break;
+    case 96: ylaunch<96>(variant, g, inverse, batch, spec, tspec, st, s); break;
+    case 64: ylaunch<64>(variant, g, inverse, batch, spec, tspec, st, s); break;
+    case 128: ylaunch<128>(variant, g, inverse, batch, spec, tspec, st, s); break;
+    default: ylaunch<256>(variant, g, inverse, batch, spec, tspec, st, s); break;
   }
 }
 

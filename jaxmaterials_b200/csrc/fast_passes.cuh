@@ -17,8 +17,9 @@ void launch_zpass(const GridDesc& g, int mode, int batch, const float* lambda, c
                   float* eps, float2* spec, const double* eps_bar, const float* eps0,
                   InstanceState* st, const Medium* med, const AndersonArgs<float>& aa, cudaStream_t s);
 // tspec != nullptr: the x-pass side is the tiled layout in tspec (the forward pass writes
-// it, the inverse pass reads it); otherwise the transform runs in place on spec.
-void launch_ypass(const GridDesc& g, bool inverse, int batch, float2* spec, float2* tspec,
+// it, the inverse pass reads it); otherwise the transform runs in place on spec. variant:
+// kz columns per block (0: 8 at 128, 16 elsewhere; 1: the other of 8 and 16).
+void launch_ypass(const GridDesc& g, int variant, bool inverse, int batch, float2* spec, float2* tspec,
                   const InstanceState* st, cudaStream_t s);
 // The tiled spectrum layout between the y and x passes applies (nx <= 128, ny and nz/2 a
 // multiple of 8, every extent supported).

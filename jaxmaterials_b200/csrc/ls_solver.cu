@@ -407,8 +407,8 @@ template <typename T>
 void pass_y(lsb_solver* s, bool inverse, int batch, cplx<T>* spec) {
   if constexpr (sizeof(T) == 4) {
     if (use_fast32(s)) {
-      fast::launch_ypass(s->g, inverse, batch, spec, s->tiled ? s->d_tspec32 : nullptr, s->d_state,
-                         s->stream);
+      fast::launch_ypass(s->g, s->yvariant, inverse, batch, spec, s->tiled ? s->d_tspec32 : nullptr,
+                         s->d_state, s->stream);
       return;
     }
   }
@@ -754,7 +754,7 @@ int run_phase(lsb_solver* s, int batch, const T* lam, const T* mu, T* eps, cplx<
 // (LSB_TUNE_CACHE, else $HOME/.cache/jaxmaterials_b200/tune.tsv; an empty value or "0"
 // disables the file), so that later processes skip the timing.
 struct TuneChoice {
-  int tiled, xvariant, slab;
+  int tiled, xvariant, slab, yvariant;
 };
 constexpr int kTuneReps = 3;
 
@@ -780,7 +780,7 @@ void tune_load_locked() {
     std::istringstream ls(line);
     std::string key;
     TuneChoice c{};
-    if (std::getline(ls, key, '\t') && (ls >> c.tiled >> c.xvariant >> c.slab)) (*g_tune)[key] = c;
+    if (std::getline(ls, key, '\t') && (ls >> c.tiled >> c.xvariant >> c.slab >> c.yvariant)) (*g_tune)[key] = c;
   }
 }
 
@@ -796,7 +796,9 @@ void tune_store_locked(const std::string& key, const TuneChoice& c, float ms) {
       if (k == dir.size() || dir[k] == '/') mkdir(dir.substr(0, k).c_str(), 0755);
   }
   std::ofstream out(path, std::ios::app);
-  if (out) out << key << '\t' << c.tiled << '\t' << c.xvariant << '\t' << c.slab << '\t' << ms << '\n';
+  if (out)
+    out << key << '\t' << c.tiled << '\t' << c.xvariant << '\t' << c.slab << '\t' << c.yvariant << '\t' << ms
+        << '\n';
 }
 
 std::string tune_key(const lsb_solver* s) {
@@ -806,7 +808,8 @@ std::string tune_key(const lsb_solver* s) {
     dev = std::string(prop.name) + "/" + std::to_string(prop.multiProcessorCount);
   const char* law = s->g.cf32 ? "aniso" : (s->g.dmg32 ? "damage" : "iso");
   char buf[256];
-  std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|m%d|%s", dev.c_str(), s->g.nx, s->g.ny, s->g.nz,
+  // (|y: the entries that carry the y-pass variant)
+  std::snprintf(buf, sizeof(buf), "%s|%dx%dx%d|m%d|%s|y", dev.c_str(), s->g.nx, s->g.ny, s->g.nz,
                 s->depth, law);
   return buf;
 }
@@ -815,6 +818,7 @@ void apply_choice(lsb_solver* s, const TuneChoice& c) {
   s->tiled = c.tiled && s->d_tspec32 != nullptr && fast::tiled_supported(s->g);
   s->slab = c.slab && s->tiled && fast::slab_supported(s->g);
   s->xvariant = c.xvariant;
+  s->yvariant = c.yvariant;
   if (s->tiled) s->sh32.x_blocks_per_instance = fast::x_tiles_tiled(s->g);
   else s->sh32.x_blocks_per_instance = fast::x_tiles(s->g, s->xvariant) * s->g.ny;
 }
@@ -878,13 +882,20 @@ int tune_passes(lsb_solver* s, int batch, const float* d_lambda, const float* d_
       return 0;
     }
   }
+  // (each configuration with either y-pass column count, except the slab pass, which has
+  // no y pass of its own)
   std::vector<TuneChoice> cand;
   if (s->d_tspec32 && fast::tiled_supported(s->g)) {
-    cand.push_back({1, 0, 0});
-    if (fast::slab_supported(s->g) && !s->g.cf32 && !s->g.dmg32) cand.push_back({1, 0, 1});
+    cand.push_back({1, 0, 0, 0});
+    cand.push_back({1, 0, 0, 1});
+    if (fast::slab_supported(s->g) && !s->g.cf32 && !s->g.dmg32) cand.push_back({1, 0, 1, 0});
   }
-  cand.push_back({0, 0, 0});
-  if (fast::x_tiles(s->g, 0) != fast::x_tiles(s->g, 1)) cand.push_back({0, 1, 0});
+  cand.push_back({0, 0, 0, 0});
+  cand.push_back({0, 0, 0, 1});
+  if (fast::x_tiles(s->g, 0) != fast::x_tiles(s->g, 1)) {
+    cand.push_back({0, 1, 0, 0});
+    cand.push_back({0, 1, 0, 1});
+  }
   TuneChoice best = cand[0];
   float best_ms = 0.f;
   if (cand.size() > 1) {
@@ -1245,6 +1256,16 @@ int lsb_tile_variant(lsb_solver* solver, int variant) {
       solver->sh32.x_blocks_per_instance = fast::x_tiles(solver->g, variant) * solver->g.ny;
   }
   return solver->xvariant;
+}
+
+int lsb_y_variant(lsb_solver* solver, int variant) {
+  if (!solver) return fail(-1, "null solver");
+  if (variant < -1 || variant > 1) return fail(-1, "y-pass variant %d outside [-1, 1]", variant);
+  if (variant >= 0 && solver->fast32) {
+    solver->yvariant = variant;
+    solver->xtuned = true;  // the caller's choice: no autotuning
+  }
+  return solver->yvariant;
 }
 
 int lsb_pass_config(lsb_solver* solver, int* out) {

@@ -31,6 +31,7 @@ struct lsb_solver {
   bool slab_allowed = false;  // measured slower than the separate passes (opt-in)
   cudaError_t launch_error = cudaSuccess;  // first failed cluster launch since the last check
   int xvariant = 0;      // x-pass tile variant of the fast passes (chosen by timing)
+  int yvariant = 0;      // y-pass column-count variant of the fast passes (chosen by timing)
   bool xtuned = false;   // xvariant has been chosen
   bool warm_history = false;  // d_eps0 enters the Anderson history instead of starting it
   GridDesc g{};

@@ -144,19 +144,25 @@ class Solver:
         return _lib.check(self._lib.lsb_tile_variant(self._h, -1 if variant is None else int(variant)),
                           "lsb_tile_variant")
 
+    def y_variant(self, variant=None):
+        """y-pass variant in use (kz columns per block; chosen by timing on the first FP32
+        solve); an argument 0 or 1 fixes it (bit-identical results either way)."""
+        return _lib.check(self._lib.lsb_y_variant(self._h, -1 if variant is None else int(variant)),
+                          "lsb_y_variant")
+
     def set_tiled(self, on=True):
         """Tiled spectrum layout between the y and x passes (the default where it applies;
         results are bit-identical either way). Returns whether it is in use."""
         return bool(_lib.check(self._lib.lsb_set_tiled(self._h, 1 if on else 0), "lsb_set_tiled"))
 
     def pass_config(self):
-        """FP32 pass configuration: dict(tiled, xvariant, slab, settled); settled once the
-        autotuner ran (first FP32 solve) or the caller fixed it."""
+        """FP32 pass configuration: dict(tiled, xvariant, slab, yvariant, settled);
+        settled once the autotuner ran (first FP32 solve) or the caller fixed it."""
         out = np.zeros(4, dtype=np.int32)
         _lib.check(self._lib.lsb_pass_config(self._h, out.ctypes.data_as(_lib.c_int_p)),
                    "lsb_pass_config")
         return {"tiled": bool(out[0]), "xvariant": int(out[1]), "slab": bool(out[2]),
-                "settled": bool(out[3])}
+                "yvariant": self.y_variant(), "settled": bool(out[3])}
 
     def set_device_loop(self, on=True):
         """Run each solve phase as one graph launch whose WHILE node stops on the device

@@ -625,14 +625,18 @@ def test_autotuner_caches_its_choice(ls, tmp_path, monkeypatch):
     assert cfg["settled"]
     lines = [l.split("\t") for l in cache.read_text().splitlines()]
     assert any("32x32x32|m2|iso" in l[0] for l in lines)
+    assert all(len(l) == 6 for l in lines)  # key, tiled, x variant, slab, y variant, ms
     s2 = Solver(g, batch=3, depth=2)
     s2.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=1)
     assert s2.pass_config() == cfg
     s2.close()
-    for tiled, slab in ((True, False), (True, True), (False, False)):
+    for tiled, slab, variant, yv in ((True, False, 0, 0), (True, False, 0, 1), (True, True, 0, 0),
+                                     (False, False, 0, 0), (False, False, 1, 1)):
         f = Solver(g, batch=3, depth=2)
         f.set_tiled(tiled)
         f.set_slab(slab)
+        f.tile_variant(variant)
+        assert f.y_variant(yv) == yv
         rf = f.solve(lm, mu, eb, rtol=0.0, atol=0.0, maxiter=10)
         assert torch.equal(rf.epsilon, r.epsilon)
         f.close()
