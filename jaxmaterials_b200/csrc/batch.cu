@@ -459,9 +459,11 @@ extern "C" int lsb_c_eff_batch(int nstruct, const int* voxels, const double* ext
                            sorted_sizes.begin());
     return std::min(least, greatest + rank);
   };
-  // One graph for the whole dataset (LSB_BATCH_GRAPH=0: the threaded schedule below).
+  // One graph for the whole dataset (LSB_BATCH_GRAPH=0: the threaded schedule below; FP64
+  // solves, which start in FP64, also take the threaded schedule: the graph's solves start
+  // in FP32).
   const char* gmode = std::getenv("LSB_BATCH_GRAPH");
-  if (!(gmode && gmode[0] == '0' && gmode[1] == 0)) {
+  if (!(gmode && gmode[0] == '0' && gmode[1] == 0) && precision != LSB_PREC_FP64) {
     std::vector<int> prio(buckets.size());
     for (size_t b = 0; b < buckets.size(); ++b) prio[b] = priority_of(b);
     const int grc = run_dataset_graph(buckets, device, budget, depth, precision, (double)rtol, (double)atol,

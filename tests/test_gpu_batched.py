@@ -123,6 +123,15 @@ def test_c_eff_batch_graph_equals_threads(monkeypatch):
         np.testing.assert_array_equal(g[1], t[1])
         np.testing.assert_array_equal(g[2], t[2])
         assert (g[2] == 1).all()
+    # FP64 solves (FP64 from the first update) in either mode, against the FP32-start ones
+    f64 = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("LSB_BATCH_GRAPH", mode)
+        f64[mode] = c_eff_batch(lms[:2], mus[:2], list(gs[:2]), rtol=1e-9, maxiter=3000, depth=5,
+                                precision="fp64")
+    np.testing.assert_array_equal(f64["1"][0], f64["0"][0])
+    rel = np.linalg.norm(f64["1"][0] - out["1", 2e-7][0][:2]) / np.linalg.norm(f64["1"][0])
+    assert rel < 1e-5
 
 
 def test_c_eff_batch_graph_buckets_by_extents(monkeypatch):
