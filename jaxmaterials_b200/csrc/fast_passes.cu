@@ -647,6 +647,13 @@ __host__ __device__ constexpr int z_ld() {
 struct ZLayout {  // byte offsets inside the z pass's dynamic shared memory
   size_t zbuf, rst, est, lst, total;
 };
+// Modes 1 and 3 (compiled per mode) read their strain rows (and, mode 1, lambda and mu)
+// only after the inverse z transform: those rows are staged late, into the region of the
+// spectrum rows once they have been expanded into the transform buffer, so that the copies
+// overlap the transform and the block needs less shared memory (at 128: 27 KB and eight
+// resident blocks for mode 3 instead of 39 KB and five; 31 KB and seven for mode 1).
+template <int MODE>
+__host__ __device__ constexpr bool z_late() { return MODE == 1 || MODE == 3; }
 // MODE < 0: the mode is a run-time argument (every staging region); otherwise only the
 // regions that mode stages (spectrum rows for 1 and 3, strain rows for 1-3, lambda and mu
 // rows for 0-2), so that the other modes keep more blocks resident.
@@ -660,6 +667,8 @@ __host__ __device__ constexpr ZLayout z_layout() {
   constexpr size_t rs = r ? (size_t)6 * L * NZH * 8 : 0;
   constexpr size_t es = e ? (size_t)6 * L * NZ * 4 : 0;
   constexpr size_t ls = l ? (size_t)2 * L * NZ * 4 : 0;
+  if constexpr (z_late<MODE>())
+    return ZLayout{0, zb, zb, zb + es, zb + (rs > es + ls ? rs : es + ls)};
   return ZLayout{0, zb, zb + rs, zb + rs + es, zb + rs + es + ls};
 }
 
@@ -698,6 +707,16 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
   __syncthreads();
 }
 
+// Resident blocks the kernel of a mode is compiled for: the plain update (mode 1, whose
+// late staging leaves room for seven blocks at 128) as many as its shared memory allows,
+// at most eight; the other modes z_min_blocks.
+template <int NZ, int MODE>
+__host__ __device__ constexpr int z_min_blocks_mode() {
+  constexpr int smem = (int)((228u * 1024) / (z_layout<NZ, MODE>().total + 1024 + 128));
+  constexpr int want = smem > 8 ? 8 : smem;
+  return MODE == 1 && want > z_min_blocks<NZ>() ? want : z_min_blocks<NZ>();
+}
+
 // Modes as the generic z pass: 0 init from eps_bar/eps0, 1 plain update, 2 keep eps
 // (not rewritten), 3 Anderson residual into the rings.
 // bulk: the block's global chunks are 16-byte aligned (TMA bulk copies); otherwise the
@@ -706,7 +725,7 @@ __device__ __forceinline__ void zline_fft(float2* zbuf, int q, int p, const floa
 // entries read per voxel from global memory; lambda and mu not staged).
 // MODE >= 0 fixes the mode at compile time (mode_arg is then ignored).
 template <int NZ, int LAW, int MODE>
-__global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fast(
+__global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks_mode<NZ, MODE>()) zpass_fast(
     GridDesc g, int mode_arg, int bulk, const float* __restrict__ lambda, const float* __restrict__ mu,
     float* __restrict__ eps, float2* __restrict__ spec, const double* __restrict__ eps_bar,
     const float* __restrict__ eps0, InstanceState* __restrict__ st, const Medium* __restrict__ med,
@@ -719,7 +738,8 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
   float2* rst = reinterpret_cast<float2*>(zfraw + LY.rst);    // [6][L][NZH] spectrum rows
   float* est = reinterpret_cast<float*>(zfraw + LY.est);      // [6][L][NZ] strain rows
   float* lst = reinterpret_cast<float*>(zfraw + LY.lst);      // [2][L][NZ] lambda, mu rows
-  __shared__ __align__(8) unsigned long long mbar_word;
+  __shared__ __align__(8) unsigned long long mbar_word[2];  // early and late staging
+  constexpr bool late = z_late<MODE>();
   const int b = blockIdx.y;
   if (!active32(st[b])) return;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -736,23 +756,40 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
   const bool need_e = (mode == 1 || mode == 2 || mode == 3);
   const bool need_l = (mode != 3) && LAW != 2;
 
-  // ---- stage this block's inputs in shared memory
+  // ---- stage this block's inputs in shared memory (modes 1 and 3: the spectrum rows now,
+  // the strain (and lambda, mu) rows after the spectrum rows are consumed)
+  const unsigned ebytes = L * NZ * 4;
+  auto stage_late_bulk = [&](unsigned mbar2) {
+    // (the block's reads of the spectrum rows are ordered before these async-proxy writes
+    // by the preceding barrier and the proxy fence)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const unsigned total = 6 * ebytes + (need_l ? 2 * ebytes : 0);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar2), "r"(total) : "memory");
+    for (int c = 0; c < 6; ++c)
+      bulk_g2s(est + (size_t)c * L * NZ, eb + (size_t)c * g.nv + l0 * NZ, ebytes, mbar2);
+    if (need_l) {
+      bulk_g2s(lst, lambda + l0 * NZ, ebytes, mbar2);
+      bulk_g2s(lst + L * NZ, mu + l0 * NZ, ebytes, mbar2);
+    }
+  };
   if (bulk) {
-    const unsigned mbar = smem_u32(&mbar_word);
+    const unsigned mbar = smem_u32(&mbar_word[0]);
     if (tid == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mbar) : "memory");
+      if (late) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar_word[1])) : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     if (tid == 0) {
-      const unsigned rbytes = L * NZH * 8, ebytes = L * NZ * 4;
-      const unsigned total = (need_r ? 6 * rbytes : 0) + (need_e ? 6 * ebytes : 0) + (need_l ? 2 * ebytes : 0);
+      const unsigned rbytes = L * NZH * 8;
+      const bool e_now = need_e && !late, l_now = need_l && !late;
+      const unsigned total = (need_r ? 6 * rbytes : 0) + (e_now ? 6 * ebytes : 0) + (l_now ? 2 * ebytes : 0);
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(total) : "memory");
       for (int c = 0; c < 6; ++c) {
         if (need_r) bulk_g2s(rst + (size_t)c * L * NZH, sb + ((size_t)c * nlines + l0) * NZH, rbytes, mbar);
-        if (need_e) bulk_g2s(est + (size_t)c * L * NZ, eb + (size_t)c * g.nv + l0 * NZ, ebytes, mbar);
+        if (e_now) bulk_g2s(est + (size_t)c * L * NZ, eb + (size_t)c * g.nv + l0 * NZ, ebytes, mbar);
       }
-      if (need_l) {
+      if (l_now) {
         bulk_g2s(lst, lambda + l0 * NZ, ebytes, mbar);
         bulk_g2s(lst + L * NZ, mu + l0 * NZ, ebytes, mbar);
       }
@@ -772,10 +809,10 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
     for (int c = 0; c < 6; ++c) {
       if (need_r)
         for (int i = tid; i < L * NZH; i += nt) rst[c * L * NZH + i] = sb[((size_t)c * nlines + l0) * NZH + i];
-      if (need_e)
+      if (need_e && !late)
         for (int i = tid; i < L * NZ; i += nt) est[c * L * NZ + i] = eb[(size_t)c * g.nv + l0 * NZ + i];
     }
-    if (need_l)
+    if (need_l && !late)
       for (int i = tid; i < L * NZ; i += nt) {
         lst[i] = lambda[l0 * NZ + i];
         lst[L * NZ + i] = mu[l0 * NZ + i];
@@ -798,7 +835,32 @@ __global__ void __launch_bounds__(z_threads<NZ>(), z_min_blocks<NZ>()) zpass_fas
       if (!selfconj) Z[NZ - k] = make_float2(A.x + B.y, A.y - B.x);
     }
     __syncthreads();
-    zline_fft<NZ>(zbuf, q, p, tw);
+    if constexpr (late) {
+      // the strain (and lambda, mu) rows into the spectrum rows' region, during the transform
+      if (bulk) {
+        if (tid == 0) stage_late_bulk(smem_u32(&mbar_word[1]));
+      } else {
+        for (int c = 0; c < 6; ++c)
+          for (int i = tid; i < L * NZ; i += nt) est[c * L * NZ + i] = eb[(size_t)c * g.nv + l0 * NZ + i];
+        if (need_l)
+          for (int i = tid; i < L * NZ; i += nt) {
+            lst[i] = lambda[l0 * NZ + i];
+            lst[L * NZ + i] = mu[l0 * NZ + i];
+          }
+      }
+    }
+    zline_fft<NZ>(zbuf, q, p, tw);  // (ends with a barrier: the plain late loads are visible)
+    if constexpr (late) {
+      if (bulk && !mbar_wait(smem_u32(&mbar_word[1]))) {
+        // as for the early copies: report, stop the instance, wait once more (bounded)
+        if (tid == 0) {
+          st[b].status = kTimeout;
+          st[b].done = 1;
+        }
+        if (!mbar_wait(smem_u32(&mbar_word[1])) && tid == 0) st[b].copies_lost = 1;
+        return;
+      }
+    }
   }
 
   if (mode == 3) {
