@@ -74,3 +74,34 @@ def test_committed_traffic_matches_accounting():
         assert 0.85 <= ratio <= 1.10, (name, ratio)
         checked += 1
     assert checked >= 7
+
+
+def _run_reference_arm(extra_env):
+    import subprocess
+    import sys
+
+    env = dict(os.environ, **extra_env)
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                           "--steps", "1", "--warmup", "0", "--cpu-sample-s", "1"],
+                          capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` (the CPU port timed on a bounded sample) prints one JSON
+    line with the own arm's metric, unit and direction, a cpu_baseline describing the run and
+    an e2e object with no host-device copies; under torchrun only rank 0 prints."""
+    r = _run_reference_arm({"RANK": "0"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC
+    assert d["unit"] == "solves/s" and d["higher_is_better"] is True and d["value"] > 0
+    assert d["config"]["workload"].startswith(bench.WORKLOAD)
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert cb["unit"] == d["unit"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    r1 = _run_reference_arm({"RANK": "1", "WORLD_SIZE": "2"})
+    assert r1.returncode == 0 and not [l for l in r1.stdout.splitlines() if l.startswith("{")]
