@@ -14,6 +14,11 @@ and cites the file:line it restates:
 * ``cuda/src/fourier.cu`` -- Hermitian weights of the half-spectrum norm;
 * ``src/jaxmaterials/data/data.py`` -- C_eff assembly from six unit loads.
 
+One function restates a published scheme instead of the reference's:
+``conjugate_gradient`` (Zeman et al. 2010) solves the same equation with the reference's
+Gamma^0, criterion and stopping rule; it is the checker for a conjugate-gradient solver
+mode.
+
 Pinned against the reference itself: ``tests/golden/make_golden.py`` runs the
 reference's Python solver on seeded inputs and stores its outputs, and
 ``tests/test_oracle.py`` checks this module against those fixtures and against every
@@ -340,6 +345,68 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
             history.append(e)
         it += 1
     return eps[0], sigma, it
+
+
+def conjugate_gradient(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, maxiter=1000,
+                       dtype=np.float64, workers=None, history=None):
+    """Conjugate gradients on the Lippmann-Schwinger equation (J. Zeman, J. Vondrejc,
+    J. Novak, I. Marek, J. Comput. Phys. 229 (2010) 8065-8071).
+
+    The strain is eps = eps_bar + x with x a compatible zero-mean field solving
+    G[C : x] = -G[C : eps_bar], where G is the projection onto compatible zero-mean strains
+    (the Gamma^0 of ``fourier_solve`` for the reference medium lambda0 = 0, mu0 = 1/2, i.e.
+    C0 the identity). On compatible fields G C is symmetric positive definite in the inner
+    product sum_ij a_ij b_ij (Voigt weights 1, 1, 1, 2, 2, 2), so plain CG applies; every
+    update costs one stress evaluation and one forward/inverse transform pair, as a
+    Moulinec-Suquet update does. Criterion and stop are those of ``lippmann_schwinger``
+    (e <= atol or e <= rtol * e0, e0 the criterion of eps_bar; the criterion is evaluated on
+    the stress of eps_bar + x after every update). Returns ``(epsilon, sigma, iterations)``.
+    """
+    w = _workers(workers)
+    shape = grid.shape
+    axes = (-3, -2, -1)
+    lmbda = np.asarray(lmbda, dtype=dtype)
+    mu = np.asarray(mu, dtype=dtype)
+    xizero = half(get_xizero(grid, dtype=dtype), grid)
+    xi = half(get_xi(grid, dtype=dtype), grid)
+    wv = VOIGT_WEIGHTS.astype(dtype)[:, None, None, None]
+
+    def project(tau):
+        tau_hat = sfft.rfftn(tau, axes=axes, workers=w)
+        return -np.asarray(sfft.irfftn(fourier_solve(tau_hat, 0.0, 0.5, xizero), s=shape,
+                                       axes=axes, workers=w), dtype=dtype)
+
+    def dot(a, b):
+        return float(np.sum(a * b * wv))
+
+    def crit(sig):
+        return relative_divergence_half(sfft.rfftn(sig, axes=axes, workers=w), xi, grid)
+
+    eb = np.broadcast_to(np.asarray(epsilon_bar, dtype=dtype)[:, None, None, None], (6,) + shape)
+    x = np.zeros((6,) + shape, dtype=dtype)
+    sigma = compute_sigma(lmbda, mu, eb)
+    e = crit(sigma)
+    e0 = e
+    if history is not None:
+        history.append(e)
+    r = -project(sigma)
+    p = r.copy()
+    rr = dot(r, r)
+    it = 0
+    while e > atol and e > rtol * e0 and it < maxiter:
+        q = project(compute_sigma(lmbda, mu, p))
+        alpha = rr / dot(p, q)
+        x += alpha * p
+        r -= alpha * q
+        rr_new = dot(r, r)
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+        sigma = compute_sigma(lmbda, mu, eb + x)
+        e = crit(sigma)
+        if history is not None:
+            history.append(e)
+        it += 1
+    return eb + x, sigma, it
 
 
 def c_eff(lmbda, mu, grid, rtol=1e-6, atol=1e-20, depth=0, maxiter=1000,

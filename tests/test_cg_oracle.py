@@ -1,0 +1,43 @@
+"""The conjugate-gradient restatement in the oracle (Zeman et al. 2010; CPU, FP64) solves
+the reference's equation to the reference's criterion: it reaches the same stopping rule as
+the Moulinec-Suquet loop, its mean stress equals that of a tightly converged Anderson solve
+to the tolerance's order, and on config 1's 32^3 cross-ply (contrast about 26) it needs
+fewer updates than Anderson m = 5 (which needs about 2.7 times fewer than the plain loop)."""
+
+import numpy as np
+
+from oracle import ls_oracle as O
+
+N = 32
+
+
+def _material():
+    from jaxmaterials_b200.data import fibres
+
+    lm, mu = fibres.lame_fields(fibres.config_structure("c1", seed=0))
+    return lm.astype(np.float64), mu.astype(np.float64), O.Grid(N, N, N, float(N), float(N), float(N))
+
+
+def test_cg_matches_and_beats_anderson():
+    lm, mu, g = _material()
+    for load in (0, 3):
+        eb = np.zeros(6)
+        eb[load] = 1.0
+        h = []
+        eps, sig, it_cg = O.conjugate_gradient(lm, mu, eb, g, rtol=1e-6, atol=1e-30, history=h)
+        assert h[-1] <= 1e-6 * h[0] and it_cg == len(h) - 1
+        _, _, it_aa = O.lippmann_schwinger(lm, mu, eb, g, rtol=1e-6, atol=1e-30, depth=5,
+                                           maxiter=500, dtype=np.float64)
+        _, s_ref, _ = O.lippmann_schwinger(lm, mu, eb, g, rtol=1e-9, atol=1e-30, depth=5,
+                                           maxiter=2000, dtype=np.float64)
+        m_cg, m_ref = sig.mean(axis=(1, 2, 3)), s_ref.mean(axis=(1, 2, 3))
+        assert np.abs(m_cg - m_ref).max() / np.abs(m_ref).max() < 1e-6
+        assert np.allclose(eps.mean(axis=(1, 2, 3)), eb, atol=1e-12)
+        assert it_cg < it_aa, (load, it_cg, it_aa)
+
+
+def test_cg_homogeneous_needs_no_update():
+    g = O.Grid(8, 6, 4, 1.0, 1.0, 1.0)
+    lm = np.full(g.shape, 1.3)
+    eps, _, it = O.conjugate_gradient(lm, lm, [1.0, 0.2, 0.3, 0.1, 0.0, 0.4], g, atol=1e-12)
+    assert it == 0 and np.allclose(eps[:, 0, 0, 0], [1.0, 0.2, 0.3, 0.1, 0.0, 0.4])
