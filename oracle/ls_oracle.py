@@ -348,7 +348,7 @@ def lippmann_schwinger(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, dept
 
 
 def conjugate_gradient(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, maxiter=1000,
-                       dtype=np.float64, workers=None, history=None, restart=0):
+                       dtype=np.float64, workers=None, history=None, restart=0, stress=None):
     """Conjugate gradients on the Lippmann-Schwinger equation (J. Zeman, J. Vondrejc,
     J. Novak, I. Marek, J. Comput. Phys. 229 (2010) 8065-8071).
 
@@ -365,6 +365,8 @@ def conjugate_gradient(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, maxi
     by the true one, -G[C : (eps_bar + x)], and the search direction by it (beta = 0): in
     FP32 fields the recursive residual drifts and plain CG stalls near 2e-6 and then
     diverges, while with this replacement every 20 updates it converges as in FP64.
+    ``stress``: a linear law ``stress(lmbda, mu, eps)`` with a symmetric positive definite
+    stiffness in place of the isotropic one (as in ``lippmann_schwinger``).
     Returns ``(epsilon, sigma, iterations)``.
     """
     w = _workers(workers)
@@ -375,6 +377,7 @@ def conjugate_gradient(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, maxi
     xizero = half(get_xizero(grid, dtype=dtype), grid)
     xi = half(get_xi(grid, dtype=dtype), grid)
     wv = VOIGT_WEIGHTS.astype(dtype)[:, None, None, None]
+    law = stress or compute_sigma
 
     def project(tau):
         tau_hat = sfft.rfftn(tau, axes=axes, workers=w)
@@ -389,7 +392,7 @@ def conjugate_gradient(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, maxi
 
     eb = np.broadcast_to(np.asarray(epsilon_bar, dtype=dtype)[:, None, None, None], (6,) + shape)
     x = np.zeros((6,) + shape, dtype=dtype)
-    sigma = compute_sigma(lmbda, mu, eb)
+    sigma = law(lmbda, mu, eb)
     e = crit(sigma)
     e0 = e
     if history is not None:
@@ -399,11 +402,11 @@ def conjugate_gradient(lmbda, mu, epsilon_bar, grid, rtol=1e-6, atol=1e-20, maxi
     rr = dot(r, r)
     it = 0
     while e > atol and e > rtol * e0 and it < maxiter:
-        q = project(compute_sigma(lmbda, mu, p))
+        q = project(law(lmbda, mu, p))
         alpha = dtype(rr / dot(p, q))
         x += alpha * p
         r -= alpha * q
-        sigma = compute_sigma(lmbda, mu, eb + x)
+        sigma = law(lmbda, mu, eb + x)
         e = crit(sigma)
         if history is not None:
             history.append(e)

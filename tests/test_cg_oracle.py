@@ -65,3 +65,28 @@ def test_cg_fp32_needs_true_residual_replacement():
                                            maxiter=300, dtype=np.float32)
         assert it32 <= 1.2 * it64 and it32 < it_aa, (load, it32, it64, it_aa)
     assert stalled >= 1
+
+
+def test_cg_anisotropic_law():
+    """CG with the anisotropic law (21 stiffness entries per voxel, positive definite): the
+    mean stress of a tightly converged Anderson solve with the anisotropic Gamma^0. This
+    random two-phase field has a low contrast (plain iteration 34-35 updates), where CG and
+    Anderson m = 5 are even (20-21 against 19-20 updates); the gap opens with the contrast."""
+    from oracle import aniso_oracle as A
+    from tests.aniso_materials import two_phase_field
+
+    n = (16, 12, 10)
+    g = O.Grid(*n, 1.0, 1.0, 1.0)
+    c21 = two_phase_field(n, seed=3)
+    law = lambda lm, m, e: A.stress(c21, e)  # noqa: E731
+    dummy = np.ones(n)
+    for load in (0, 4):
+        eb = np.zeros(6)
+        eb[load] = 1.0
+        _, sig, it_cg = O.conjugate_gradient(dummy, dummy, eb, g, rtol=1e-6, atol=1e-30, stress=law)
+        _, s_ref, _ = A.lippmann_schwinger(c21, eb, g, rtol=1e-10, atol=1e-30, depth=5, maxiter=2000)
+        _, _, it_aa = A.lippmann_schwinger(c21, eb, g, rtol=1e-6, atol=1e-30, depth=5, maxiter=500)
+        _, _, it_pl = A.lippmann_schwinger(c21, eb, g, rtol=1e-6, atol=1e-30, depth=0, maxiter=500)
+        m_cg, m_ref = sig.mean(axis=(1, 2, 3)), s_ref.mean(axis=(1, 2, 3))
+        assert np.abs(m_cg - m_ref).max() / np.abs(m_ref).max() < 1e-6
+        assert it_cg <= it_aa + 2 and it_cg < 0.7 * it_pl, (load, it_cg, it_aa, it_pl)
